@@ -1,0 +1,335 @@
+"""Benchmark: periodic FP64 multigrid solves/s on one 256^3 grid, plus the 256^3 stencil roofline.
+
+Workload (one "step"): -Lap u = f on a periodic cell-centred 256^3 grid (h = 1/256), f = 8 sine
+modes (seed 1, mean removed), 7-point Laplacian, weighted Jacobi omega = 2/3, 2^3 averaging
+restriction, piecewise-constant prolongation, coarsest grid 4^3, iterated from u = 0 to a 1e-10
+relative max-norm residual, all in FP64 on the GPU. The cycle is V(4,4): V(2,2) with this
+restriction/prolongation pair stalls at depth (reference CPU path: 0.48, 0.72, 0.95 per cycle at
+32^3, 64^3, 128^3), so it never reaches 1e-10 at 256^3.
+
+  value : solves/s with inputs resident in HBM (device-timed, max over ranks)
+  e2e   : the same through the public API with host buffers: H2D of f, solve, D2H of u per step
+  stencil: Stencil::apply 7-point FP64 on a 256^3 box (src 258^3), GB/s and fraction of HBM
+  roofline: the dominant kernel, the finest-level Jacobi sweep (k_star_tma<Lap7, EpiRelax>)
+
+Multi-GPU (torchrun): every rank solves its own grid (replicas; no data-path collective), value is
+the whole-job rate. --impl reference times the reference's own CPU code (oracle/_ref) on host cores.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N = 256
+LEVELS = 6            # 256 -> 4
+NU1 = NU2 = 4
+NU_BOTTOM = 10
+OMEGA = 2.0 / 3.0
+TOL = 1e-10
+MAX_ITER = 100
+STENCIL_BYTES = 8 * (258 ** 3 + 256 ** 3)          # algorithmic bytes of dst |= L(src), 256^3
+RELAX_BYTES = 24 * 256 ** 3                        # read phi, read rho, write phi_new
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+def workload_config():
+    return {"workload": "periodic Poisson multigrid, 256^3 cell-centred FP64, 7-point, V(%d,%d) weighted Jacobi "
+                        "omega=2/3, 2^3 average restriction, constant prolongation, coarsest 4^3, tol 1e-10 "
+                        "(max-norm, relative), f = 8 sine modes seed 1" % (NU1, NU2),
+            "n": N, "levels": LEVELS + 1, "nu1": NU1, "nu2": NU2, "nu_bottom": NU_BOTTOM, "omega": OMEGA,
+            "tol": TOL, "l2_policy": "inputs larger than L2 (each 256^3 field is 134 MB; solver state ~0.9 GB)"}
+
+
+class Clocks:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, mx, reasons = [], None, set()
+        for line in out.strip().splitlines():
+            f = [v.strip() for v in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"], f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference_rate(iters_per_solve, procs=None, reps=1):
+    """Reference CPU path (oracle/_ref) on host cores: each process times `reps` V-cycles plus the
+    residual norm of the 256^3 solve; the rate scales by the GPU's cycle count (same arithmetic,
+    same count). Independent processes, one solve each, as the reference solver is single-threaded."""
+    import multiprocessing as mp
+    from oracle.oracle import Ref
+    ncpu = os.cpu_count() or 1
+    if procs is None:
+        procs = max(1, min(16, ncpu // 2))
+    if Ref.available():
+        ctx = mp.get_context("spawn")
+        with ctx.Pool(procs) as pool:
+            times = pool.map(_ref_cycle_time, [reps] * procs)
+        t_cycle = float(np.mean(times)) / reps
+        rate = procs / (t_cycle * iters_per_solve)
+        return {"value": rate, "unit": "solves/s", "cores": procs, "kind": "reference",
+                "sample": "%d V(%d,%d) cycle(s) + residual norm of the 256^3 solve in each of %d processes "
+                          "(reference LevelBoxData/Stencil code, box 64, 1 thread each), scaled by %d cycles per "
+                          "solve; mean cycle %.2f s" % (reps, NU1, NU2, procs, iters_per_solve, t_cycle)}
+    # the C restatement with OpenMP threads
+    from oracle.oracle import Port
+    from proto_b200 import workloads as W
+    P = Port()
+    rho = W.poisson_rho(N, seed=1).reshape(-1).copy()
+    phi = np.zeros(N ** 3)
+    t0 = time.perf_counter()
+    n, _ = P.mg_cs(N, LEVELS, NU1, NU2, NU_BOTTOM, OMEGA, 1.0, None, reps, 0.0, rho, phi)
+    t = (time.perf_counter() - t0) / max(n, 1)
+    return {"value": 1.0 / (t * iters_per_solve), "unit": "solves/s", "cores": P.num_threads(), "kind": "port",
+            "sample": "%d V-cycle(s) of the 256^3 solve with the C restatement (OpenMP), scaled by %d cycles" %
+                      (reps, iters_per_solve)}
+
+
+def _ref_cycle_time(reps):
+    sys.path.insert(0, ROOT)
+    from oracle.oracle import Ref
+    from proto_b200 import workloads as W
+    R = Ref()
+    rho = W.poisson_rho(N, seed=1).reshape(-1).copy()
+    return R.mg_cs_time_cycles(N, 64, LEVELS, NU1, NU2, NU_BOTTOM, OMEGA, rho, reps)
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    iters = 14   # cycles per solve of this workload (the GPU arm measures the same count)
+    try:
+        import json as _j
+        p = os.path.join(ROOT, "profiles", "bench_iters.json")
+        if os.path.exists(p):
+            iters = int(_j.load(open(p))["iters"])
+    except Exception:
+        pass
+    t0 = time.perf_counter()
+    cb = cpu_reference_rate(iters)
+    wall = time.perf_counter() - t0
+    line = {"impl": "reference", "metric": "MG solves/s", "value": cb["value"], "unit": "solves/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 / cb["value"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic", "config": workload_config(), "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "wall_s": wall}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    import proto_b200 as pb
+    from proto_b200 import workloads as W
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(v):
+        if dist is None:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    params = pb.MGParams(n=N, levels=LEVELS, nu1=NU1, nu2=NU2, nu_bottom=NU_BOTTOM, omega=OMEGA,
+                         max_iter=MAX_ITER, tol=TOL)
+    mg = pb.Multigrid(params)
+    rho_host = W.poisson_rho(N, seed=1).reshape(-1).copy()
+    rho = torch.from_numpy(rho_host).cuda()
+    phi = torch.zeros(N ** 3, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def one_solve():
+        phi.zero_()
+        return mg.solve(rho, phi)
+
+    for _ in range(max(args.warmup, 3)):
+        it, hist = one_solve()
+    iters = it
+    barrier()
+    clocks = Clocks(local)
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    per_solve = []
+    ev0.record(stream)
+    for _ in range(args.steps):
+        e_a, e_b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e_a.record(stream)
+        it, hist = one_solve()
+        e_b.record(stream)
+        per_solve.append((e_a, e_b))
+        assert it == iters
+    ev1.record(stream)
+    barrier()
+    clk = clocks.stop()
+    t_dev = ev0.elapsed_time(ev1) / 1000.0
+    lat = sorted(a.elapsed_time(b) for a, b in per_solve)
+    t_max = max_over_ranks(t_dev)
+    value = world * args.steps / t_max
+
+    # end to end: host buffers, H2D of f and D2H of u inside the timed region
+    rho_pin = torch.from_numpy(rho_host).pin_memory()
+    out_pin = torch.empty(N ** 3, dtype=torch.float64).pin_memory()
+    rho_dev = torch.empty_like(rho)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        rho_dev.copy_(rho_pin, non_blocking=True)
+        phi.zero_()
+        mg.solve(rho_dev, phi)
+        out_pin.copy_(phi, non_blocking=True)
+    e1.record(stream)
+    barrier()
+    t_e2e = max_over_ranks(e0.elapsed_time(e1) / 1000.0)
+    e2e = world * args.steps / t_e2e
+
+    # kernel-level figures (device events on the launching stream)
+    coefs = [-6.0, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0]
+    offs = [(0, 0, 0), (1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1)]
+    S = pb.Stencil(coefs, offs)
+    src = torch.rand(258 ** 3, dtype=torch.float64, device="cuda")
+    dst = torch.empty(256 ** 3, dtype=torch.float64, device="cuda")
+    sbox, dbox = pb.Box.cube(256).grow(1), pb.Box.cube(256)
+    reps = 20
+    for _ in range(3):
+        S.apply(src, sbox, dst, dbox, scale=65536.0)
+    barrier()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(reps):
+        S.apply(src, sbox, dst, dbox, scale=65536.0)
+    b.record(stream)
+    barrier()
+    t_st = a.elapsed_time(b) / 1000.0 / reps
+    for _ in range(3):
+        mg.relax(1)
+    barrier()
+    a.record(stream)
+    for _ in range(reps):
+        mg.relax(1)
+    b.record(stream)
+    barrier()
+    t_rx = a.elapsed_time(b) / 1000.0 / reps
+    pb.device_check()
+    peak, peak_kind = measured_peaks()
+    st_gbs = STENCIL_BYTES / t_st / 1e9
+    rx_gbs = RELAX_BYTES / t_rx / 1e9
+
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "relax_traffic.json")
+    if os.path.exists(tp):
+        try:
+            traffic = json.load(open(tp)).get("bytes_per_launch_256")
+        except Exception:
+            traffic = None
+
+    if rank == 0:
+        launches = 3 + iters * mg.launches_per_cycle() + 1
+        line = {
+            "metric": "MG solves/s", "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * t_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(), "iters_per_solve": iters, "final_rel_residual": hist[-1] / hist[0],
+            "latency_ms": {"p50": lat[len(lat) // 2], "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
+            "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": 8 * N ** 3,
+                    "d2h_bytes_per_step": 8 * N ** 3},
+            "stencil": {"metric": "Stencil::apply 7-point FP64 256^3 GB/s", "value": st_gbs, "unit": "GB/s",
+                        "frac_of_hbm": st_gbs / peak, "us_per_apply": t_st * 1e6,
+                        "gpts_per_s": 256 ** 3 / t_st / 1e9, "algorithmic_bytes": STENCIL_BYTES},
+            "roofline": {"bound": "hbm", "kernel": "k_star_tma<Lap7,EpiRelax> (finest-level Jacobi sweep)",
+                         "achieved": rx_gbs, "peak": peak, "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
+                         "unit": "GB/s", "frac": rx_gbs / peak, "traffic": traffic,
+                         "algorithmic_bytes_per_launch": RELAX_BYTES, "us_per_launch": t_rx * 1e6},
+            "gpu_launches": launches * args.steps,
+            "clocks": clk,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            try:
+                line["cpu_baseline"] = cpu_reference_rate(iters)
+            except Exception as e:  # the baseline never hides the GPU result
+                line["cpu_baseline"] = {"error": str(e)}
+        try:
+            os.makedirs(os.path.join(ROOT, "profiles"), exist_ok=True)
+        except OSError:
+            pass
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

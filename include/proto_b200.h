@@ -1,0 +1,182 @@
+/*
+ * proto_b200.h — C ABI of the B200 (sm_100a) structured-grid library.
+ *
+ * Every entry point is extern "C", takes plain pointers, sizes and boxes, returns an int status
+ * (PB_OK == 0, negative on error; nothing aborts or exits) and enqueues its GPU work on the
+ * caller's CUDA stream (a cudaStream_t passed as void*; NULL is the legacy default stream).
+ * Field pointers are DEVICE pointers owned by the caller; the library never frees them.
+ *
+ * Data layout is the reference's BoxData layout (include/base/Proto_BoxData.H:311 and
+ * include/base/implem/Proto_BoxDataImplem.H:700-720 in the reference project): a field of C
+ * components on Box [lo,hi] holds C contiguous blocks, each x fastest, linear index
+ * (x-lo.x) + nx*((y-lo.y) + ny*(z-lo.z)) (Box::sindex, Proto_BoxImplem.H:76-86).
+ *
+ * Floating-point results of the FP64 entry points are bitwise equal to the reference's CPU path
+ * (Stencil::hostApply term order, scale folded into the coefficients, one rounding per written
+ * operation, no fused multiply-add).
+ */
+#ifndef PROTO_B200_H
+#define PROTO_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------------------------- */
+enum {
+    PB_OK = 0,
+    PB_ERR_ARG = -1,          /* null pointer, bad count, bad enum                               */
+    PB_ERR_BOX = -2,          /* box empty where forbidden, or outside the field it indexes      */
+    PB_ERR_CUDA = -3,         /* a CUDA runtime call failed; pb_last_cuda_error() has the code   */
+    PB_ERR_ALIGN = -4,        /* pointer alignment the call requires is not met                  */
+    PB_ERR_NOMEM = -5,        /* device or host allocation failed                                */
+    PB_ERR_UNSUPPORTED = -6,  /* valid request outside what this build implements                */
+    PB_ERR_BUDGET = -7,       /* request exceeds the configured memory budget                    */
+    PB_ERR_DEVICE = -8,       /* a kernel flagged an error (bounded wait expired, bad plan)      */
+    PB_ERR_GHOST = -9         /* ghost width smaller than the stencil footprint                  */
+};
+
+typedef struct { int lo[3]; int hi[3]; } pb_box;   /* inclusive corners, like Proto::Box */
+
+const char* pb_status_string(int status);
+int pb_last_cuda_error(void);
+/* Reads (and clears) the device-side error flag of the current device; synchronises the stream. */
+int pb_device_check(void* stream);
+/* Library version string and the compute capability it was built for ("sm_100a"). */
+const char* pb_version(void);
+
+/* ---- Stencil (reference: Stencil<T>, include/base/Proto_Stencil.H:239-911) -------------------
+ * A closed coefficient/offset table in insertion order (Stencil::addCoef keeps insertion order,
+ * Proto_StencilImplem.H:238-276), with source ratio, destination ratio and destination shift.
+ * Replaces Stencil::closeForDevice (Proto_StencilImplem.H:539-556): immutable once created. */
+typedef struct pb_stencil pb_stencil;
+
+int pb_stencil_create(const double* coefs, const int* offsets /* nterms x 3 */, int nterms,
+                      const int src_ratio[3], const int dst_ratio[3], const int dst_shift[3],
+                      pb_stencil** out);
+int pb_stencil_destroy(pb_stencil* s);
+/* Number of terms, span (bounding box of the offsets) and the specialised kernel picked
+ * (0 generic table kernel, 1 seven-point Laplacian, 2 thirteen-point Laplacian). */
+int pb_stencil_info(const pb_stencil* s, int* nterms, pb_box* span, int* shape);
+
+/* Stencil::apply(src, dst, box, initToZero, scale) (Proto_StencilImplem.H:412-431, the DEVICE
+ * branch protoApply at :844-895). 'box' is in the stencil's index space; an empty box (any
+ * hi < lo) is inferred as indexDomain(dstBox) & indexRange(srcBox), as the reference does.
+ * init_to_zero = 1 is "dst |= S(src, scale)", 0 is "dst += S(src, scale)". */
+int pb_stencil_apply_f64(const pb_stencil* s, const double* src, pb_box src_box,
+                         double* dst, pb_box dst_box, pb_box box, int ncomp,
+                         int init_to_zero, double scale, void* stream);
+int pb_stencil_apply_f32(const pb_stencil* s, const float* src, pb_box src_box,
+                         float* dst, pb_box dst_box, pb_box box, int ncomp,
+                         int init_to_zero, float scale, void* stream);
+
+/* Fused stencil + forall (one HBM pass). With Lu = S(u, scale) on 'box' (inferred when empty):
+ *   PB_EPI_AXPBY : out = a*Lu + b*u          (forall body "out = a*Lu + b*u")
+ *   PB_EPI_EULER : out = u + a*Lu            (forall body "u += dt*Lu", written out of place)
+ * Each result is bitwise what the reference gets from "BoxData Lu = S(u, scale)" followed by
+ * forallInPlace over the same box. */
+enum { PB_EPI_AXPBY = 1, PB_EPI_EULER = 2 };
+int pb_stencil_apply_fused_f64(const pb_stencil* s, int epilogue, const double* u, pb_box u_box,
+                               double* out, pb_box out_box, pb_box box, double scale,
+                               double a, double b, void* stream);
+
+/* ---- BoxData algebra and pointwise kernels (reference: BoxData::operatorT,
+ * Proto_BoxDataImplem.H:938-985 and :1086-1110; setVal :1261-1279; copyTo :493-640) ---------- */
+enum { PB_OP_ADD = 0, PB_OP_SUB = 1, PB_OP_MUL = 2, PB_OP_DIV = 3, PB_OP_ASSIGN = 4 };
+/* dst op= src on dst_box & src_box, every component */
+int pb_boxdata_op_f64(int op, double* dst, pb_box dst_box, const double* src, pb_box src_box,
+                      int ncomp, void* stream);
+/* dst op= scalar on 'region' (empty region = whole dst box) */
+int pb_boxdata_scalar_f64(int op, double* dst, pb_box dst_box, pb_box region, double scalar,
+                          int ncomp, void* stream);
+/* copyTo(dst, srcRegion, shift): dst(p + shift) = src(p) for p in src_region & src_box with
+ * p + shift in dst_box */
+int pb_boxdata_copy_f64(const double* src, pb_box src_box, double* dst, pb_box dst_box,
+                        pb_box src_region, const int shift[3], int ncomp, void* stream);
+/* forall "out = a*x + b*y" over out_box & x_box & y_box (one component) */
+int pb_forall_axpby_f64(double* out, pb_box out_box, const double* x, pb_box x_box,
+                        const double* y, pb_box y_box, double a, double b, void* stream);
+
+/* ---- Reductions (reference: Reduction<T,OP,MEM>, include/base/Proto_Reduction.H:30-185) ------
+ * op: 0 Max (initial value DBL_MIN, as the reference), 1 Min, 2 Abs (absMax), 3 Sum, 4 SumAbs,
+ * 5 SumSquare, over 'region' of a field on 'box' (empty region = whole box), one component.
+ * pb_reduce_f64 waits for the result (Reduction::fetch); the _async form leaves the result in
+ * device memory. Max/Min/Abs are exact; sums use a fixed two-level tree (deterministic run to run). */
+int pb_reduce_f64(int op, const double* data, pb_box box, pb_box region, double* result, void* stream);
+int pb_reduce_async_f64(int op, const double* data, pb_box box, pb_box region, double* result_dev,
+                        void* stream);
+
+/* ---- Prolongation (reference: InterpStencil<T>::Constant, Proto_InterpStencilDefs.H:1-15,
+ * applied by InterpStencil::apply, Proto_InterpStencilImplem.H:91-118) ----------------------
+ * dst(p) (=|+=) scale*src(p/ratio) over range(src_box) & dst_box. */
+int pb_interp_constant_f64(int ratio, const double* src, pb_box src_box, double* dst, pb_box dst_box,
+                           int overwrite, double scale, void* stream);
+
+/* ---- Level data and ghost exchange (reference: LevelBoxData::exchange,
+ * include/base/implem/Proto_LevelBoxDataImplem.H:315-329; motion plans :900-951) ---------------
+ * A level is npatch disjoint patches tiling 'domain' (uneven sizes allowed), each stored as its
+ * box grown by 'ghost', all in ONE device slab: patch i starts at element offset offsets[i]
+ * (pb_level_layout fills the offsets and the slab size in elements per component; components of
+ * a patch are contiguous blocks). Exchange sets every ghost cell to the valid cell at its periodic
+ * image, in one kernel launch for the whole level. */
+typedef struct pb_level pb_level;
+int pb_level_create(const pb_box* patches, int npatch, const int ghost[3], pb_box domain,
+                    const int periodic[3], int ncomp, pb_level** out);
+int pb_level_destroy(pb_level* lv);
+int pb_level_layout(const pb_level* lv, long long* offsets /* npatch, may be NULL */,
+                    long long* slab_elems, int* nitems);
+int pb_level_exchange_f64(const pb_level* lv, double* slab, void* stream);
+/* Batched stencil step over every patch of a level, one launch: out = u + a*S(u, scale) on each
+ * patch's valid box (PB_EPI_EULER), or out = S(u, scale) (epilogue 0). u and out are slabs of the
+ * same level. */
+int pb_level_stencil_f64(const pb_level* lv, const pb_stencil* s, int epilogue, const double* u_slab,
+                         double* out_slab, double scale, double a, void* stream);
+
+/* ---- Point-Jacobi multigrid (reference: LevelMultigridSolver, include/utils/implem/
+ * Proto_LevelMultigridSolverImplem.H:85-433, and the archived LevelMultigrid,
+ * examples/_archived/LevelMultigrid/src/LevelMultigrid.cpp) ------------------------------------
+ * Periodic cell-centred N^3 grid, one box per level, levels+1 grids (N >> levels is the coarsest).
+ * form PB_MG_POISSON: solves L_h phi = rhs with the reference's archived smoother written as
+ *   phi += L(phi, omega/6) + (-omega*h*h/6)*rhs        (omega = 1/2 reproduces the archived solver)
+ * form PB_MG_HELMHOLTZ: alpha*phi - beta*L_h phi = rhs with per-cell alpha,
+ *   phi += (omega*r)/(alpha + 6*beta/h^2),  r = rhs - (alpha*phi - beta*L(phi, 1/h^2))
+ * Correction-scheme V(nu1,nu2) cycles, nu_bottom sweeps on the coarsest grid, 2^3 averaging
+ * restriction, piecewise-constant prolongation, max-norm residual; stops when
+ * res < tol*res0 or after max_iter cycles.
+ * precision PB_MG_FP64: every level in FP64, bitwise equal to the CPU reference path.
+ * precision PB_MG_MIXED: FP64 residual, correction and norms around FP32 V-cycles (iterative
+ * refinement); converges to the same tolerance, not bitwise. */
+enum { PB_MG_POISSON = 0, PB_MG_HELMHOLTZ = 1 };
+enum { PB_MG_FP64 = 0, PB_MG_MIXED = 1 };
+typedef struct {
+    int n;            /* finest edge (cells); n must be divisible by 2^levels (coarsest edge >= 1) */
+    int levels;       /* number of coarsenings                                                  */
+    int nu1, nu2, nu_bottom;
+    double omega;
+    double beta;      /* Helmholtz only */
+    int form;         /* PB_MG_POISSON / PB_MG_HELMHOLTZ */
+    int precision;    /* PB_MG_FP64 / PB_MG_MIXED */
+    int max_iter;
+    double tol;
+} pb_mg_params;
+typedef struct pb_mg pb_mg;
+int pb_mg_create(const pb_mg_params* p, pb_mg** out);
+int pb_mg_destroy(pb_mg* mg);
+/* Device bytes held by a solver with these parameters (for admission against a budget). */
+long long pb_mg_device_bytes(const pb_mg_params* p);
+/* alpha: device pointer, n^3 cells (x fastest), Helmholtz form only. */
+int pb_mg_set_alpha(pb_mg* mg, const double* alpha, void* stream);
+/* rhs, phi: device pointers to n^3 cells (x fastest); phi holds the initial guess and receives the
+ * solution. hist (host, max_iter+1 doubles, may be NULL) receives the residual norms; *iters the
+ * number of V-cycles. Blocks until the solve ends. */
+int pb_mg_solve(pb_mg* mg, const double* rhs, double* phi, int* iters, double* hist, void* stream);
+/* LevelMultigridSolver's relax on the finest level: 'sweeps' Jacobi sweeps of the solver's current
+ * state (the state left by the last pb_mg_solve). Enqueued only; does not synchronise. */
+int pb_mg_relax(pb_mg* mg, int sweeps, void* stream);
+/* Kernel launches one V-cycle plus its residual norm issues for these parameters. */
+int pb_mg_launches_per_cycle(const pb_mg_params* p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PROTO_B200_H */

@@ -67,11 +67,12 @@ void or_box_coarsen(const int* lo, const int* hi, const int* r, int* olo, int* o
     for (int d = 0; d < 3; d++) { olo[d] = coarsen_lo(lo[d], r[d]); ohi[d] = coarsen_hi(hi[d], r[d]); }
 }
 
-/* taperCoarsen: high = C integer division (toward zero), low = ceil(lo / r) */
+/* taperCoarsen: high = Point division (rounds toward -infinity, Proto_PointImplem.H:212-239),
+ * low = ceil(lo / r) */
 void or_box_taper_coarsen(const int* lo, const int* hi, const int* r, int* olo, int* ohi)
 {
     for (int d = 0; d < 3; d++) {
-        ohi[d] = hi[d] / r[d];
+        ohi[d] = coarsen_hi(hi[d], r[d]);
         olo[d] = (int)ceil((double)lo[d] / (double)r[d]);
     }
 }

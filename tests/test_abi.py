@@ -1,0 +1,56 @@
+"""The C-ABI library loads, exports every symbol the header declares, and validates arguments on
+the host (no GPU work). CPU only."""
+import ctypes
+
+import pytest
+
+import proto_b200 as pb
+
+
+def test_library_exports_header_symbols():
+    L = pb.lib()
+    names = pb.header_functions()
+    assert len(names) > 20
+    missing = [n for n in names if not hasattr(L, n)]
+    assert missing == []
+
+
+def test_version_and_status_strings():
+    assert b"sm_100a" in pb.lib().pb_version()
+    assert pb.status_string(0) == "ok"
+    assert "footprint" in pb.status_string(-9)
+
+
+def test_stencil_create_and_shape_detection(golden):
+    from tests.util import table
+    _, arrays = golden
+    for name, shape in [("laplacian", 1), ("laplacian13", 2), ("laplacian27", 0), ("avgdown2", 0)]:
+        c, o, m = table(arrays, name)
+        s = pb.Stencil(c, o, tuple(m[:3]), tuple(m[3:6]), tuple(m[6:9]))
+        n, span, sh = s.info()
+        assert n == len(c) and sh == shape
+    c, o, m = table(arrays, "laplacian13")
+    n, span, sh = pb.Stencil(c, o).info()
+    assert span.lo == (-2, -2, -2) and span.hi == (2, 2, 2)
+
+
+def test_stencil_reordered_is_not_specialised(golden):
+    from tests.util import table
+    c, o, m = table(golden[1], "laplacian")
+    # same terms, different insertion order: a different summation order, so the table kernel
+    s = pb.Stencil(c[::-1].copy(), o[::-1].copy())
+    assert s.info()[2] == 0
+
+
+def test_argument_errors():
+    L = pb.lib()
+    h = ctypes.c_void_p()
+    c = (ctypes.c_double * 1)(1.0)
+    o = (ctypes.c_int * 3)(0, 0, 0)
+    bad_ratio = (ctypes.c_int * 3)(0, 1, 1)
+    assert L.pb_stencil_create(c, o, 1, bad_ratio, None, None, ctypes.byref(h)) == -1
+    assert L.pb_stencil_create(None, None, 1, None, None, None, ctypes.byref(h)) == -1
+    with pytest.raises(pb.ProtoError):
+        pb.Multigrid(pb.MGParams(n=48, levels=5))
+    assert pb.MGParams(n=48, levels=5).device_bytes() == -1
+    assert pb.MGParams(n=256, levels=6).device_bytes() > 256 ** 3 * 8 * 3

@@ -1,0 +1,59 @@
+"""Multigrid on the GPU: residual histories bitwise equal to the reference CPU path."""
+import numpy as np
+import pytest
+
+from proto_b200 import workloads as W
+from tests.util import digest
+
+pytestmark = pytest.mark.gpu
+
+
+def _solve(pb, cfg, alpha=None, rhs=None):
+    import torch
+    N = cfg["N"]
+    if cfg["kind"] == "archived":
+        p = pb.MGParams(n=N, levels=cfg["numLevels"], nu1=6, nu2=6, nu_bottom=10, omega=0.5,
+                        max_iter=cfg["maxIter"], tol=cfg["tol"])
+    else:
+        p = pb.MGParams(n=N, levels=cfg["levels"], nu1=cfg["nu1"], nu2=cfg["nu2"], nu_bottom=cfg["nub"],
+                        omega=cfg["omega"], max_iter=cfg["maxIter"], tol=cfg["tol"],
+                        form=pb.MG_HELMHOLTZ if alpha is not None else pb.MG_POISSON)
+    mg = pb.Multigrid(p)
+    rho = W.poisson_rho(N, seed=1) if rhs is None else rhs
+    if alpha is not None:
+        mg.set_alpha(torch.from_numpy(alpha.reshape(-1).copy()).cuda())
+    r = torch.from_numpy(rho.reshape(-1).copy()).cuda()
+    phi = torch.zeros(N ** 3, dtype=torch.float64, device="cuda")
+    it, hist = mg.solve(r, phi)
+    pb.device_check()
+    return it, hist, phi.cpu().numpy()
+
+
+@pytest.mark.parametrize("name", ["archived_32", "cs_v22_32", "cs_v22_64"])
+def test_poisson_history_bitwise(golden, pb, name):
+    cfg = golden[0]["mg"][name]
+    it, hist, phi = _solve(pb, cfg)
+    assert it == cfg["iters"]
+    assert hist == cfg["hist"]
+    assert digest(phi) == cfg["phi_sha256"]
+
+
+def test_helmholtz_history_bitwise(golden, pb):
+    cfg = golden[0]["mg"]["helm_v22_32"]
+    alpha = W.helmholtz_alpha(cfg["N"], seed=3)
+    it, hist, phi = _solve(pb, cfg, alpha=alpha, rhs=-W.poisson_rho(cfg["N"], seed=1))
+    assert it == cfg["iters"]
+    assert hist == cfg["hist"]
+    assert digest(phi) == cfg["phi_sha256"]
+
+
+def test_large_grid_against_port(pb, port):
+    """128^3, V(4,4): the TMA relax kernel on the fine levels, history bitwise vs the C port."""
+    N, lev = 128, 5
+    rho = W.poisson_rho(N, seed=1)
+    cfg = dict(kind="cs", N=N, levels=lev, nu1=4, nu2=4, nub=10, omega=2.0 / 3.0, maxIter=6, tol=1e-10)
+    it, hist, phi = _solve(pb, cfg)
+    p2 = np.zeros(N ** 3)
+    n2, h2 = port.mg_cs(N, lev, 4, 4, 10, 2.0 / 3.0, 1.0, None, 6, 1e-10, rho.reshape(-1).copy(), p2)
+    assert it == n2 and hist == list(h2)
+    assert np.array_equal(phi, p2)

@@ -70,6 +70,12 @@ int pb_stencil_apply_f32(const pb_stencil* s, const float* src, pb_box src_box,
                          float* dst, pb_box dst_box, pb_box box, int ncomp,
                          int init_to_zero, float scale, void* stream);
 
+/* Launch shape of the star-stencil kernels, process wide (autotuner / profiling): mode 0 picks
+ * per box (TMA z-streaming above min_tma_points cells, one thread per point below), 1 forces the
+ * TMA kernel, 2 the one-thread-per-point kernel; zc is the z extent per CTA (0: about six CTAs
+ * per SM); ty the CTA height in rows of 64 points (4, 8 or 16). min_tma_points < 0 keeps it. */
+int pb_star_tune_set(int mode, int zc, int ty, long long min_tma_points);
+
 /* Fused stencil + forall (one HBM pass). With Lu = S(u, scale) on 'box' (inferred when empty):
  *   PB_EPI_AXPBY : out = a*Lu + b*u          (forall body "out = a*Lu + b*u")
  *   PB_EPI_EULER : out = u + a*Lu            (forall body "u += dt*Lu", written out of place)

@@ -784,9 +784,8 @@ public:
     {
         m_p.max_iter = maxIter;
         m_p.tol = tol;
-        pb_mg_destroy(m_h.get());   // parameters changed: rebuild (cheap relative to a solve)
+        m_h.reset();                // parameters changed: rebuild (cheap relative to a solve)
         pb_mg* h = nullptr;
-        m_h.reset();
         check(pb_mg_create(&m_p, &h), "LevelMultigrid::solve");
         m_h = std::shared_ptr<pb_mg>(h, [](pb_mg* m) { pb_mg_destroy(m); });
         std::vector<double> hist(maxIter + 1);

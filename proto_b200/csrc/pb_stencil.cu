@@ -168,6 +168,23 @@ int stencil_coefs(const pb_stencil* s, double* c, int cap)
 static StarTune g_default_tune;
 StarTune& default_star_tune() { return g_default_tune; }
 
+} // namespace pb
+
+// Launch-shape knobs of the star kernels (used by the autotuner and by profiling sweeps):
+// mode 0 auto / 1 TMA only / 2 simple only; zc z-chunk (0 heuristic); ty CTA height (4, 8, 16).
+extern "C" int pb_star_tune_set(int mode, int zc, int ty, long long min_tma_points)
+{
+    if (mode < 0 || mode > 2 || zc < 0 || (ty != 4 && ty != 8 && ty != 16)) return PB_ERR_ARG;
+    pb::StarTune& t = pb::default_star_tune();
+    t.mode = mode;
+    t.zc = zc;
+    t.ty = ty;
+    if (min_tma_points >= 0) t.min_tma_points = min_tma_points;
+    return PB_OK;
+}
+
+namespace pb {
+
 // ---- apply dispatch ---------------------------------------------------------------------------
 static inline OutMap out_map(const Box3& ib, const Box3& db)
 {

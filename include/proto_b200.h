@@ -112,6 +112,19 @@ int pb_reduce_f64(int op, const double* data, pb_box box, pb_box region, double*
 int pb_reduce_async_f64(int op, const double* data, pb_box box, pb_box region, double* result_dev,
                         void* stream);
 
+/* Allocation-free reduction. No counterpart in the reference: same operations and result
+ * semantics as pb_reduce_async_f64, for callers that cannot have the library call cudaMalloc
+ * (stream capture in progress, device memory owned by another allocator or a fixed budget).
+ * Its scratch is a static device array of 4096 partial results plus a ticket (about 33 KB per GPU
+ * that loads the library, held until exit), so the region volume is limited to 4096*2048 =
+ * 8,388,608 cells; larger regions return PB_ERR_BUDGET. The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture. Every call shares the array: calls whose kernels overlap on the GPU
+ * (different streams, no ordering between them) race. The result is written to result_dev
+ * (device memory); nothing is allocated and nothing synchronises. */
+int pb_reduce_noalloc_f64(int op, const double* data, pb_box box, pb_box region, double* result_dev,
+                          void* stream);
+
 /* ---- Prolongation (reference: InterpStencil<T>::Constant, Proto_InterpStencilDefs.H:1-15,
  * applied by InterpStencil::apply, Proto_InterpStencilImplem.H:91-118) ----------------------
  * dst(p) (=|+=) scale*src(p/ratio) over range(src_box) & dst_box. */

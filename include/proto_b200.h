@@ -70,11 +70,18 @@ int pb_stencil_apply_f32(const pb_stencil* s, const float* src, pb_box src_box,
                          float* dst, pb_box dst_box, pb_box box, int ncomp,
                          int init_to_zero, float scale, void* stream);
 
-/* Launch shape of the star-stencil kernels, process wide (autotuner / profiling): mode 0 picks
- * per box (TMA z-streaming above min_tma_points cells, one thread per point below), 1 forces the
- * TMA kernel, 2 the one-thread-per-point kernel; zc is the z extent per CTA (0: about six CTAs
- * per SM); ty the CTA height in rows of 64 points (4, 8 or 16). min_tma_points < 0 keeps it. */
-int pb_star_tune_set(int mode, int zc, int ty, long long min_tma_points);
+/* Launch-shape knobs of the star kernels (no counterpart in the reference, whose stencils run
+ * on the host or as one CUDA thread per point). mode 0 picks the kernel per box (TMA z-streaming
+ * above min_tma_points cells, one thread per point below), 1 forces the TMA kernel, 2 the
+ * one-thread-per-point kernel; zc is the z extent per CTA (0: chosen from the occupancy so that
+ * whole waves of CTAs fill the SMs); ty the CTA tile height in rows of 64 points and yb the rows
+ * each consumer thread computes, (ty, yb) one of (4,1), (8,1), (8,2), (16,4).
+ * min_tma_points < 0 keeps the current threshold. */
+int pb_star_tune_set(int mode, int zc, int ty, int yb, long long min_tma_points);
+/* Depth of the TMA kernel's shared-memory ring (0: 2R+4 planes, else 2R+1..16) and whether
+ * per-point auxiliary fields of fused kernels (multigrid right-hand sides) are staged through it
+ * by TMA (1) or read from global memory (0). */
+int pb_star_tune_ring(int nst, int aux_smem);
 
 /* Fused stencil + forall (one HBM pass). With Lu = S(u, scale) on 'box' (inferred when empty):
  *   PB_EPI_AXPBY : out = a*Lu + b*u          (forall body "out = a*Lu + b*u")
@@ -164,9 +171,14 @@ int pb_level_stencil_f64(const pb_level* lv, const pb_stencil* s, int epilogue, 
  * res < tol*res0 or after max_iter cycles.
  * precision PB_MG_FP64: every level in FP64, bitwise equal to the CPU reference path.
  * precision PB_MG_MIXED: FP64 residual, correction and norms around FP32 V-cycles (iterative
- * refinement); converges to the same tolerance, not bitwise. */
+ * refinement); converges to the same tolerance, not bitwise. Needs nu1, nu2, levels >= 1.
+ * bottom PB_MG_BOTTOM_RELAX: nu_bottom Jacobi sweeps on the coarsest grid (the reference's bottom).
+ * bottom PB_MG_BOTTOM_DIRECT: exact coarsest solve through the inverse of the coarsest operator
+ *   (at most 512 coarsest cells; a singular operator gets the constant (6/h^2)/N added to every
+ *   entry, which fixes the solution's mean). */
 enum { PB_MG_POISSON = 0, PB_MG_HELMHOLTZ = 1 };
 enum { PB_MG_FP64 = 0, PB_MG_MIXED = 1 };
+enum { PB_MG_BOTTOM_RELAX = 0, PB_MG_BOTTOM_DIRECT = 1 };
 typedef struct {
     int n;            /* finest edge (cells); n must be divisible by 2^levels (coarsest edge >= 1) */
     int levels;       /* number of coarsenings                                                  */
@@ -177,6 +189,7 @@ typedef struct {
     int precision;    /* PB_MG_FP64 / PB_MG_MIXED */
     int max_iter;
     double tol;
+    int bottom;       /* PB_MG_BOTTOM_RELAX / PB_MG_BOTTOM_DIRECT */
 } pb_mg_params;
 typedef struct pb_mg pb_mg;
 int pb_mg_create(const pb_mg_params* p, pb_mg** out);

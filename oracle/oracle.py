@@ -78,13 +78,16 @@ class Port:
         data = _f64(data)
         return self.lib.or_reduce(_c_int(op), _p(data), ctypes.c_long(data.size))
 
-    def mg_cs(self, N, levels, nu1, nu2, nu_bottom, omega, beta, alpha, max_iter, tol, rhs, phi):
+    def mg_cs(self, N, levels, nu1, nu2, nu_bottom, omega, beta, alpha, max_iter, tol, rhs, phi, bottom=0):
+        """bottom 0: nu_bottom coarsest sweeps (the reference's); 1: exact coarsest solve."""
         hist = np.zeros(max_iter + 1)
         rhs = _f64(rhs)
         alpha = None if alpha is None else _f64(alpha)
         n = self.lib.or_mg_cs(_c_int(N), _c_int(levels), _c_int(nu1), _c_int(nu2), _c_int(nu_bottom),
                               _c_dbl(omega), _c_dbl(beta), _p(alpha), _c_int(max_iter), _c_dbl(tol),
-                              _p(rhs), _p(phi), _p(hist))
+                              _p(rhs), _p(phi), _p(hist), _c_int(bottom))
+        if n < 0:
+            raise RuntimeError("or_mg_cs: singular coarsest operator")
         return n, hist[: n + 1]
 
     def plain_apply(self, n, u, out, h, a, b):

@@ -310,6 +310,8 @@ typedef struct {
     double** rhs;          /* per level: n^3 */
     double** alpha;        /* per level: n^3 (Helmholtz) */
     double** tmp;          /* per level: n^3 */
+    int bottom;            /* 0: nuBottom sweeps on the coarsest grid, 1: exact solve with ainv */
+    double* ainv;          /* bottom == 1: inverse of the coarsest operator */
 } or_cs;
 
 static int lvl_n(const or_cs* m, int l) { return m->N >> (m->levels - l); }
@@ -407,6 +409,73 @@ static double cs_resnorm(or_cs* m, int l)
     return best;
 }
 
+/* Exact coarsest solve (no counterpart in the reference, whose bottom solver is relaxation): the
+ * inverse of the coarsest operator by Gauss-Jordan elimination with partial pivoting on [A | I].
+ * A = L(., 1/h^2) (Poisson form) or diag(alpha) - beta*L(., 1/h^2) (Helmholtz form), periodic;
+ * a singular A (Poisson, or alpha == 0 everywhere) gets (6/h^2)/N added to every entry. Each row
+ * takes alpha first, then the 7-point terms in insertion order. Returns 0 on success. */
+static int cs_coarse_inverse(int n0, double h, int helm, double beta, const double* alpha, double* inv)
+{
+    int N = n0 * n0 * n0;
+    double hs = 1. / (h * h);
+    long W = 2L * N;
+    double* M = (double*)calloc((size_t)N * W, sizeof(double));
+    int singular = !helm;
+    if (helm) {
+        singular = 1;
+        for (int i = 0; i < N; i++) singular = singular && alpha[i] == 0.0;
+    }
+    for (int z = 0; z < n0; z++) for (int y = 0; y < n0; y++) for (int x = 0; x < n0; x++) {
+        int i = x + n0 * (y + n0 * z);
+        if (helm) M[i * W + i] += alpha[i];
+        for (int j = 0; j < 7; j++) {
+            int qx = (x + LAP7_OFF[j][0] + n0) % n0, qy = (y + LAP7_OFF[j][1] + n0) % n0, qz = (z + LAP7_OFF[j][2] + n0) % n0;
+            int k = qx + n0 * (qy + n0 * qz);
+            double t = helm ? (-beta) * (LAP7_C[j] * hs) : (LAP7_C[j] * hs);
+            M[i * W + k] += t;
+        }
+    }
+    if (singular) {
+        double reg = (6.0 * hs) / N;
+        for (int i = 0; i < N; i++) for (int k = 0; k < N; k++) M[i * W + k] += reg;
+    }
+    for (int i = 0; i < N; i++) M[i * W + N + i] = 1.0;
+    for (int c = 0; c < N; c++) {
+        int p = c;
+        double best = fabs(M[c * W + c]);
+        for (int r = c + 1; r < N; r++)
+            if (fabs(M[r * W + c]) > best) { best = fabs(M[r * W + c]); p = r; }
+        if (best == 0.0) { free(M); return -1; }
+        if (p != c)
+            for (long j = 0; j < W; j++) { double t = M[p * W + j]; M[p * W + j] = M[c * W + j]; M[c * W + j] = t; }
+        double piv = M[c * W + c];
+        for (long j = 0; j < W; j++) M[c * W + j] = M[c * W + j] / piv;
+        for (int r = 0; r < N; r++) {
+            if (r == c) continue;
+            double f = M[r * W + c];
+            if (f != 0.0)
+                for (long j = 0; j < W; j++) M[r * W + j] = M[r * W + j] - f * M[c * W + j];
+        }
+    }
+    for (int i = 0; i < N; i++) for (int k = 0; k < N; k++) inv[(long)i * N + k] = M[i * W + N + k];
+    free(M);
+    return 0;
+}
+
+/* phi = Ainv * rhs on the coarsest level, products summed in column order */
+static void cs_bottom_direct(or_cs* m)
+{
+    int n = lvl_n(m, 0), N = n * n * n;
+    long S = n + 2;
+    for (int i = 0; i < N; i++) {
+        double acc = 0.0;
+        for (int j = 0; j < N; j++) acc = acc + m->ainv[(long)i * N + j] * m->rhs[0][j];
+        int x = i % n, y = (i / n) % n, z = i / (n * n);
+        m->phi[0][IDX(x + 1, y + 1, z + 1, S)] = acc;
+    }
+    fill_periodic(m->phi[0], n, 1);
+}
+
 static void cs_vcycle(or_cs* m, int l)
 {
     if (l > 0) {
@@ -425,6 +494,8 @@ static void cs_vcycle(or_cs* m, int l)
             u[i] = u[i] + 1.0 * d[IDX(x/2+1, y/2+1, z/2+1, Sc)];
         }
         cs_relax(m, l, m->nu2);
+    } else if (m->bottom) {
+        cs_bottom_direct(m);
     } else {
         cs_relax(m, l, m->nuBottom);
     }
@@ -437,7 +508,8 @@ static void cs_vcycle(or_cs* m, int l)
  * parameters, plus the Helmholtz form. rhs/phi: N^3 (x fastest). hist: maxIter+1 entries.
  * Returns the number of V-cycles run. */
 int or_mg_cs(int N, int levels, int nu1, int nu2, int nuBottom, double omega, double beta,
-             const double* alpha, int maxIter, double tol, const double* rhs, double* phi, double* hist)
+             const double* alpha, int maxIter, double tol, const double* rhs, double* phi, double* hist,
+             int bottom)
 {
     or_cs m;
     m.N = N; m.levels = levels; m.nu1 = nu1; m.nu2 = nu2; m.nuBottom = nuBottom;
@@ -463,6 +535,13 @@ int or_mg_cs(int N, int levels, int nu1, int nu2, int nuBottom, double omega, do
         memcpy(m.alpha[levels], alpha, sizeof(double) * (size_t)N*N*N);
         for (int l = levels; l > 0; l--) avgdown(m.alpha[l], lvl_n(&m, l), m.alpha[l-1]);
     }
+    m.bottom = bottom;
+    m.ainv = 0;
+    if (bottom) {
+        long n0 = lvl_n(&m, 0), N0 = n0 * n0 * n0;
+        m.ainv = (double*)calloc((size_t)(N0 * N0), sizeof(double));
+        if (cs_coarse_inverse((int)n0, lvl_h(&m, 0), m.helm, beta, m.alpha[0], m.ainv) != 0) { free(m.ainv); return -1; }
+    }
     double r0 = cs_resnorm(&m, levels);
     hist[0] = r0;
     int it = 0;
@@ -476,6 +555,7 @@ int or_mg_cs(int N, int levels, int nu1, int nu2, int nuBottom, double omega, do
         phi[IDX(x, y, z, N)] = m.phi[levels][IDX(x+1, y+1, z+1, S)];
     for (int l = 0; l < nl; l++) { free(m.phi[l]); free(m.rhs[l]); free(m.alpha[l]); free(m.tmp[l]); }
     free(m.phi); free(m.rhs); free(m.alpha); free(m.tmp);
+    free(m.ainv);
     return it;
 }
 

@@ -15,7 +15,8 @@ __all__ = ["ProtoError", "lib", "Box", "Stencil", "Level", "Multigrid", "MGParam
            "boxdata_op", "boxdata_scalar", "boxdata_copy", "forall_axpby", "reduce", "reduce_async",
            "interp_constant", "device_check", "OP_ADD", "OP_SUB", "OP_MUL", "OP_DIV", "OP_ASSIGN",
            "RED_MAX", "RED_MIN", "RED_ABS", "RED_SUM", "RED_SUMABS", "RED_SUMSQ", "EPI_AXPBY", "EPI_EULER",
-           "MG_POISSON", "MG_HELMHOLTZ", "MG_FP64", "MG_MIXED", "header_functions"]
+           "MG_POISSON", "MG_HELMHOLTZ", "MG_FP64", "MG_MIXED", "MG_BOTTOM_RELAX", "MG_BOTTOM_DIRECT",
+           "header_functions"]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "lib", "libproto_b200.so")
@@ -26,6 +27,7 @@ RED_MAX, RED_MIN, RED_ABS, RED_SUM, RED_SUMABS, RED_SUMSQ = 0, 1, 2, 3, 4, 5
 EPI_AXPBY, EPI_EULER = 1, 2
 MG_POISSON, MG_HELMHOLTZ = 0, 1
 MG_FP64, MG_MIXED = 0, 1
+MG_BOTTOM_RELAX, MG_BOTTOM_DIRECT = 0, 1
 
 _c_int, _c_dbl, _c_flt, _vp, _c_ll = ctypes.c_int, ctypes.c_double, ctypes.c_float, ctypes.c_void_p, ctypes.c_longlong
 
@@ -37,7 +39,7 @@ class pb_box(ctypes.Structure):
 class pb_mg_params(ctypes.Structure):
     _fields_ = [("n", _c_int), ("levels", _c_int), ("nu1", _c_int), ("nu2", _c_int), ("nu_bottom", _c_int),
                 ("omega", _c_dbl), ("beta", _c_dbl), ("form", _c_int), ("precision", _c_int),
-                ("max_iter", _c_int), ("tol", _c_dbl)]
+                ("max_iter", _c_int), ("tol", _c_dbl), ("bottom", _c_int)]
 
 
 class ProtoError(RuntimeError):
@@ -277,8 +279,8 @@ class Level:
 
 class MGParams:
     def __init__(self, n, levels, nu1=2, nu2=2, nu_bottom=10, omega=2.0 / 3.0, beta=1.0, form=MG_POISSON,
-                 precision=MG_FP64, max_iter=100, tol=1e-10):
-        self.c = pb_mg_params(n, levels, nu1, nu2, nu_bottom, omega, beta, form, precision, max_iter, tol)
+                 precision=MG_FP64, max_iter=100, tol=1e-10, bottom=0):
+        self.c = pb_mg_params(n, levels, nu1, nu2, nu_bottom, omega, beta, form, precision, max_iter, tol, bottom)
 
     def device_bytes(self):
         return lib().pb_mg_device_bytes(ctypes.byref(self.c))

@@ -14,8 +14,9 @@ LIB_DIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIB_DIR, "libproto_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# host code never contracts a*b+c into FMA (the direct coarse solve's inverse must match the oracle's)
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
-         "-Xcompiler", "-fvisibility=default"]
+         "-Xcompiler", "-fvisibility=default", "-Xcompiler", "-ffp-contract=off"]
 
 
 def sources():

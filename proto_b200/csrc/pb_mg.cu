@@ -18,7 +18,9 @@
 //   resnorm        : max | -rho + L(phi, 1/h^2) |                           (block max + one atomic)
 // Each kernel repeats the reference's floating-point operations in the reference's order with no
 // FMA, so the FP64 solver reproduces the reference CPU path's residual history bit for bit.
+#include <cmath>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "pb_internal.cuh"
@@ -29,9 +31,10 @@ namespace pb {
 PB_DEFINE_ERROR_READER(read_error_mg)
 
 // Writes v to the valid cell (x,y,z) of an (n+2)^3 grown periodic box and to every ghost cell
-// that is a periodic image of it.
+// that is a periodic image of it. Out of line: only cells on the box boundary call it, and keeping
+// its index arrays out of the fused stencil kernels keeps their register count low.
 template <typename T>
-__device__ __forceinline__ void store_periodic(T* out, int n, int x, int y, int z, T v)
+__device__ __noinline__ void store_periodic_images(T* out, int n, int x, int y, int z, T v)
 {
     const long long S = n + 2, S2 = S * S;
     int xs[3], ys[3], zs[3];
@@ -51,84 +54,221 @@ __device__ __forceinline__ void store_periodic(T* out, int n, int x, int y, int 
 }
 
 template <typename T>
-struct MGLevelArgs {
-    const T* rhs;      // n^3
-    const T* alpha;    // n^3 (Helmholtz)
-    T* out;            // (n+2)^3
+__device__ __forceinline__ void store_periodic(T* out, int n, int x, int y, int z, T v)
+{
+    const long long S = n + 2;
+    if (x == 0 || x == n - 1 || y == 0 || y == n - 1 || z == 0 || z == n - 1) store_periodic_images(out, n, x, y, z, v);
+    else out[(x + 1) + S * ((y + 1) + S * (long long)(z + 1))] = v;
+}
+
+// Row cursor of a periodic (n+2)^3 output: the address of the row's valid cell at its first z, that
+// z, and flags (1: the row is inside the box, 2: it lies on an x or y face, so every cell of it has
+// ghost images).
+template <typename T>
+struct PeriodicRow {
+    T* p;
+    int z0;
+    int flags;
+    __device__ __forceinline__ bool active() const { return flags & 1; }
+};
+template <typename T>
+__device__ __forceinline__ PeriodicRow<T> periodic_row(T* out, int n, int x, int y, int z0, bool active)
+{
+    const long long S = n + 2;
+    PeriodicRow<T> r;
+    r.p = active ? out + (x + 1) + S * ((y + 1) + S * (long long)(z0 + 1)) : out;
+    r.z0 = z0;
+    r.flags = (active ? 1 : 0) | ((x == 0 || x == n - 1 || y == 0 || y == n - 1) ? 2 : 0);
+    return r;
+}
+// boundary cell given by its address in the grown box: recover (x, y, z) and write the images
+template <typename T>
+__device__ __noinline__ void store_periodic_at(T* out, int n, T* q, T v)
+{
+    const long long S = n + 2, i = q - out;
+    const int x = (int)(i % S) - 1, y = (int)((i / S) % S) - 1, z = (int)(i / (S * S)) - 1;
+    store_periodic_images(out, n, x, y, z, v);
+}
+template <typename T>
+__device__ __forceinline__ void store_row(T* out, int n, const PeriodicRow<T>& r, int zo, T v)
+{
+    const int z = r.z0 + zo;
+    T* q = r.p + (long long)zo * (n + 2) * (n + 2);
+    if ((r.flags & 2) || z == 0 || z == n - 1) store_periodic_at(out, n, q, v);
+    else *q = v;
+}
+template <typename T>
+__device__ __forceinline__ T load_row(const PeriodicRow<T>& r, int n, int zo)
+{
+    return r.p[(long long)zo * (n + 2) * (n + 2)];
+}
+
+// Scalars of one level's smoother.
+template <typename T>
+struct RelaxCoef {
     int n;
     int helm;
-    T neg_lambda;      // Poisson form
+    T neg_lambda;        // Poisson form: -omega*h*h/6
     T beta, omega, diagB;
 };
 
-// relax epilogue: acc = L(phi, w) (Poisson) or L(phi, 1/h^2) (Helmholtz), centre = phi
+// One Jacobi sweep value from the stencil sum acc (L(phi, omega/6) for the Poisson form,
+// L(phi, 1/h^2) for the Helmholtz form), the centre value c, rho and alpha.
+template <typename T>
+__device__ __forceinline__ T relax_value(const RelaxCoef<T>& k, T acc, T c, T rho, T al)
+{
+    if (!k.helm) return dadd(c, dadd(acc, dmul(k.neg_lambda, rho)));
+    const T r = dsub(rho, dsub(dmul(al, c), dmul(k.beta, acc)));
+    return dadd(c, ddiv(dmul(k.omega, r), dadd(al, k.diagB)));
+}
+
+// relax epilogue: auxiliary field 0 = rho, 1 = alpha (Helmholtz)
 template <typename T>
 struct EpiRelax {
-    MGLevelArgs<T> a;
-    __device__ __forceinline__ T init(int, int, int, bool) const { return T(0); }
-    __device__ __forceinline__ void finish(int x, int y, int z, T acc, T c) const
+    T* out;
+    RelaxCoef<T> k;
+    using Row = PeriodicRow<T>;
+    __device__ __forceinline__ Row row(int x, int y, int z0, bool active) const { return periodic_row(out, k.n, x, y, z0, active); }
+    __device__ __forceinline__ T init(const Row&, int, const AuxCtx&) const { return T(0); }
+    __device__ __forceinline__ void finish(const Row& r, int zo, T acc, T c, const AuxCtx& ax) const
     {
-        const long long i = x + (long long)a.n * (y + (long long)a.n * z);
-        T v;
-        if (!a.helm) {
-            T t = dadd(acc, dmul(a.neg_lambda, a.rhs[i]));
-            v = dadd(c, t);
-        } else {
-            T al = a.alpha[i];
-            T r = dsub(a.rhs[i], dsub(dmul(al, c), dmul(a.beta, acc)));
-            v = dadd(c, ddiv(dmul(a.omega, r), dadd(al, a.diagB)));
-        }
-        store_periodic(a.out, a.n, x, y, z, v);
+        if (!r.active()) return;
+        const T al = k.helm ? ax.get<T>(1) : T(0);
+        store_row(out, k.n, r, zo, relax_value(k, acc, c, ax.get<T>(0), al));
     }
-    __device__ __forceinline__ void end() const {}
+    __device__ __forceinline__ void end_warp() const {}
+    __device__ __forceinline__ void end_block() const {}
 };
 
-// residual max-norm epilogue: Poisson acc starts at (0 - rho) with L(phi, 1/h^2)
+// Last FP32 post-smoothing sweep of a mixed-precision cycle, fused with the FP64 correction:
+// u64 += (double) e_new, periodic images included. Auxiliary fields as in EpiRelax.
+struct EpiRelaxUpdate {
+    double* u;
+    RelaxCoef<float> k;
+    using Row = PeriodicRow<double>;
+    __device__ __forceinline__ Row row(int x, int y, int z0, bool active) const { return periodic_row(u, k.n, x, y, z0, active); }
+    __device__ __forceinline__ float init(const Row&, int, const AuxCtx&) const { return 0.f; }
+    __device__ __forceinline__ void finish(const Row& r, int zo, float acc, float c, const AuxCtx& ax) const
+    {
+        if (!r.active()) return;
+        const float al = k.helm ? ax.get<float>(1) : 0.f;
+        const float e = relax_value(k, acc, c, ax.get<float>(0), al);
+        store_row(u, k.n, r, zo, dadd(load_row(r, k.n, zo), (double)e));
+    }
+    __device__ __forceinline__ void end_warp() const {}
+    __device__ __forceinline__ void end_block() const {}
+};
+
+// residual max-norm epilogue: Poisson acc starts at (0 - rho) with L(phi, 1/h^2); Helmholtz
+// r = rho - (alpha*phi - beta*L(phi, 1/h^2)). Auxiliary fields as in EpiRelax.
 template <typename T>
 struct EpiResnorm {
-    MGLevelArgs<T> a;
+    int helm;
+    T beta;
     double* result;
     double m;
-    __device__ __forceinline__ T init(int x, int y, int z, bool active) const
+    using Row = OutRow<T>;
+    __device__ __forceinline__ Row row(int, int, int, bool active) const { return Row{nullptr, active}; }
+    __device__ __forceinline__ T init(const Row& r, int, const AuxCtx& ax) const
     {
-        if (a.helm || !active) return T(0);
-        return dsub(T(0), a.rhs[x + (long long)a.n * (y + (long long)a.n * z)]);
+        if (helm || !r.active) return T(0);
+        return dsub(T(0), ax.get<T>(0));
     }
-    __device__ __forceinline__ void finish(int x, int y, int z, T acc, T c)
+    __device__ __forceinline__ void finish(const Row& r, int, T acc, T c, const AuxCtx& ax)
     {
-        if (!a.helm) {
+        if (!r.active) return;
+        if (!helm) {
             m = upd_abs(m, (double)acc);
         } else {
-            const long long i = x + (long long)a.n * (y + (long long)a.n * z);
-            T r = dsub(a.rhs[i], dsub(dmul(a.alpha[i], c), dmul(a.beta, acc)));
-            m = upd_abs(m, (double)r);
+            const T res = dsub(ax.get<T>(0), dsub(dmul(ax.get<T>(1), c), dmul(beta, acc)));
+            m = upd_abs(m, (double)res);
         }
     }
-    __device__ __forceinline__ void end() { block_max_atomic(m, result); }
+    __device__ __forceinline__ void end_warp() const { warp_max_atomic(m, result); }
+    __device__ __forceinline__ void end_block() const { block_max_atomic(m, result); }
+};
+
+// Mixed precision, one pass over the FP64 state u (auxiliary fields: 0 = f, 1 = alpha):
+//   r = (0 + f) + L(u, -1/h^2)  |  r = f - (alpha*u - beta*L(u, 1/h^2))   (FP64)
+//   norm = max |r|; rhs32 = float(r); first FP32 sweep of the next cycle from e = 0 into e32.
+struct Res64Row {
+    PeriodicRow<float> e;
+    float* r;
+};
+struct EpiRes64 {
+    float* e32;          // (n+2)^3
+    float* rhs32;        // n^3
+    int helm;
+    double beta;
+    RelaxCoef<float> k;
+    double* result;
+    double m;
+    using Row = Res64Row;
+    __device__ __forceinline__ Row row(int x, int y, int z0, bool active) const
+    {
+        Row r;
+        r.e = periodic_row(e32, k.n, x, y, z0, active);
+        r.r = active ? rhs32 + x + (long long)k.n * (y + (long long)k.n * z0) : rhs32;
+        return r;
+    }
+    __device__ __forceinline__ double init(const Row& r, int, const AuxCtx& ax) const
+    {
+        if (helm || !r.e.active()) return 0.0;
+        return dadd(0.0, ax.get<double>(0));
+    }
+    __device__ __forceinline__ void finish(const Row& r, int zo, double acc, double c, const AuxCtx& ax)
+    {
+        if (!r.e.active()) return;
+        double res = acc;
+        float al = 0.f;
+        if (helm) {
+            const double a64 = ax.get<double>(1);
+            res = dsub(ax.get<double>(0), dsub(dmul(a64, c), dmul(beta, acc)));
+            al = __double2float_rn(a64);
+        }
+        m = upd_abs(m, res);
+        const float r32 = __double2float_rn(res);
+        r.r[(long long)zo * k.n * k.n] = r32;
+        store_row(e32, k.n, r.e, zo, relax_value(k, 0.f, 0.f, r32, al));
+    }
+    __device__ __forceinline__ void end_warp() const { warp_max_atomic(m, result); }
+    __device__ __forceinline__ void end_block() const { block_max_atomic(m, result); }
 };
 
 // first sweep from phi == 0 (every read of phi would return +0.0)
 template <typename T>
-__global__ void __launch_bounds__(256) k_relax_first(MGLevelArgs<T> a)
+__global__ void __launch_bounds__(256) k_relax_first(const T* __restrict__ rhs, const T* __restrict__ alpha, T* out,
+                                                     RelaxCoef<T> k)
 {
-    const long long total = (long long)a.n * a.n * a.n;
+    const int n = k.n;
+    const long long total = (long long)n * n * n;
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
-        int x = (int)(i % a.n);
-        long long q = i / a.n;
-        int y = (int)(q % a.n), z = (int)(q / a.n);
-        const T zero = T(0);
-        T v;
-        if (!a.helm) {
-            T t = dadd(zero, dmul(a.neg_lambda, a.rhs[i]));
-            v = dadd(zero, t);
-        } else {
-            T al = a.alpha[i];
-            T r = dsub(a.rhs[i], dsub(dmul(al, zero), dmul(a.beta, zero)));
-            v = dadd(zero, ddiv(dmul(a.omega, r), dadd(al, a.diagB)));
-        }
-        store_periodic(a.out, a.n, x, y, z, v);
+        int x = (int)(i % n);
+        long long q = i / n;
+        int y = (int)(q % n), z = (int)(q / n);
+        const T al = k.helm ? alpha[i] : T(0);
+        store_periodic(out, n, x, y, z, relax_value(k, T(0), T(0), rhs[i], al));
     }
+}
+
+// exact coarsest-level solve: out = Ainv * rhs (one thread per cell, products summed in column order)
+template <typename T>
+__global__ void __launch_bounds__(256) k_bottom_direct(const T* __restrict__ ainv, const T* __restrict__ rhs, T* out,
+                                                       int n)
+{
+    const int N = n * n * n;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        T acc = T(0);
+        for (int j = 0; j < N; j++) acc = dadd(acc, dmul(ainv[(long long)i * N + j], rhs[j]));
+        store_periodic(out, n, i % n, (i / n) % n, i / (n * n), acc);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_to_float(const double* __restrict__ a, float* b, long long n)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        b[i] = __double2float_rn(a[i]);
 }
 
 // coarse right-hand side: AvgDown(2) of the fine residual, children in Box([0,1]^3) order
@@ -239,23 +379,94 @@ __global__ void __launch_bounds__(256) k_avgdown_plain(const T* __restrict__ f, 
     }
 }
 
+
+template <typename T>
 struct MGLevel {
     int n;
     double h, hsqinv;
-    double* phi[2] = {nullptr, nullptr};
-    double* rhs = nullptr;
-    double* alpha = nullptr;
+    T* phi[2] = {nullptr, nullptr};
+    T* rhs = nullptr;
+    T* alpha = nullptr;
     int cur = 0;
 };
+
+// Inverse of the coarsest-level operator (N = n0^3 <= 512 cells), by Gauss-Jordan elimination with
+// partial pivoting on [A | I]. A = L(., 1/h^2) (Poisson form) or diag(alpha) - beta*L(., 1/h^2)
+// (Helmholtz form), periodic; when A is singular (Poisson, or alpha == 0 everywhere) the constant
+// (6/h^2)/N is added to every entry, which fixes the mean of the solution. Row by row, the terms
+// enter A in the order alpha, then the 7-point terms 0, +x, -x, +y, -y, +z, -z.
+static bool coarse_inverse(int n0, double h, int helm, double beta, const double* alpha, std::vector<double>& inv)
+{
+    static const int off[7][3] = {{0, 0, 0}, {1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+    static const double cc[7] = {-6.0, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0};
+    const int N = n0 * n0 * n0;
+    const double hs = 1. / (h * h);
+    std::vector<double> M((size_t)N * 2 * N, 0.0);
+    const size_t W = 2 * (size_t)N;
+    bool singular = !helm;
+    if (helm) {
+        singular = true;
+        for (int i = 0; i < N; i++) singular = singular && alpha[i] == 0.0;
+    }
+    for (int z = 0; z < n0; z++)
+        for (int y = 0; y < n0; y++)
+            for (int x = 0; x < n0; x++) {
+                const int i = x + n0 * (y + n0 * z);
+                if (helm) M[i * W + i] += alpha[i];
+                for (int j = 0; j < 7; j++) {
+                    const int qx = (x + off[j][0] + n0) % n0, qy = (y + off[j][1] + n0) % n0, qz = (z + off[j][2] + n0) % n0;
+                    const int k = qx + n0 * (qy + n0 * qz);
+                    const double t = helm ? (-beta) * (cc[j] * hs) : (cc[j] * hs);
+                    M[i * W + k] += t;
+                }
+            }
+    if (singular) {
+        const double reg = (6.0 * hs) / N;
+        for (int i = 0; i < N; i++)
+            for (int k = 0; k < N; k++) M[i * W + k] += reg;
+    }
+    for (int i = 0; i < N; i++) M[i * W + N + i] = 1.0;
+    for (int c = 0; c < N; c++) {
+        int p = c;
+        double best = std::fabs(M[c * W + c]);
+        for (int r = c + 1; r < N; r++)
+            if (std::fabs(M[r * W + c]) > best) {
+                best = std::fabs(M[r * W + c]);
+                p = r;
+            }
+        if (best == 0.0) return false;
+        if (p != c)
+            for (size_t j = 0; j < W; j++) std::swap(M[p * W + j], M[c * W + j]);
+        const double piv = M[c * W + c];
+        for (size_t j = 0; j < W; j++) M[c * W + j] = M[c * W + j] / piv;
+        for (int r = 0; r < N; r++) {
+            if (r == c) continue;
+            const double f = M[r * W + c];
+            if (f != 0.0)
+                for (size_t j = 0; j < W; j++) M[r * W + j] = M[r * W + j] - f * M[c * W + j];
+        }
+    }
+    inv.assign((size_t)N * N, 0.0);
+    for (int i = 0; i < N; i++)
+        for (int k = 0; k < N; k++) inv[(size_t)i * N + k] = M[i * W + N + k];
+    return true;
+}
 
 } // namespace pb
 
 struct pb_mg {
     pb_mg_params p;
-    std::vector<pb::MGLevel> lv;   // index 0 = coarsest
+    std::vector<pb::MGLevel<double>> lv;    // FP64 hierarchy, index 0 = coarsest (precision FP64)
+    std::vector<pb::MGLevel<float>> lv32;   // FP32 hierarchy including the finest grid (precision MIXED)
+    double* u64 = nullptr;                  // MIXED: FP64 solution, (n+2)^3 with periodic images
+    double* f64 = nullptr;                  // MIXED: FP64 right-hand side, n^3
+    double* alpha64 = nullptr;              // MIXED, Helmholtz: FP64 alpha, n^3
+    double* ainv64 = nullptr;               // direct bottom solve: inverse of the coarsest operator
+    float* ainv32 = nullptr;
     double* d_res = nullptr;
-    double* h_res = nullptr;       // pinned
+    double* h_res = nullptr;                // pinned
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    int graph_cur[2] = {0, 0};              // FP64: finest-level buffer index a graph leaves behind
     cudaStream_t graph_stream = nullptr;
     int device = 0;
 };
@@ -263,118 +474,207 @@ struct pb_mg {
 using namespace pb;
 
 static inline double lambda_of(const pb_mg_params& p, double h) { return (p.omega * (h * h)) / 6.0; }
+static inline bool is_mixed(const pb_mg* mg) { return mg->p.precision == PB_MG_MIXED; }
+static inline bool is_helm(const pb_mg* mg) { return mg->p.form == PB_MG_HELMHOLTZ; }
 
-static int launch_relax(pb_mg* mg, int l, bool first, cudaStream_t st)
+template <typename T>
+static Box3 grown_box(const MGLevel<T>& L)
 {
-    MGLevel& L = mg->lv[l];
-    MGLevelArgs<double> a;
-    a.rhs = L.rhs;
-    a.alpha = L.alpha;
-    a.out = L.phi[1 - L.cur];
-    a.n = L.n;
-    a.helm = mg->p.form == PB_MG_HELMHOLTZ;
-    a.neg_lambda = -lambda_of(mg->p, L.h);
-    a.beta = mg->p.beta;
-    a.omega = mg->p.omega;
-    a.diagB = 6.0 * mg->p.beta * L.hsqinv;
-    long long total = (long long)L.n * L.n * L.n;
+    Box3 b;
+    for (int d = 0; d < 3; d++) { b.lo[d] = -1; b.hi[d] = L.n; }
+    return b;
+}
+template <typename T>
+static Box3 valid_box(const MGLevel<T>& L)
+{
+    Box3 b;
+    for (int d = 0; d < 3; d++) { b.lo[d] = 0; b.hi[d] = L.n - 1; }
+    return b;
+}
+// 7-point coefficients times s (the reference's Stencil * scale: coefficient*s unless s == 1)
+template <typename T>
+static Coefs<T> lap7_coefs(double s)
+{
+    Coefs<T> cf;
+    for (int j = 0; j < 13; j++) cf.c[j] = T(0);
+    for (int j = 0; j < 7; j++) {
+        const double c = (j == 0) ? -6.0 : 1.0;
+        cf.c[j] = (T)((s != 1.0) ? c * s : c);
+    }
+    return cf;
+}
+template <typename T>
+static RelaxCoef<T> relax_coef(const pb_mg* mg, const MGLevel<T>& L)
+{
+    RelaxCoef<T> k;
+    k.n = L.n;
+    k.helm = is_helm(mg);
+    k.neg_lambda = (T)(-lambda_of(mg->p, L.h));
+    k.beta = (T)mg->p.beta;
+    k.omega = (T)mg->p.omega;
+    k.diagB = (T)(6.0 * mg->p.beta * L.hsqinv);
+    return k;
+}
+// rho (and alpha for the Helmholtz form) of a level as the star kernels' auxiliary fields
+template <typename T>
+static AuxSpecs level_aux(const pb_mg* mg, const T* rhs, const T* alpha, const MGLevel<T>& L)
+{
+    AuxSpecs a = no_aux();
+    const Box3 vb = valid_box(L);
+    a.n = is_helm(mg) ? 2 : 1;
+    a.in_smem = 1;
+    a.a[0] = aux_spec(rhs, vb, vb, (int)sizeof(T));
+    if (is_helm(mg)) a.a[1] = aux_spec(alpha, vb, vb, (int)sizeof(T));
+    return a;
+}
+
+template <typename T>
+static int launch_relax(pb_mg* mg, MGLevel<T>& L, bool first, cudaStream_t st)
+{
+    const RelaxCoef<T> k = relax_coef(mg, L);
     if (first) {
-        k_relax_first<double><<<grid_for(total, 256), 256, 0, st>>>(a);
+        const long long total = (long long)L.n * L.n * L.n;
+        k_relax_first<T><<<grid_for(total, 256), 256, 0, st>>>(L.rhs, L.alpha, L.phi[1 - L.cur], k);
         PB_LAUNCH_CHECK();
     } else {
-        Coefs<double> cf;
-        double w = mg->p.omega / 6.0;
-        double s = a.helm ? L.hsqinv : w;
-        for (int j = 0; j < 7; j++) {
-            double c = (j == 0) ? -6.0 : 1.0;
-            cf.c[j] = (s != 1.0) ? c * s : c;
-        }
-        EpiRelax<double> epi;
-        epi.a = a;
-        Box3 sb, ib;
-        for (int d = 0; d < 3; d++) { sb.lo[d] = -1; sb.hi[d] = L.n; ib.lo[d] = 0; ib.hi[d] = L.n - 1; }
-        int e = launch_star<ShapeLap7>(L.phi[L.cur], sb, ib, cf, epi, st, default_star_tune());
+        EpiRelax<T> epi;
+        epi.out = L.phi[1 - L.cur];
+        epi.k = k;
+        const double s = is_helm(mg) ? L.hsqinv : mg->p.omega / 6.0;
+        int e = launch_star<ShapeLap7>(L.phi[L.cur], grown_box(L), valid_box(L), lap7_coefs<T>(s), epi, st,
+                                       default_star_tune(), level_aux(mg, L.rhs, L.alpha, L));
         if (e != PB_OK) return e;
     }
     L.cur = 1 - L.cur;
     return PB_OK;
 }
 
-static int launch_resnorm(pb_mg* mg, int l, cudaStream_t st)
+// last FP32 post-sweep of the finest level fused with u64 += e
+static int launch_relax_update(pb_mg* mg, MGLevel<float>& L, cudaStream_t st)
 {
-    MGLevel& L = mg->lv[l];
-    PB_CUDA(cudaMemsetAsync(mg->d_res, 0, sizeof(double), st));
-    EpiResnorm<double> epi;
-    epi.a.rhs = L.rhs;
-    epi.a.alpha = L.alpha;
-    epi.a.out = nullptr;
-    epi.a.n = L.n;
-    epi.a.helm = mg->p.form == PB_MG_HELMHOLTZ;
-    epi.a.beta = mg->p.beta;
-    epi.result = mg->d_res;
-    epi.m = 0.0;
-    Coefs<double> cf;
-    for (int j = 0; j < 7; j++) {
-        double c = (j == 0) ? -6.0 : 1.0;
-        cf.c[j] = (L.hsqinv != 1.0) ? c * L.hsqinv : c;
-    }
-    Box3 sb, ib;
-    for (int d = 0; d < 3; d++) { sb.lo[d] = -1; sb.hi[d] = L.n; ib.lo[d] = 0; ib.hi[d] = L.n - 1; }
-    return launch_star<ShapeLap7>(L.phi[L.cur], sb, ib, cf, epi, st, default_star_tune());
+    EpiRelaxUpdate epi;
+    epi.u = mg->u64;
+    epi.k = relax_coef(mg, L);
+    const double s = is_helm(mg) ? L.hsqinv : mg->p.omega / 6.0;
+    return launch_star<ShapeLap7>(L.phi[L.cur], grown_box(L), valid_box(L), lap7_coefs<float>(s), epi, st,
+                                  default_star_tune(), level_aux(mg, L.rhs, L.alpha, L));
 }
 
-static int relax_sweeps(pb_mg* mg, int l, int k, bool zero_start, cudaStream_t st)
+static int launch_resnorm(pb_mg* mg, MGLevel<double>& L, cudaStream_t st)
+{
+    PB_CUDA(cudaMemsetAsync(mg->d_res, 0, sizeof(double), st));
+    EpiResnorm<double> epi;
+    epi.helm = is_helm(mg);
+    epi.beta = mg->p.beta;
+    epi.result = mg->d_res;
+    epi.m = 0.0;
+    return launch_star<ShapeLap7>(L.phi[L.cur], grown_box(L), valid_box(L), lap7_coefs<double>(L.hsqinv), epi, st,
+                                  default_star_tune(), level_aux(mg, L.rhs, L.alpha, L));
+}
+
+// MIXED: FP64 residual of u64 + norm + FP32 right-hand side + first FP32 sweep of the finest level
+static int launch_res64(pb_mg* mg, cudaStream_t st)
+{
+    MGLevel<float>& L = mg->lv32.back();
+    PB_CUDA(cudaMemsetAsync(mg->d_res, 0, sizeof(double), st));
+    EpiRes64 epi;
+    epi.e32 = L.phi[1];
+    epi.rhs32 = L.rhs;
+    epi.helm = is_helm(mg);
+    epi.beta = mg->p.beta;
+    epi.k = relax_coef(mg, L);
+    epi.result = mg->d_res;
+    epi.m = 0.0;
+    MGLevel<double> G;
+    G.n = L.n;
+    G.h = L.h;
+    G.hsqinv = L.hsqinv;
+    const double s = is_helm(mg) ? L.hsqinv : -L.hsqinv;
+    int e = launch_star<ShapeLap7>((const double*)mg->u64, grown_box(G), valid_box(G), lap7_coefs<double>(s), epi, st,
+                                   default_star_tune(), level_aux(mg, (const double*)mg->f64, (const double*)mg->alpha64, G));
+    L.cur = 1;
+    return e;
+}
+
+template <typename T>
+static int relax_sweeps(pb_mg* mg, MGLevel<T>& L, int k, bool zero_start, cudaStream_t st)
 {
     for (int s = 0; s < k; s++) {
-        int e = launch_relax(mg, l, zero_start && s == 0, st);
+        int e = launch_relax(mg, L, zero_start && s == 0, st);
         if (e != PB_OK) return e;
     }
-    if (zero_start && k == 0) {
-        MGLevel& L = mg->lv[l];
-        PB_CUDA(cudaMemsetAsync(L.phi[L.cur], 0, sizeof(double) * (size_t)(L.n + 2) * (L.n + 2) * (L.n + 2), st));
-    }
+    if (zero_start && k == 0) PB_CUDA(cudaMemsetAsync(L.phi[L.cur], 0, sizeof(T) * (size_t)(L.n + 2) * (L.n + 2) * (L.n + 2), st));
     return PB_OK;
 }
 
-static int vcycle(pb_mg* mg, int l, bool zero_start, cudaStream_t st)
+template <typename T>
+static const T* bottom_inverse(const pb_mg* mg);
+template <>
+const double* bottom_inverse<double>(const pb_mg* mg) { return mg->ainv64; }
+template <>
+const float* bottom_inverse<float>(const pb_mg* mg) { return mg->ainv32; }
+
+// V-cycle on level l of hierarchy lv. pre_done: the first pre-smoothing sweep already ran (the
+// mixed-precision residual pass does it); fuse_update: the last post-smoothing sweep adds its
+// result to the FP64 solution instead of storing it.
+template <typename T>
+static int vcycle(pb_mg* mg, std::vector<MGLevel<T>>& lv, int l, bool zero_start, int pre_done, bool fuse_update,
+                  cudaStream_t st)
 {
-    MGLevel& L = mg->lv[l];
+    MGLevel<T>& L = lv[l];
     if (zero_start) L.cur = 0;
     int e;
     if (l > 0) {
-        MGLevel& C = mg->lv[l - 1];
-        if ((e = relax_sweeps(mg, l, mg->p.nu1, zero_start, st)) != PB_OK) return e;
-        Coefs<double> cf;
-        bool helm = mg->p.form == PB_MG_HELMHOLTZ;
-        double s = helm ? L.hsqinv : -L.hsqinv;
-        for (int j = 0; j < 7; j++) {
-            double c = (j == 0) ? -6.0 : 1.0;
-            cf.c[j] = (s != 1.0) ? c * s : c;
-        }
-        long long nc3 = (long long)C.n * C.n * C.n;
-        k_resid_restrict<double><<<grid_for(nc3, 256), 256, 0, st>>>(L.phi[L.cur], L.rhs, L.alpha, C.rhs, L.n, helm, cf,
-                                                                     mg->p.beta);
+        MGLevel<T>& C = lv[l - 1];
+        if ((e = relax_sweeps(mg, L, mg->p.nu1 - pre_done, zero_start && !pre_done, st)) != PB_OK) return e;
+        const double s = is_helm(mg) ? L.hsqinv : -L.hsqinv;
+        const long long nc3 = (long long)C.n * C.n * C.n;
+        k_resid_restrict<T><<<grid_for(nc3, 256), 256, 0, st>>>(L.phi[L.cur], L.rhs, L.alpha, C.rhs, L.n, is_helm(mg),
+                                                                lap7_coefs<T>(s), (T)mg->p.beta);
         PB_LAUNCH_CHECK();
-        if ((e = vcycle(mg, l - 1, true, st)) != PB_OK) return e;
-        long long n3 = (long long)L.n * L.n * L.n;
-        k_prolong<double><<<grid_for(n3, 256), 256, 0, st>>>(L.phi[L.cur], C.phi[C.cur], L.n);
+        if ((e = vcycle(mg, lv, l - 1, true, 0, false, st)) != PB_OK) return e;
+        const long long n3 = (long long)L.n * L.n * L.n;
+        k_prolong<T><<<grid_for(n3, 256), 256, 0, st>>>(L.phi[L.cur], C.phi[C.cur], L.n);
         PB_LAUNCH_CHECK();
-        return relax_sweeps(mg, l, mg->p.nu2, false, st);
+        if (!fuse_update) return relax_sweeps(mg, L, mg->p.nu2, false, st);
+        if ((e = relax_sweeps(mg, L, mg->p.nu2 - 1, false, st)) != PB_OK) return e;
+        if constexpr (std::is_same<T, float>::value) return launch_relax_update(mg, L, st);
+        return PB_ERR_ARG;
     }
-    return relax_sweeps(mg, l, mg->p.nu_bottom, zero_start, st);
+    if (mg->p.bottom == PB_MG_BOTTOM_DIRECT) {
+        const int N = L.n * L.n * L.n;
+        k_bottom_direct<T><<<(N + 255) / 256, 256, 0, st>>>(bottom_inverse<T>(mg), L.rhs, L.phi[0], L.n);
+        PB_LAUNCH_CHECK();
+        L.cur = 0;
+        return PB_OK;
+    }
+    return relax_sweeps(mg, L, mg->p.nu_bottom, zero_start, st);
 }
 
-static int mg_free(pb_mg* mg)
+template <typename T>
+static void free_levels(std::vector<MGLevel<T>>& lv)
 {
-    for (auto& L : mg->lv) {
+    for (auto& L : lv) {
         cudaFree(L.phi[0]);
         cudaFree(L.phi[1]);
         cudaFree(L.alpha);
         cudaFree(L.rhs);
     }
+    lv.clear();
+}
+
+static int mg_free(pb_mg* mg)
+{
+    free_levels(mg->lv);
+    free_levels(mg->lv32);
     for (int k = 0; k < 2; k++)
         if (mg->graph[k]) cudaGraphExecDestroy(mg->graph[k]);
     if (mg->graph_stream) cudaStreamDestroy(mg->graph_stream);
+    cudaFree(mg->u64);
+    cudaFree(mg->f64);
+    cudaFree(mg->alpha64);
+    cudaFree(mg->ainv64);
+    cudaFree(mg->ainv32);
     cudaFree(mg->d_res);
     cudaFreeHost(mg->h_res);
     delete mg;
@@ -384,10 +684,17 @@ static int mg_free(pb_mg* mg)
 // One V-cycle on the finest level followed by the residual norm into h_res.
 static int cycle_and_norm(pb_mg* mg, cudaStream_t st)
 {
-    int top = (int)mg->lv.size() - 1;
-    int e = vcycle(mg, top, false, st);
-    if (e != PB_OK) return e;
-    if ((e = launch_resnorm(mg, top, st)) != PB_OK) return e;
+    int e;
+    if (is_mixed(mg)) {
+        const int top = (int)mg->lv32.size() - 1;
+        mg->lv32[top].cur = 1;   // the residual pass left the first sweep in phi[1]
+        if ((e = vcycle(mg, mg->lv32, top, false, 1, true, st)) != PB_OK) return e;
+        if ((e = launch_res64(mg, st)) != PB_OK) return e;
+    } else {
+        const int top = (int)mg->lv.size() - 1;
+        if ((e = vcycle(mg, mg->lv, top, false, 0, false, st)) != PB_OK) return e;
+        if ((e = launch_resnorm(mg, mg->lv[top], st)) != PB_OK) return e;
+    }
     PB_CUDA(cudaMemcpyAsync(mg->h_res, mg->d_res, sizeof(double), cudaMemcpyDeviceToHost, st));
     return PB_OK;
 }
@@ -399,6 +706,63 @@ static int params_ok(const pb_mg_params* p)
     if (p->nu1 < 0 || p->nu2 < 0 || p->nu_bottom < 0 || p->max_iter < 0) return PB_ERR_ARG;
     if (p->form != PB_MG_POISSON && p->form != PB_MG_HELMHOLTZ) return PB_ERR_ARG;
     if (p->precision != PB_MG_FP64 && p->precision != PB_MG_MIXED) return PB_ERR_ARG;
+    if (p->bottom != PB_MG_BOTTOM_RELAX && p->bottom != PB_MG_BOTTOM_DIRECT) return PB_ERR_ARG;
+    const long long n0 = p->n >> p->levels;
+    if (p->bottom == PB_MG_BOTTOM_DIRECT && n0 * n0 * n0 > 512) return PB_ERR_ARG;
+    // the mixed cycle fuses its first pre-sweep and its last post-sweep of the finest grid
+    if (p->precision == PB_MG_MIXED && (p->nu1 < 1 || p->nu2 < 1 || p->levels < 1)) return PB_ERR_ARG;
+    return PB_OK;
+}
+
+template <typename T>
+static bool alloc_levels(const pb_mg_params* p, std::vector<MGLevel<T>>& lv)
+{
+    lv.resize(p->levels + 1);
+    for (int l = 0; l <= p->levels; l++) {
+        MGLevel<T>& L = lv[l];
+        L.n = p->n >> (p->levels - l);
+        L.h = (double)(1 << (p->levels - l)) / (double)p->n;
+        L.hsqinv = 1. / (L.h * L.h);
+        const size_t g = sizeof(T) * (size_t)(L.n + 2) * (L.n + 2) * (L.n + 2);
+        const size_t c = sizeof(T) * (size_t)L.n * L.n * L.n;
+        bool ok = cudaMalloc(&L.phi[0], g) == cudaSuccess && cudaMalloc(&L.phi[1], g) == cudaSuccess &&
+                  cudaMalloc(&L.rhs, c) == cudaSuccess;
+        if (ok && p->form == PB_MG_HELMHOLTZ) ok = cudaMalloc(&L.alpha, c) == cudaSuccess;
+        if (ok) ok = cudaMemset(L.phi[0], 0, g) == cudaSuccess && cudaMemset(L.phi[1], 0, g) == cudaSuccess;
+        if (!ok) return false;
+    }
+    return true;
+}
+
+// Builds the coarsest-level inverse from the coarsest alpha held on the device (Helmholtz form)
+// and uploads it in the solver's precision(s).
+static int setup_bottom(pb_mg* mg)
+{
+    if (mg->p.bottom != PB_MG_BOTTOM_DIRECT) return PB_OK;
+    const bool mixed = is_mixed(mg);
+    const int n0 = mixed ? mg->lv32[0].n : mg->lv[0].n;
+    const double h = mixed ? mg->lv32[0].h : mg->lv[0].h;
+    const int N = n0 * n0 * n0;
+    std::vector<double> alpha(N, 0.0);
+    if (is_helm(mg)) {
+        PB_CUDA(cudaDeviceSynchronize());
+        if (mixed) {
+            std::vector<float> a32(N);
+            PB_CUDA(cudaMemcpy(a32.data(), mg->lv32[0].alpha, sizeof(float) * N, cudaMemcpyDeviceToHost));
+            for (int i = 0; i < N; i++) alpha[i] = a32[i];
+        } else {
+            PB_CUDA(cudaMemcpy(alpha.data(), mg->lv[0].alpha, sizeof(double) * N, cudaMemcpyDeviceToHost));
+        }
+    }
+    std::vector<double> inv;
+    if (!coarse_inverse(n0, h, is_helm(mg), mg->p.beta, alpha.data(), inv)) return PB_ERR_ARG;
+    if (mixed) {
+        std::vector<float> inv32(inv.size());
+        for (size_t i = 0; i < inv.size(); i++) inv32[i] = (float)inv[i];
+        PB_CUDA(cudaMemcpy(mg->ainv32, inv32.data(), sizeof(float) * inv32.size(), cudaMemcpyHostToDevice));
+    } else {
+        PB_CUDA(cudaMemcpy(mg->ainv64, inv.data(), sizeof(double) * inv.size(), cudaMemcpyHostToDevice));
+    }
     return PB_OK;
 }
 
@@ -407,12 +771,22 @@ extern "C" {
 long long pb_mg_device_bytes(const pb_mg_params* p)
 {
     if (params_ok(p) != PB_OK) return -1;
+    const long long es = p->precision == PB_MG_MIXED ? 4 : 8;
     long long total = 0;
     for (int l = 0; l <= p->levels; l++) {
-        long long n = p->n >> (p->levels - l);
-        long long g = (n + 2) * (n + 2) * (n + 2);
-        total += 2 * g * 8 + n * n * n * 8;
+        const long long n = p->n >> (p->levels - l);
+        const long long g = (n + 2) * (n + 2) * (n + 2);
+        total += 2 * g * es + n * n * n * es;
+        if (p->form == PB_MG_HELMHOLTZ) total += n * n * n * es;
+    }
+    if (p->precision == PB_MG_MIXED) {
+        const long long n = p->n;
+        total += (n + 2) * (n + 2) * (n + 2) * 8 + n * n * n * 8;
         if (p->form == PB_MG_HELMHOLTZ) total += n * n * n * 8;
+    }
+    if (p->bottom == PB_MG_BOTTOM_DIRECT) {
+        const long long n0 = p->n >> p->levels, N = n0 * n0 * n0;
+        total += N * N * es;
     }
     return total + 256;
 }
@@ -422,33 +796,33 @@ int pb_mg_create(const pb_mg_params* p, pb_mg** out)
     int e = params_ok(p);
     if (e != PB_OK) return e;
     if (!out) return PB_ERR_ARG;
-    if (p->precision == PB_MG_MIXED) return PB_ERR_UNSUPPORTED;
     pb_mg* mg = new (std::nothrow) pb_mg;
     if (!mg) return PB_ERR_NOMEM;
     mg->p = *p;
     cudaGetDevice(&mg->device);
-    mg->lv.resize(p->levels + 1);
-    for (int l = 0; l <= p->levels; l++) {
-        MGLevel& L = mg->lv[l];
-        L.n = p->n >> (p->levels - l);
-        L.h = (double)(1 << (p->levels - l)) / (double)p->n;
-        L.hsqinv = 1. / (L.h * L.h);
-        size_t g = sizeof(double) * (size_t)(L.n + 2) * (L.n + 2) * (L.n + 2);
-        size_t c = sizeof(double) * (size_t)L.n * L.n * L.n;
-        bool ok = cudaMalloc(&L.phi[0], g) == cudaSuccess && cudaMalloc(&L.phi[1], g) == cudaSuccess &&
-                  cudaMalloc(&L.rhs, c) == cudaSuccess;
-        if (ok && p->form == PB_MG_HELMHOLTZ) ok = cudaMalloc(&L.alpha, c) == cudaSuccess;
-        if (ok) ok = cudaMemset(L.phi[0], 0, g) == cudaSuccess && cudaMemset(L.phi[1], 0, g) == cudaSuccess;
-        if (!ok) {
-            cudaGetLastError();
-            mg_free(mg);
-            return PB_ERR_NOMEM;
-        }
+    bool ok;
+    const long long n0 = p->n >> p->levels, N0 = n0 * n0 * n0;
+    if (p->precision == PB_MG_MIXED) {
+        const size_t n = (size_t)p->n;
+        ok = alloc_levels(p, mg->lv32) && cudaMalloc(&mg->u64, 8 * (n + 2) * (n + 2) * (n + 2)) == cudaSuccess &&
+             cudaMalloc(&mg->f64, 8 * n * n * n) == cudaSuccess &&
+             cudaMemset(mg->u64, 0, 8 * (n + 2) * (n + 2) * (n + 2)) == cudaSuccess;
+        if (ok && p->form == PB_MG_HELMHOLTZ) ok = cudaMalloc(&mg->alpha64, 8 * n * n * n) == cudaSuccess;
+        if (ok && p->bottom == PB_MG_BOTTOM_DIRECT) ok = cudaMalloc(&mg->ainv32, sizeof(float) * N0 * N0) == cudaSuccess;
+    } else {
+        ok = alloc_levels(p, mg->lv);
+        if (ok && p->bottom == PB_MG_BOTTOM_DIRECT) ok = cudaMalloc(&mg->ainv64, sizeof(double) * N0 * N0) == cudaSuccess;
     }
-    if (cudaMalloc(&mg->d_res, sizeof(double)) != cudaSuccess || cudaMallocHost(&mg->h_res, sizeof(double)) != cudaSuccess) {
+    if (ok) ok = cudaMalloc(&mg->d_res, sizeof(double)) == cudaSuccess && cudaMallocHost(&mg->h_res, sizeof(double)) == cudaSuccess;
+    if (!ok) {
         cudaGetLastError();
         mg_free(mg);
         return PB_ERR_NOMEM;
+    }
+    // Poisson form: the coarsest operator is known now; Helmholtz waits for alpha
+    if (!is_helm(mg) && (e = setup_bottom(mg)) != PB_OK) {
+        mg_free(mg);
+        return e;
     }
     *out = mg;
     return PB_OK;
@@ -463,15 +837,32 @@ int pb_mg_destroy(pb_mg* mg)
 int pb_mg_set_alpha(pb_mg* mg, const double* alpha, void* stream)
 {
     if (!mg || !alpha) return PB_ERR_ARG;
-    if (mg->p.form != PB_MG_HELMHOLTZ) return PB_ERR_ARG;
+    if (!is_helm(mg)) return PB_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
-    int top = (int)mg->lv.size() - 1;
-    MGLevel& T = mg->lv[top];
-    PB_CUDA(cudaMemcpyAsync(T.alpha, alpha, sizeof(double) * (size_t)T.n * T.n * T.n, cudaMemcpyDeviceToDevice, st));
-    for (int l = top; l > 0; l--) {
-        long long nc3 = (long long)mg->lv[l - 1].n * mg->lv[l - 1].n * mg->lv[l - 1].n;
-        k_avgdown_plain<double><<<grid_for(nc3, 256), 256, 0, st>>>(mg->lv[l].alpha, mg->lv[l - 1].alpha, mg->lv[l].n);
+    if (is_mixed(mg)) {
+        const int top = (int)mg->lv32.size() - 1;
+        const long long n3 = (long long)mg->p.n * mg->p.n * mg->p.n;
+        PB_CUDA(cudaMemcpyAsync(mg->alpha64, alpha, sizeof(double) * n3, cudaMemcpyDeviceToDevice, st));
+        k_to_float<<<grid_for(n3, 256), 256, 0, st>>>(mg->alpha64, mg->lv32[top].alpha, n3);
         PB_LAUNCH_CHECK();
+        for (int l = top; l > 0; l--) {
+            const long long nc3 = (long long)mg->lv32[l - 1].n * mg->lv32[l - 1].n * mg->lv32[l - 1].n;
+            k_avgdown_plain<float><<<grid_for(nc3, 256), 256, 0, st>>>(mg->lv32[l].alpha, mg->lv32[l - 1].alpha, mg->lv32[l].n);
+            PB_LAUNCH_CHECK();
+        }
+    } else {
+        const int top = (int)mg->lv.size() - 1;
+        MGLevel<double>& T = mg->lv[top];
+        PB_CUDA(cudaMemcpyAsync(T.alpha, alpha, sizeof(double) * (size_t)T.n * T.n * T.n, cudaMemcpyDeviceToDevice, st));
+        for (int l = top; l > 0; l--) {
+            const long long nc3 = (long long)mg->lv[l - 1].n * mg->lv[l - 1].n * mg->lv[l - 1].n;
+            k_avgdown_plain<double><<<grid_for(nc3, 256), 256, 0, st>>>(mg->lv[l].alpha, mg->lv[l - 1].alpha, mg->lv[l].n);
+            PB_LAUNCH_CHECK();
+        }
+    }
+    if (mg->p.bottom == PB_MG_BOTTOM_DIRECT) {
+        PB_CUDA(cudaStreamSynchronize(st));
+        return setup_bottom(mg);
     }
     return PB_OK;
 }
@@ -480,42 +871,56 @@ int pb_mg_solve(pb_mg* mg, const double* rhs, double* phi, int* iters, double* h
 {
     if (!mg || !rhs || !phi) return PB_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
-    int top = (int)mg->lv.size() - 1;
-    MGLevel& T = mg->lv[top];
-    const long long n3 = (long long)T.n * T.n * T.n;
-    PB_CUDA(cudaMemcpyAsync(T.rhs, rhs, sizeof(double) * n3, cudaMemcpyDeviceToDevice, st));
-    T.cur = 0;
-    k_pack_in<double><<<grid_for(n3, 256), 256, 0, st>>>(phi, T.phi[0], T.n);
-    PB_LAUNCH_CHECK();
-    int e = launch_resnorm(mg, top, st);
-    if (e != PB_OK) return e;
+    const bool mixed = is_mixed(mg);
+    const int n = mg->p.n;
+    const long long n3 = (long long)n * n * n;
+    int e;
+    MGLevel<double>* T = mixed ? nullptr : &mg->lv.back();
+    if (mixed) {
+        PB_CUDA(cudaMemcpyAsync(mg->f64, rhs, sizeof(double) * n3, cudaMemcpyDeviceToDevice, st));
+        k_pack_in<double><<<grid_for(n3, 256), 256, 0, st>>>(phi, mg->u64, n);
+        PB_LAUNCH_CHECK();
+        if ((e = launch_res64(mg, st)) != PB_OK) return e;
+    } else {
+        PB_CUDA(cudaMemcpyAsync(T->rhs, rhs, sizeof(double) * n3, cudaMemcpyDeviceToDevice, st));
+        T->cur = 0;
+        k_pack_in<double><<<grid_for(n3, 256), 256, 0, st>>>(phi, T->phi[0], n);
+        PB_LAUNCH_CHECK();
+        if ((e = launch_resnorm(mg, *T, st)) != PB_OK) return e;
+    }
     PB_CUDA(cudaMemcpyAsync(mg->h_res, mg->d_res, sizeof(double), cudaMemcpyDeviceToHost, st));
     PB_CUDA(cudaStreamSynchronize(st));
     const double r0 = *mg->h_res;
     if (hist) hist[0] = r0;
     int it = 0;
     while (it < mg->p.max_iter) {
-        // replay the captured V-cycle when one exists for this buffer parity; capture otherwise
-        int par = T.cur;
-        if (!mg->graph[par] && it > 0) {
+        // Replay the captured cycle when one exists for this state; capture it otherwise. The FP64
+        // cycle flips the finest level's buffer nu1 + nu2 times, so it has one graph per parity;
+        // the mixed cycle always starts from the same buffers.
+        const int par = mixed ? 0 : T->cur;
+        if (!mg->graph[par] && (it > 0 || mixed)) {
             if (!mg->graph_stream) PB_CUDA(cudaStreamCreateWithFlags(&mg->graph_stream, cudaStreamNonBlocking));
             cudaGraph_t g;
             PB_CUDA(cudaStreamBeginCapture(mg->graph_stream, cudaStreamCaptureModeThreadLocal));
             e = cycle_and_norm(mg, mg->graph_stream);
             cudaError_t ce = cudaStreamEndCapture(mg->graph_stream, &g);
-            if (e != PB_OK) return e;
+            if (e != PB_OK) {
+                if (ce == cudaSuccess) cudaGraphDestroy(g);
+                return e;
+            }
             if (ce != cudaSuccess) { set_cuda_error(ce); return PB_ERR_CUDA; }
             ce = cudaGraphInstantiate(&mg->graph[par], g, 0);
             cudaGraphDestroy(g);
             if (ce != cudaSuccess) { set_cuda_error(ce); return PB_ERR_CUDA; }
-            T.cur = par;   // capture recorded the parity flips without running them
-            // reset the coarse levels' parity bookkeeping (they restart at zero every visit)
+            if (!mixed) {
+                // capture recorded the buffer flips without running them
+                mg->graph_cur[par] = T->cur;
+                T->cur = par;
+            }
         }
         if (mg->graph[par]) {
             PB_CUDA(cudaGraphLaunch(mg->graph[par], st));
-            // the graph flips the finest level's buffer (nu1 + nu2) times
-            if ((mg->p.nu1 + mg->p.nu2) & 1) T.cur = 1 - par;
-            else T.cur = par;
+            if (!mixed) T->cur = mg->graph_cur[par];
         } else {
             if ((e = cycle_and_norm(mg, st)) != PB_OK) return e;
         }
@@ -525,9 +930,11 @@ int pb_mg_solve(pb_mg* mg, const double* rhs, double* phi, int* iters, double* h
         if (hist) hist[it] = r;
         if (r < mg->p.tol * r0) break;
     }
-    k_pack_out<double><<<grid_for(n3, 256), 256, 0, st>>>(T.phi[T.cur], phi, T.n);
+    const double* src = mixed ? mg->u64 : T->phi[T->cur];
+    k_pack_out<double><<<grid_for(n3, 256), 256, 0, st>>>(src, phi, n);
     PB_LAUNCH_CHECK();
     PB_CUDA(cudaStreamSynchronize(st));
+    if (read_error_mg() > 0 || read_error_stencil() > 0) return PB_ERR_DEVICE;
     if (iters) *iters = it;
     return PB_OK;
 }
@@ -535,15 +942,19 @@ int pb_mg_solve(pb_mg* mg, const double* rhs, double* phi, int* iters, double* h
 int pb_mg_relax(pb_mg* mg, int sweeps, void* stream)
 {
     if (!mg || sweeps < 0) return PB_ERR_ARG;
-    int top = (int)mg->lv.size() - 1;
-    return relax_sweeps(mg, top, sweeps, false, (cudaStream_t)stream);
+    if (is_mixed(mg)) return relax_sweeps(mg, mg->lv32.back(), sweeps, false, (cudaStream_t)stream);
+    return relax_sweeps(mg, mg->lv.back(), sweeps, false, (cudaStream_t)stream);
 }
 
 int pb_mg_launches_per_cycle(const pb_mg_params* p)
 {
     if (params_ok(p) != PB_OK) return -1;
-    // levels top..1: nu1 + nu2 sweeps, one restriction, one prolongation; bottom sweeps; one norm
-    return p->levels * (p->nu1 + p->nu2 + 2) + p->nu_bottom + 1;
+    // levels top..1: nu1 + nu2 sweeps, one restriction, one prolongation; the bottom solve; one norm
+    // (mixed: the first pre-sweep and the last post-sweep fuse into the residual and update passes,
+    // and the residual pass replaces the norm)
+    const int bottom = p->bottom == PB_MG_BOTTOM_DIRECT ? 1 : p->nu_bottom;
+    if (p->precision == PB_MG_MIXED) return p->levels * (p->nu1 + p->nu2 + 2) - 1 + bottom + 1;
+    return p->levels * (p->nu1 + p->nu2 + 2) + bottom + 1;
 }
 
 } // extern "C"

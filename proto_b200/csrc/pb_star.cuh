@@ -1,11 +1,12 @@
 // Star-shaped stencil kernels (terms only on the axes, |offset| <= R) for sm_100a.
 //
 // Two kernels share the same epilogue interface:
-//   k_star_tma    : TMA-staged z-streaming. A CTA owns a 64 x TY column of output points and a
-//                   chunk of z; planes of the source tile (with an R-wide halo in x and y) arrive
-//                   in shared memory through cp.async.bulk.tensor into an NST-deep ring guarded by
-//                   mbarriers, z-neighbours live in a (2R+1)-register window per thread, x/y
-//                   neighbours are read from the centre plane in shared memory.
+//   k_star_tma    : TMA-staged z-streaming, warp specialised. A CTA owns a 64 x TY column of output
+//                   points and a chunk of z. One producer warp brings planes of the source tile
+//                   (with an R-wide halo in x and y) into shared memory with cp.async.bulk.tensor,
+//                   through an NST-deep ring of full/empty mbarriers; consumer warps keep the z
+//                   neighbours of YB rows in a (2R+1)-deep register window and read x/y neighbours
+//                   from the centre plane in shared memory.
 //   k_star_simple : one thread per point, read-only cached global loads (small boxes, and any
 //                   box the TMA alignment rules exclude).
 //
@@ -49,8 +50,9 @@ struct StarGeom {
     int nx, ny, nz;
     int ox, oy, oz;
     int Sx, Sy, Sz;
-    int zc;     // z chunk per CTA (TMA kernel)
-    int pad;    // TMA kernel: smem x offset of the halo start
+    int zc;     // TMA kernel: z extent per CTA
+    int pad;    // TMA kernel: shared-memory x offset of the halo start (16-byte alignment)
+    int nst;    // TMA kernel: stages in the ring (>= 2R+1, <= 16)
 };
 
 constexpr int kStarTX = 64;
@@ -63,6 +65,17 @@ struct StarSmem {
     static constexpr int PLANE_TX = BX * BY * (int)sizeof(T);       // bytes one TMA box delivers
     static constexpr int PLANE = (PLANE_TX + 127) / 128 * 128;
 };
+
+// Warp-wide max of a non-negative value followed by one atomic per warp (the warp-specialised
+// kernel's consumer warps finish independently).
+__device__ inline void warp_max_atomic(double v, double* result)
+{
+    for (int o = 16; o > 0; o >>= 1) {
+        double w = __shfl_down_sync(0xffffffffu, v, o);
+        v = (v < w) ? w : v;
+    }
+    if ((threadIdx.x & 31) == 0 && v > 0.0) atomic_max_nonneg(result, v);
+}
 
 // Block-wide max of a non-negative value followed by one atomic per CTA (deterministic: max is
 // order independent). Every thread of the block must call it.
@@ -89,120 +102,215 @@ __device__ inline void block_max_atomic(double v, double* result)
     }
 }
 
-template <class S, typename T, int TY, int NST, class Epi>
-__global__ void __launch_bounds__(kStarTX * TY)
-    k_star_tma(const __grid_constant__ CUtensorMap tmap, const StarGeom g, const Coefs<T> cf, const Epi epi_in)
+// Auxiliary per-point fields an epilogue reads (e.g. the right-hand side of a relaxation): up to
+// two, each a field with its own element size and box. In the TMA kernel they travel through the
+// same pipeline as the source planes (one 64 x TY tile per output plane) or are read from global
+// memory; in the simple kernel they are read from global memory.
+struct AuxSpec {
+    const void* base;
+    int esize;                 // 8 or 4 bytes
+    int Sx, Sy, Sz;            // extents of the field
+    int ox, oy, oz;            // field-local coordinates of index point (0,0,0)
+};
+struct AuxSpecs {
+    int n;
+    int in_smem;               // TMA kernel: 1 stages the tiles through shared memory, 0 reads global memory
+    AuxSpec a[2];
+};
+// What an epilogue sees: per auxiliary field, the address of this point's value.
+struct AuxCtx {
+    const void* p[2];
+    template <typename A>
+    __device__ __forceinline__ A get(int k) const { return *reinterpret_cast<const A*>(p[k]); }
+};
+
+template <int TY>
+struct AuxTile {
+    static constexpr int width(int esize) { return esize == 8 ? kStarTX + 2 : kStarTX + 4; }   // room for a 16-byte pad
+    static constexpr int bytes(int esize) { return ((width(esize) * TY * esize) + 127) / 128 * 128; }
+};
+
+// Warp-specialised TMA z-streaming star kernel. Threads: 64 x (TY/YB) consumers, each computing YB
+// rows of one x column, plus one producer warp that issues the TMA copies. Stage s of the NST-deep
+// ring holds source plane q (q % NST == s) and, when q - R is an output plane, the auxiliary tiles
+// of that plane; full[s] completes when its bytes land, empty[s] when every consumer warp is done
+// with it. Epilogues see one row at a time through a cursor set up once per row (Epi::Row). Waits
+// are bounded; on expiry the kernel flags DEV_WAIT_TIMEOUT and leaves.
+template <class S, typename T, int TY, int YB, class Epi>
+__global__ void __launch_bounds__(kStarTX * (TY / YB) + 32, (kStarTX * (TY / YB) + 32) <= 288 ? 3 : 2)
+    k_star_tma(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CUtensorMap amap0,
+               const __grid_constant__ CUtensorMap amap1, const StarGeom g, const AuxSpecs aux, const Coefs<T> cf,
+               const Epi epi_in)
 {
     using SM = StarSmem<S, T, TY>;
     constexpr int R = S::R;
-    static_assert(NST >= 2 * R + 1, "ring must hold the whole z window");
+    constexpr int NCW = kStarTX * (TY / YB) / 32;     // consumer warps
+    static_assert(TY % YB == 0, "rows per thread must divide the tile");
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + NST * SM::PLANE);
-    __shared__ int s_abort;
-    __shared__ int s_issued;     // planes whose TMA copy has been issued (written by thread 0)
+    const int NST = g.nst;                            // the launcher checks 2R+1 <= NST <= 16
+    const bool aux_sm = aux.in_smem != 0;
+    const int aux_b0 = (aux_sm && aux.n > 0) ? AuxTile<TY>::bytes(aux.a[0].esize) : 0;
+    const int aux_b1 = (aux_sm && aux.n > 1) ? AuxTile<TY>::bytes(aux.a[1].esize) : 0;
+    const int stage = SM::PLANE + aux_b0 + aux_b1;
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + NST * stage);
+    uint64_t* empty = full + NST;
 
-    Epi epi = epi_in;
-    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kStarTX + tx;
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
     const int x0 = blockIdx.x * kStarTX, y0 = blockIdx.y * TY;
     const int zb = blockIdx.z * g.zc;
     const int nzl = min(g.zc, g.nz - zb);
     if (nzl <= 0) return;
     const int nplanes = nzl + 2 * R;
-    const int xs = g.ox + x0 - R - g.pad;            // 16-byte aligned element coordinate
-    const int ys = g.oy + y0 - R;
-    const int zs0 = g.oz + zb - R;
-    const int x = x0 + tx, y = y0 + ty;
-    const bool active = (x < g.nx) && (y < g.ny);
-    const int sc = (ty + R) * SM::BX + (tx + R + g.pad);   // centre element inside a plane
 
     if (tid == 0) {
-        s_abort = 0;
-        for (int s = 0; s < NST; s++) mbar_init(&bars[s], 1);
+        for (int s = 0; s < NST; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], NCW);
+        }
         fence_barrier_init();
     }
     __syncthreads();
-    if (tid == 0) {
-        int np = nplanes < NST ? nplanes : NST;
-        for (int q = 0; q < np; q++) {
-            mbar_arrive_expect_tx(&bars[q], SM::PLANE_TX);
-            tma_load_3d(smem_raw + q * SM::PLANE, &tmap, &bars[q], xs, ys, zs0 + q);
-        }
-        s_issued = np;
-    }
-    int qpending = 0;   // first plane not yet consumed
-    auto plane = [&](int q) -> const T* { return reinterpret_cast<const T*>(smem_raw + (q % NST) * SM::PLANE); };
 
-    T win[2 * R + 1];
+    if (warp == NCW) {
+        // ---- producer warp ----
+        if (lane == 0) {
+            const int xs = g.ox + x0 - R - g.pad, ys = g.oy + y0 - R, zs0 = g.oz + zb - R;
+            int s = 0;
+            uint32_t eph = 0;   // parity bits of the next empty-wait per slot
+            int issued = 0;
+            for (int q = 0; q < nplanes; q++) {
+                if (q >= NST) {
+                    if (!mbar_wait(&empty[s], (eph >> s) & 1)) break;
+                    eph ^= 1u << s;
+                }
+                unsigned char* st = smem_raw + s * stage;
+                const int zo = q - R;
+                const bool with_aux = aux_sm && aux.n > 0 && zo >= 0 && zo < nzl;
+                uint32_t bytes = SM::PLANE_TX;
+                if (with_aux) {
+                    bytes += AuxTile<TY>::width(aux.a[0].esize) * TY * aux.a[0].esize;
+                    if (aux.n > 1) bytes += AuxTile<TY>::width(aux.a[1].esize) * TY * aux.a[1].esize;
+                }
+                mbar_arrive_expect_tx(&full[s], bytes);
+                tma_load_3d(st, &tmap, &full[s], xs, ys, zs0 + q);
+                if (with_aux) {
+                    const AuxSpec& a0 = aux.a[0];
+                    tma_load_3d(st + SM::PLANE, &amap0, &full[s], a0.ox + x0 - (a0.ox % (16 / a0.esize)), a0.oy + y0,
+                                a0.oz + zb + zo);
+                    if (aux.n > 1) {
+                        const AuxSpec& a1 = aux.a[1];
+                        tma_load_3d(st + SM::PLANE + aux_b0, &amap1, &full[s], a1.ox + x0 - (a1.ox % (16 / a1.esize)),
+                                    a1.oy + y0, a1.oz + zb + zo);
+                    }
+                }
+                if (++s == NST) s = 0;
+                issued = q + 1;
+            }
+            // Copies still in flight must land before the CTA's shared memory goes away (the consumers
+            // wait for every plane on a normal exit; this covers an exit after a timed-out wait).
+            for (int q = max(0, issued - NST); q < issued; q++) mbar_wait(&full[q % NST], (q / NST) & 1);
+        }
+        return;
+    }
+
+    // ---- consumer warps ----
+    Epi epi = epi_in;
+    const int tx = tid & (kStarTX - 1), ty = tid / kStarTX;
+    const int x = x0 + tx;
+    const int yr0 = ty * YB;                               // first tile row of this thread
+    const bool xin = x < g.nx;
+    const int sc0 = (yr0 + R) * SM::BX + (tx + R + g.pad); // centre element of the first row
+    // per-row epilogue state, computed once; auxiliary-field addresses of row r are
+    // base + abase + r * arow (shared-memory tile or global field)
+    typename Epi::Row rows[YB];
+#pragma unroll
+    for (int r = 0; r < YB; r++) {
+        const int y = y0 + yr0 + r;
+        rows[r] = epi.row(x, y, zb, xin && (y < g.ny));
+    }
+    long long abase0, abase1, astep0 = 0, astep1 = 0;
+    int arow0, arow1;
+    {
+        const AuxSpec& a0 = aux.a[0];
+        const AuxSpec& a1 = aux.a[1];
+        if (aux_sm) {
+            const int w0 = AuxTile<TY>::width(a0.esize), w1 = AuxTile<TY>::width(a1.esize);
+            abase0 = ((long long)yr0 * w0 + tx + a0.ox % (16 / a0.esize)) * a0.esize;
+            abase1 = ((long long)yr0 * w1 + tx + a1.ox % (16 / a1.esize)) * a1.esize;
+            arow0 = w0 * a0.esize;
+            arow1 = w1 * a1.esize;
+        } else {
+            const int y = y0 + yr0;
+            abase0 = ((x + a0.ox) + (long long)a0.Sx * ((y + a0.oy) + (long long)a0.Sy * (zb + a0.oz))) * a0.esize;
+            abase1 = ((x + a1.ox) + (long long)a1.Sx * ((y + a1.oy) + (long long)a1.Sy * (zb + a1.oz))) * a1.esize;
+            arow0 = a0.Sx * a0.esize;
+            arow1 = a1.Sx * a1.esize;
+            astep0 = (long long)a0.Sx * a0.Sy * a0.esize;
+            astep1 = (long long)a1.Sx * a1.Sy * a1.esize;
+        }
+    }
+    uint32_t fph = 0;                                      // parity bits of the next full-wait per slot
     bool ok = true;
+    T win[YB][2 * R + 1];
+    // window: planes 0 .. 2R-1
 #pragma unroll
     for (int q = 0; q < 2 * R; q++) {
-        ok &= mbar_wait(&bars[q % NST], (q / NST) & 1);
-        win[q] = plane(q)[sc];
-    }
-    if (!ok) s_abort = 1;
-    __syncthreads();
-    if (s_abort) goto drain;
-    qpending = 2 * R;
-    // planes 0..R-1 only fed the window: recycle their slots
-    if (tid == 0) {
-        for (int q = 0; q < R; q++) {
-            int nq = q + NST;
-            if (nq < nplanes) {
-                mbar_arrive_expect_tx(&bars[nq % NST], SM::PLANE_TX);
-                tma_load_3d(smem_raw + (nq % NST) * SM::PLANE, &tmap, &bars[nq % NST], xs, ys, zs0 + nq);
-                s_issued = nq + 1;
-            }
-        }
-    }
-
-    for (int zo = 0; zo < nzl; zo++) {
-        const int qn = zo + 2 * R, qc = zo + R;
-        qpending = qn;
-        if (!mbar_wait(&bars[qn % NST], (qn / NST) & 1)) s_abort = 1;
-        win[2 * R] = plane(qn)[sc];
-        const T* pc = plane(qc);
-        const int z = zb + zo;
-        T acc = epi.init(x, y, z, active);
+        ok &= mbar_wait(&full[q], (fph >> q) & 1);
+        fph ^= 1u << q;
+        const T* pl = reinterpret_cast<const T*>(smem_raw + q * stage);
 #pragma unroll
-        for (int j = 0; j < S::NT; j++) {
-            const int ox = S::off(j, 0), oy = S::off(j, 1), oz = S::off(j, 2);
-            T v;
-            if (oz != 0) v = win[R + oz];
-            else if (ox == 0 && oy == 0) v = win[R];
-            else v = pc[sc + oy * SM::BX + ox];
-            acc = dadd(acc, dmul(cf.c[j], v));
-        }
-        if (active) epi.finish(x, y, z, acc, win[R]);
+        for (int r = 0; r < YB; r++) win[r][q] = pl[sc0 + r * SM::BX];
+    }
+    __syncwarp();
+    // planes 0 .. R-1 only fed the window
+    if (lane == 0)
+        for (int q = 0; q < R; q++) mbar_arrive(&empty[q]);
+    int sn = 2 * R % NST, scs = R % NST;                   // slots of the newest and the centre plane
+    ok = __all_sync(0xffffffffu, ok);
+    for (int zo = 0; zo < nzl && ok; zo++) {
+        ok = __all_sync(0xffffffffu, mbar_wait(&full[sn], (fph >> sn) & 1));
+        fph ^= 1u << sn;
+        const T* pn = reinterpret_cast<const T*>(smem_raw + sn * stage);
 #pragma unroll
-        for (int k = 0; k < 2 * R; k++) win[k] = win[k + 1];
-        __syncthreads();
-        if (s_abort) goto drain;
-        if (tid == 0) {
-            int nq = qc + NST;
-            if (nq < nplanes) {
-                mbar_arrive_expect_tx(&bars[nq % NST], SM::PLANE_TX);
-                tma_load_3d(smem_raw + (nq % NST) * SM::PLANE, &tmap, &bars[nq % NST], xs, ys, zs0 + nq);
-                s_issued = nq + 1;
+        for (int r = 0; r < YB; r++) win[r][2 * R] = pn[sc0 + r * SM::BX];
+        const unsigned char* stc = smem_raw + scs * stage;
+        const T* pc = reinterpret_cast<const T*>(stc);
+        const unsigned char* ab0 = (aux_sm ? stc + SM::PLANE : reinterpret_cast<const unsigned char*>(aux.a[0].base) + zo * astep0) + abase0;
+        const unsigned char* ab1 = (aux_sm ? stc + SM::PLANE + aux_b0 : reinterpret_cast<const unsigned char*>(aux.a[1].base) + zo * astep1) + abase1;
+#pragma unroll
+        for (int r = 0; r < YB; r++) {
+            AuxCtx ax;
+            ax.p[0] = ab0 + r * arow0;
+            ax.p[1] = ab1 + r * arow1;
+            T acc = epi.init(rows[r], zo, ax);
+#pragma unroll
+            for (int j = 0; j < S::NT; j++) {
+                const int ox = S::off(j, 0), oy = S::off(j, 1), oz = S::off(j, 2);
+                T v;
+                if (oz != 0) v = win[r][R + oz];
+                else if (ox == 0 && oy == 0) v = win[r][R];
+                else if (ox == 0 && r + oy >= 0 && r + oy < YB) v = win[r + oy][R];   // another row of this thread
+                else v = pc[sc0 + (r + oy) * SM::BX + ox];
+                acc = dadd(acc, dmul(cf.c[j], v));
             }
+            epi.finish(rows[r], zo, acc, win[r][R], ax);
         }
+#pragma unroll
+        for (int r = 0; r < YB; r++)
+#pragma unroll
+            for (int k = 0; k < 2 * R; k++) win[r][k] = win[r][k + 1];
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[scs]);
+        if (++sn == NST) sn = 0;
+        if (++scs == NST) scs = 0;
     }
-    epi.end();
-    return;
-
-drain:
-    // a wait expired: give the copies still in flight a bounded chance to land, then leave
-    if (tid == 0) {
-        for (int q = qpending; q < s_issued; q++) {
-            for (uint32_t i = 0; i < kMaxWaitTries; i++)
-                if (mbar_try_wait(&bars[q % NST], (q / NST) & 1)) break;
-        }
-    }
-    __syncthreads();
+    epi.end_warp();
 }
 
 template <class S, typename T, class Epi>
-__global__ void __launch_bounds__(256) k_star_simple(const T* __restrict__ src, const StarGeom g, const Coefs<T> cf,
-                                                     const Epi epi_in)
+__global__ void __launch_bounds__(256) k_star_simple(const T* __restrict__ src, const StarGeom g, const AuxSpecs aux,
+                                                     const Coefs<T> cf, const Epi epi_in)
 {
     Epi epi = epi_in;
     const long long total = (long long)g.nx * g.ny * g.nz;
@@ -214,15 +322,21 @@ __global__ void __launch_bounds__(256) k_star_simple(const T* __restrict__ src, 
         int y = (int)(r % g.ny);
         int z = (int)(r / g.ny);
         long long base = (x + g.ox) + Sx * (y + g.oy) + Sxy * (z + g.oz);
-        T acc = epi.init(x, y, z, true);
+        AuxCtx ax;
+        ax.p[0] = reinterpret_cast<const unsigned char*>(aux.a[0].base) +
+                  ((x + aux.a[0].ox) + (long long)aux.a[0].Sx * ((y + aux.a[0].oy) + (long long)aux.a[0].Sy * (z + aux.a[0].oz))) * aux.a[0].esize;
+        ax.p[1] = reinterpret_cast<const unsigned char*>(aux.a[1].base) +
+                  ((x + aux.a[1].ox) + (long long)aux.a[1].Sx * ((y + aux.a[1].oy) + (long long)aux.a[1].Sy * (z + aux.a[1].oz))) * aux.a[1].esize;
+        const typename Epi::Row row = epi.row(x, y, z, true);
+        T acc = epi.init(row, 0, ax);
 #pragma unroll
         for (int j = 0; j < S::NT; j++) {
             const long long o = S::off(j, 0) + Sx * S::off(j, 1) + Sxy * S::off(j, 2);
             acc = dadd(acc, dmul(cf.c[j], __ldg(src + base + o)));
         }
-        epi.finish(x, y, z, acc, __ldg(src + base));
+        epi.finish(row, 0, acc, __ldg(src + base), ax);
     }
-    epi.end();
+    epi.end_block();
 }
 
 // ---- basic epilogues ---------------------------------------------------------------------------
@@ -232,18 +346,31 @@ struct OutMap {
     __device__ __forceinline__ long long at(int x, int y, int z) const { return (x + dx) + Dx * (y + dy) + Dxy * (z + dz); }
 };
 
+// Per-row output cursor: the row's address at its first z and whether the row is inside the box.
+template <typename T>
+struct OutRow {
+    T* p;
+    bool active;
+};
+
 // "dst |= S(src)" (init 0) and "dst += S(src)" (init = old dst value, then the terms)
 template <typename T>
 struct EpiStore {
     T* dst;
     OutMap m;
     int accumulate;
-    __device__ __forceinline__ T init(int x, int y, int z, bool active) const
+    using Row = OutRow<T>;
+    __device__ __forceinline__ Row row(int x, int y, int z0, bool active) const { return Row{dst + m.at(x, y, z0), active}; }
+    __device__ __forceinline__ T init(const Row& r, int zo, const AuxCtx&) const
     {
-        return (accumulate && active) ? dst[m.at(x, y, z)] : T(0);
+        return (accumulate && r.active) ? r.p[zo * m.Dxy] : T(0);
     }
-    __device__ __forceinline__ void finish(int x, int y, int z, T acc, T) const { dst[m.at(x, y, z)] = acc; }
-    __device__ __forceinline__ void end() const {}
+    __device__ __forceinline__ void finish(const Row& r, int zo, T acc, T, const AuxCtx&) const
+    {
+        if (r.active) r.p[zo * m.Dxy] = acc;
+    }
+    __device__ __forceinline__ void end_warp() const {}
+    __device__ __forceinline__ void end_block() const {}
 };
 
 // out = a*Lu + b*u  /  out = u + a*Lu
@@ -253,12 +380,15 @@ struct EpiAxpby {
     OutMap m;
     T a, b;
     int euler;
-    __device__ __forceinline__ T init(int, int, int, bool) const { return T(0); }
-    __device__ __forceinline__ void finish(int x, int y, int z, T acc, T u) const
+    using Row = OutRow<T>;
+    __device__ __forceinline__ Row row(int x, int y, int z0, bool active) const { return Row{dst + m.at(x, y, z0), active}; }
+    __device__ __forceinline__ T init(const Row&, int, const AuxCtx&) const { return T(0); }
+    __device__ __forceinline__ void finish(const Row& r, int zo, T acc, T u, const AuxCtx&) const
     {
-        dst[m.at(x, y, z)] = euler ? dadd(u, dmul(a, acc)) : dadd(dmul(a, acc), dmul(b, u));
+        if (r.active) r.p[zo * m.Dxy] = euler ? dadd(u, dmul(a, acc)) : dadd(dmul(a, acc), dmul(b, u));
     }
-    __device__ __forceinline__ void end() const {}
+    __device__ __forceinline__ void end_warp() const {}
+    __device__ __forceinline__ void end_block() const {}
 };
 
 } // namespace pb

@@ -171,15 +171,28 @@ StarTune& default_star_tune() { return g_default_tune; }
 } // namespace pb
 
 // Launch-shape knobs of the star kernels (used by the autotuner and by profiling sweeps):
-// mode 0 auto / 1 TMA only / 2 simple only; zc z-chunk (0 heuristic); ty CTA height (4, 8, 16).
-extern "C" int pb_star_tune_set(int mode, int zc, int ty, long long min_tma_points)
+// mode 0 auto / 1 TMA only / 2 simple only; zc z-chunk (0 heuristic); (ty, yb) CTA tile height and
+// rows per consumer thread.
+extern "C" int pb_star_tune_set(int mode, int zc, int ty, int yb, long long min_tma_points)
 {
-    if (mode < 0 || mode > 2 || zc < 0 || (ty != 4 && ty != 8 && ty != 16)) return PB_ERR_ARG;
+    const bool shape_ok = (ty == 4 && yb == 1) || (ty == 8 && (yb == 1 || yb == 2)) || (ty == 16 && yb == 4);
+    if (mode < 0 || mode > 2 || zc < 0 || !shape_ok) return PB_ERR_ARG;
     pb::StarTune& t = pb::default_star_tune();
     t.mode = mode;
     t.zc = zc;
     t.ty = ty;
+    t.yb = yb;
     if (min_tma_points >= 0) t.min_tma_points = min_tma_points;
+    return PB_OK;
+}
+
+extern "C" int pb_star_tune_ring(int nst, int aux_smem)
+{
+    if (nst != 0 && (nst < 3 || nst > 16)) return PB_ERR_ARG;
+    if (aux_smem != 0 && aux_smem != 1) return PB_ERR_ARG;
+    pb::StarTune& t = pb::default_star_tune();
+    t.nst = nst;
+    t.aux_smem = aux_smem;
     return PB_OK;
 }
 

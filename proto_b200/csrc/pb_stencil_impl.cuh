@@ -1,5 +1,7 @@
 // Internal declarations shared by the stencil and multigrid modules.
 #pragma once
+#include <cmath>
+#include <cstring>
 #include "pb_internal.cuh"
 #include "pb_star.cuh"
 
@@ -21,8 +23,11 @@ struct StarTune {
     enum Mode { AUTO = 0, TMA = 1, SIMPLE = 2 };
     int mode = AUTO;
     long long min_tma_points = 1 << 18;   // smaller boxes are launch/latency bound: simple kernel
-    int zc = 0;                          // z chunk per CTA; 0 = heuristic
-    int ty = 8;                          // CTA height (rows of 64 points): 4, 8 or 16
+    int zc = 0;                          // z chunk per CTA; 0 = occupancy-based heuristic
+    int ty = 8;                          // CTA tile height (rows of 64 points)
+    int yb = 2;                          // rows per consumer thread; (ty, yb) in {(4,1), (8,1), (8,2), (16,4)}
+    int nst = 0;                         // ring depth; 0 = 2R+4
+    int aux_smem = 1;                    // stage auxiliary fields through shared memory by TMA
 };
 StarTune& default_star_tune();
 int cached_sm_count();
@@ -30,44 +35,102 @@ int grid_for(long long total, int threads);
 // copies up to cap coefficients of a stencil (insertion order); returns the term count
 int stencil_coefs(const pb_stencil* s, double* c, int cap);
 
-// ---- star launch (shared with the multigrid module) -------------------------------------------
-// TMA z-streaming launch with a CTA of 64 x TY threads; zc = 0 picks about six CTAs per SM.
-template <class S, typename T, int TY, class Epi>
-int launch_star_tma(const T* src, StarGeom g, const Coefs<T>& cf, const Epi& epi, cudaStream_t st, int zc)
+inline AuxSpecs no_aux()
 {
+    AuxSpecs a{};
+    a.n = 0;
+    a.in_smem = 0;
+    return a;
+}
+// An auxiliary field of element size es stored on box fb, read at the points of index box ib.
+inline AuxSpec aux_spec(const void* base, const Box3& fb, const Box3& ib, int es)
+{
+    AuxSpec a{};
+    a.base = base;
+    a.esize = es;
+    a.Sx = (int)bsize(fb, 0);
+    a.Sy = (int)bsize(fb, 1);
+    a.Sz = (int)bsize(fb, 2);
+    a.ox = ib.lo[0] - fb.lo[0];
+    a.oy = ib.lo[1] - fb.lo[1];
+    a.oz = ib.lo[2] - fb.lo[2];
+    return a;
+}
+
+// ---- star launch (shared with the multigrid module) -------------------------------------------
+template <class S, typename T, int TY, int YB, class Epi>
+int launch_star_tma(const T* src, StarGeom g, const Coefs<T>& cf, const Epi& epi, cudaStream_t st, int zc,
+                    AuxSpecs aux, int nst)
+{
+    constexpr int R = S::R;
     constexpr int EV = 16 / (int)sizeof(T);
-    constexpr int NST = 2 * S::R + 4;
+    constexpr int NTHR = kStarTX * (TY / YB) + 32;
     using SM = StarSmem<S, T, TY>;
-    g.pad = (g.ox - S::R) % EV;
-    CUtensorMap map;
+    if (nst <= 0) nst = 2 * R + 4;
+    if (nst < 2 * R + 1 || nst > 16) return PB_ERR_ARG;
+    g.nst = nst;
+    g.pad = (g.ox - R) % EV;
+    CUtensorMap map, amap[2];
     int e = encode_tmap_3d(&map, src, (int)sizeof(T), g.Sx, g.Sy, g.Sz, SM::BX, SM::BY, 1);
     if (e != PB_OK) return e;
-    int tiles = ((g.nx + kStarTX - 1) / kStarTX) * ((g.ny + TY - 1) / TY);
+    memset(amap, 0, sizeof(amap));
+    int aux_bytes = 0;
+    if (aux.in_smem) {
+        // every auxiliary field must be TMA-addressable; otherwise read them all from global memory
+        for (int k = 0; k < aux.n && aux.in_smem; k++) {
+            const AuxSpec& a = aux.a[k];
+            if (a.ox < 0 || (a.esize != 4 && a.esize != 8) ||
+                encode_tmap_3d(&amap[k], a.base, a.esize, a.Sx, a.Sy, a.Sz, AuxTile<TY>::width(a.esize), TY, 1) != PB_OK)
+                aux.in_smem = 0;
+            else aux_bytes += AuxTile<TY>::bytes(a.esize);
+        }
+        if (!aux.in_smem) aux_bytes = 0;
+    }
+    const size_t smem = (size_t)nst * (SM::PLANE + aux_bytes) + 2 * nst * sizeof(uint64_t);
+    if (smem > 220 * 1024) return PB_ERR_ARG;
+    auto kern = k_star_tma<S, T, TY, YB, Epi>;
+    static int occ = 0;
+    static bool attr_set = false;
+    if (!attr_set) {
+        PB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+        PB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     (int)cudaSharedmemCarveoutMaxShared));
+        attr_set = true;
+    }
+    static size_t occ_smem = 0;
+    if (occ == 0 || occ_smem != smem) {
+        PB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, NTHR, smem));
+        if (occ < 1) occ = 1;
+        occ_smem = smem;
+    }
+    const long long tiles = (long long)((g.nx + kStarTX - 1) / kStarTX) * ((g.ny + TY - 1) / TY);
     if (zc <= 0) {
-        long long want = (long long)cached_sm_count() * (6 * 8 / TY);
-        zc = (int)(((long long)g.nz * tiles + want - 1) / want);
-        if (zc < 8) zc = 8;
-        zc = (zc + 7) / 8 * 8;
+        // Pick the z chunk that best balances whole waves against the 2R+1 planes of halo each
+        // CTA streams beyond its own: efficiency = (waves / ceil(waves)) * zc / (zc + 2R + 2).
+        const double slots = (double)cached_sm_count() * occ;
+        double best = -1.0;
+        zc = g.nz;
+        for (int c = 4; c <= g.nz; c += (c < 64 ? 2 : 8)) {
+            const long long blocks = tiles * ((g.nz + c - 1) / c);
+            const double waves = blocks / slots;
+            const double eff = (waves / std::ceil(waves)) * c / (double)(c + 2 * R + 2);
+            if (eff > best + 1e-9) {
+                best = eff;
+                zc = c;
+            }
+        }
     }
     if (zc > g.nz) zc = g.nz;
     g.zc = zc;
     dim3 grid((g.nx + kStarTX - 1) / kStarTX, (g.ny + TY - 1) / TY, (g.nz + zc - 1) / zc);
-    dim3 block(kStarTX, TY);
-    size_t smem = (size_t)NST * SM::PLANE + NST * sizeof(uint64_t);
-    auto kern = k_star_tma<S, T, TY, NST, Epi>;
-    static bool attr_set = false;
-    if (!attr_set) {
-        PB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr_set = true;
-    }
-    kern<<<grid, block, smem, st>>>(map, g, cf, epi);
+    kern<<<grid, NTHR, smem, st>>>(map, amap[0], amap[1], g, aux, cf, epi);
     PB_LAUNCH_CHECK();
     return PB_OK;
 }
 
 template <class S, typename T, class Epi>
 int launch_star(const T* src, const Box3& srcBox, const Box3& ib, const Coefs<T>& cf, const Epi& epi,
-                cudaStream_t st, const StarTune& tune)
+                cudaStream_t st, const StarTune& tune, AuxSpecs aux = no_aux())
 {
     StarGeom g;
     g.nx = (int)bsize(ib, 0);
@@ -81,22 +144,30 @@ int launch_star(const T* src, const Box3& srcBox, const Box3& ib, const Coefs<T>
     g.Sz = (int)bsize(srcBox, 2);
     g.zc = g.nz;
     g.pad = 0;
-    long long total = (long long)g.nx * g.ny * g.nz;
+    g.nst = 0;
+    // unused auxiliary slots point at something harmless (their addresses are formed, never read)
+    for (int k = aux.n; k < 2; k++) {
+        aux.a[k] = AuxSpec{};
+        aux.a[k].base = src;
+        aux.a[k].esize = (int)sizeof(T);
+    }
+    if (aux.n == 0) aux.in_smem = 0;
+    else aux.in_smem = aux.in_smem && tune.aux_smem;
+    const long long total = (long long)g.nx * g.ny * g.nz;
     bool use_tma = tune.mode != StarTune::SIMPLE && total >= tune.min_tma_points && g.ox >= S::R && tma_available();
-    if (tune.mode == StarTune::TMA) use_tma = use_tma || (g.ox >= S::R && tma_available());
+    if (tune.mode == StarTune::TMA) use_tma = g.ox >= S::R && tma_available();
     if (use_tma) {
-        int ty = tune.ty;
         int e;
-        if (ty == 4) e = launch_star_tma<S, T, 4>(src, g, cf, epi, st, tune.zc);
-        else if (ty == 16) e = launch_star_tma<S, T, 16>(src, g, cf, epi, st, tune.zc);
-        else e = launch_star_tma<S, T, 8>(src, g, cf, epi, st, tune.zc);
+        if (tune.ty == 4) e = launch_star_tma<S, T, 4, 1>(src, g, cf, epi, st, tune.zc, aux, tune.nst);
+        else if (tune.ty == 16) e = launch_star_tma<S, T, 16, 4>(src, g, cf, epi, st, tune.zc, aux, tune.nst);
+        else if (tune.yb == 1) e = launch_star_tma<S, T, 8, 1>(src, g, cf, epi, st, tune.zc, aux, tune.nst);
+        else e = launch_star_tma<S, T, 8, 2>(src, g, cf, epi, st, tune.zc, aux, tune.nst);
         if (e == PB_OK || tune.mode == StarTune::TMA) return e;
     }
-    int threads = 256;
-    k_star_simple<S, T, Epi><<<grid_for(total, threads), threads, 0, st>>>(src, g, cf, epi);
+    const int threads = 256;
+    k_star_simple<S, T, Epi><<<grid_for(total, threads), threads, 0, st>>>(src, g, aux, cf, epi);
     PB_LAUNCH_CHECK();
     return PB_OK;
 }
-
 
 } // namespace pb

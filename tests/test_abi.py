@@ -54,3 +54,42 @@ def test_argument_errors():
         pb.Multigrid(pb.MGParams(n=48, levels=5))
     assert pb.MGParams(n=48, levels=5).device_bytes() == -1
     assert pb.MGParams(n=256, levels=6).device_bytes() > 256 ** 3 * 8 * 3
+
+
+def test_launch_shape_knobs_validate():
+    L = pb.lib()
+    L.pb_star_tune_set.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_longlong]
+    assert L.pb_star_tune_set(0, 0, 8, 3, -1) == -1          # rows per thread must divide the tile
+    assert L.pb_star_tune_set(0, 0, 12, 1, -1) == -1
+    assert L.pb_star_tune_set(3, 0, 8, 2, -1) == -1
+    assert L.pb_star_tune_ring(2, 1) == -1                    # fewer planes than a 7-point window
+    assert L.pb_star_tune_ring(17, 1) == -1
+    assert L.pb_star_tune_ring(0, 2) == -1
+    for ty, yb in ((4, 1), (8, 1), (16, 4), (8, 2)):
+        assert L.pb_star_tune_set(0, 0, ty, yb, -1) == 0
+    assert L.pb_star_tune_ring(0, 1) == 0
+
+
+def test_multigrid_parameter_rules():
+    P = pb.MGParams
+    # exact bottom: at most 512 coarsest cells
+    assert P(n=256, levels=5, bottom=pb.MG_BOTTOM_DIRECT).device_bytes() > 0
+    assert P(n=256, levels=4, bottom=pb.MG_BOTTOM_DIRECT).device_bytes() == -1
+    assert P(n=64, levels=3, bottom=2).device_bytes() == -1
+    # mixed precision fuses a pre- and a post-sweep of the finest grid and needs a coarse grid
+    assert P(n=64, levels=3, precision=pb.MG_MIXED).device_bytes() > 0
+    assert P(n=64, levels=3, nu1=0, precision=pb.MG_MIXED).device_bytes() == -1
+    assert P(n=64, levels=3, nu2=0, precision=pb.MG_MIXED).device_bytes() == -1
+    assert P(n=64, levels=0, precision=pb.MG_MIXED).device_bytes() == -1
+    # mixed holds FP32 levels (two buffers + rhs: 12 B/cell) plus the FP64 solution and
+    # right-hand side (16 B/cell) against FP64's 24 B/cell
+    n = 256
+    b64 = P(n=n, levels=6).device_bytes()
+    bmx = P(n=n, levels=6, precision=pb.MG_MIXED).device_bytes()
+    assert b64 > 24 * n ** 3 and bmx > 28 * n ** 3
+    assert bmx - b64 < 6 * n ** 3
+    L = pb.lib()
+    lp = L.pb_mg_launches_per_cycle
+    assert lp(ctypes.byref(P(n=256, levels=6, nu1=4, nu2=4, nu_bottom=10).c)) == 6 * 10 + 10 + 1
+    assert lp(ctypes.byref(P(n=256, levels=5, nu1=4, nu2=4, bottom=1).c)) == 5 * 10 + 1 + 1
+    assert lp(ctypes.byref(P(n=256, levels=6, nu1=4, nu2=4, nu_bottom=10, precision=pb.MG_MIXED).c)) == 6 * 10 + 10

@@ -57,3 +57,80 @@ def test_large_grid_against_port(pb, port):
     n2, h2 = port.mg_cs(N, lev, 4, 4, 10, 2.0 / 3.0, 1.0, None, 6, 1e-10, rho.reshape(-1).copy(), p2)
     assert it == n2 and hist == list(h2)
     assert np.array_equal(phi, p2)
+
+
+def _gpu_solve(pb, N, levels, precision, nu=4, max_iter=60, tol=1e-10, alpha=None, rhs=None, nub=10, bottom=0):
+    import torch
+    p = pb.MGParams(n=N, levels=levels, nu1=nu, nu2=nu, nu_bottom=nub, omega=2.0 / 3.0, max_iter=max_iter, tol=tol,
+                    form=pb.MG_HELMHOLTZ if alpha is not None else pb.MG_POISSON, precision=precision,
+                    bottom=bottom)
+    mg = pb.Multigrid(p)
+    if alpha is not None:
+        mg.set_alpha(torch.from_numpy(alpha.reshape(-1).copy()).cuda())
+    rho = W.poisson_rho(N, seed=1) if rhs is None else rhs
+    r = torch.from_numpy(rho.reshape(-1).copy()).cuda()
+    phi = torch.zeros(N ** 3, dtype=torch.float64, device="cuda")
+    it, hist = mg.solve(r, phi)
+    pb.device_check()
+    return it, hist, phi.cpu().numpy()
+
+
+@pytest.mark.parametrize("N,levels", [(64, 4), (128, 5)])
+def test_mixed_precision_reaches_tolerance(pb, N, levels):
+    """FP32 V-cycles inside FP64 residual/correction: the FP64 residual reaches 1e-10 of its start
+    and the solution agrees with the FP64 solver's to the discretisation's conditioning."""
+    it64, h64, phi64 = _gpu_solve(pb, N, levels, pb.MG_FP64)
+    itm, hm, phim = _gpu_solve(pb, N, levels, pb.MG_MIXED)
+    assert hm[0] == h64[0]                      # same FP64 initial residual
+    assert hm[-1] < 1e-10 * hm[0]
+    assert itm <= it64 + 2
+    err = np.max(np.abs(phim - phi64)) / np.max(np.abs(phi64))
+    assert err < 1e-7
+
+
+def test_direct_bottom_helmholtz_bitwise(pb, port):
+    """Exact coarsest solve, Helmholtz form: history and solution bitwise vs the C port."""
+    N, lev = 64, 3
+    alpha = W.helmholtz_alpha(N, seed=3)
+    rhs = -W.poisson_rho(N, seed=1)
+    it, hist, phi = _gpu_solve(pb, N, lev, pb.MG_FP64, max_iter=20, alpha=alpha, rhs=rhs, bottom=1)
+    p2 = np.zeros(N ** 3)
+    n2, h2 = port.mg_cs(N, lev, 4, 4, 10, 2.0 / 3.0, 1.0, alpha.reshape(-1).copy(), 20, 1e-10,
+                        rhs.reshape(-1).copy(), p2, bottom=1)
+    assert it == n2 and hist == list(h2)
+    assert np.array_equal(phi, p2)
+    assert hist[-1] < 1e-10 * hist[0]
+
+
+def test_direct_bottom_poisson_bitwise(pb, port):
+    """Exact coarsest solve of the (regularised) periodic Poisson operator, 4^3 coarsest cells."""
+    N, lev = 32, 3
+    rho = W.poisson_rho(N, seed=1)
+    it, hist, phi = _gpu_solve(pb, N, lev, pb.MG_FP64, max_iter=20, bottom=1)
+    p2 = np.zeros(N ** 3)
+    n2, h2 = port.mg_cs(N, lev, 4, 4, 10, 2.0 / 3.0, 1.0, None, 20, 1e-10, rho.reshape(-1).copy(), p2, bottom=1)
+    assert it == n2 and hist == list(h2)
+    assert np.array_equal(phi, p2)
+
+
+def test_mixed_helmholtz_direct_bottom(pb):
+    N, lev = 64, 3
+    alpha = W.helmholtz_alpha(N, seed=3)
+    rhs = -W.poisson_rho(N, seed=1)
+    it64, h64, phi64 = _gpu_solve(pb, N, lev, pb.MG_FP64, alpha=alpha, rhs=rhs, bottom=1)
+    itm, hm, phim = _gpu_solve(pb, N, lev, pb.MG_MIXED, alpha=alpha, rhs=rhs, bottom=1)
+    assert hm[-1] < 1e-10 * hm[0]
+    assert itm <= it64 + 2
+    err = np.max(np.abs(phim - phi64)) / np.max(np.abs(phi64))
+    assert err < 1e-7
+
+
+def test_levels_zero_direct_is_exact(pb, port):
+    """A single grid with the exact bottom solve: one cycle, bitwise vs the C port."""
+    N = 8
+    rho = W.poisson_rho(N, seed=1)
+    it, hist, phi = _gpu_solve(pb, N, 0, pb.MG_FP64, max_iter=3, bottom=1)
+    p2 = np.zeros(N ** 3)
+    n2, h2 = port.mg_cs(N, 0, 4, 4, 10, 2.0 / 3.0, 1.0, None, 3, 1e-10, rho.reshape(-1).copy(), p2, bottom=1)
+    assert it == n2 and hist == list(h2)
+    assert np.array_equal(phi, p2)

@@ -30,13 +30,22 @@ namespace pb {
 
 PB_DEFINE_ERROR_READER(read_error_mg)
 
-// Writes v to the valid cell (x,y,z) of an (n+2)^3 grown periodic box and to every ghost cell
-// that is a periodic image of it. Out of line: only cells on the box boundary call it, and keeping
-// its index arrays out of the fused stencil kernels keeps their register count low.
+// A level is one periodic n^3 box held with a one-cell ghost layer: cell (x, y, z), -1 <= x,y,z <= n,
+// sits at (x+1) + sx*((y+1) + (n+2)*(z+1)). The x pitch sx >= n+2 is n+2 rounded up to 16 bytes,
+// so every row starts on a 16-byte boundary (a TMA requirement); columns past n+1 are padding.
 template <typename T>
-__device__ __noinline__ void store_periodic_images(T* out, int n, int x, int y, int z, T v)
+constexpr int grown_pitch(int n)
 {
-    const long long S = n + 2, S2 = S * S;
+    return (n + 2 + (16 / (int)sizeof(T)) - 1) / (16 / (int)sizeof(T)) * (16 / (int)sizeof(T));
+}
+
+// Writes v to the valid cell (x,y,z) and to every ghost cell that is a periodic image of it.
+// Out of line: only cells on the box boundary call it, and keeping its index arrays out of the
+// fused stencil kernels keeps their register count low.
+template <typename T>
+__device__ __noinline__ void store_periodic_images(T* out, int n, int sx, int x, int y, int z, T v)
+{
+    const long long Sy = sx, Sz = (long long)sx * (n + 2);
     int xs[3], ys[3], zs[3];
     int nx = 1, ny = 1, nz = 1;
     xs[0] = x + 1;
@@ -50,63 +59,120 @@ __device__ __noinline__ void store_periodic_images(T* out, int n, int x, int y, 
     if (z == n - 1) zs[nz++] = 0;
     for (int k = 0; k < nz; k++)
         for (int j = 0; j < ny; j++)
-            for (int i = 0; i < nx; i++) out[xs[i] + S * ys[j] + S2 * zs[k]] = v;
+            for (int i = 0; i < nx; i++) out[xs[i] + Sy * ys[j] + Sz * zs[k]] = v;
 }
 
 template <typename T>
-__device__ __forceinline__ void store_periodic(T* out, int n, int x, int y, int z, T v)
+__device__ __forceinline__ long long grown_index(int n, int sx, int x, int y, int z)
 {
-    const long long S = n + 2;
-    if (x == 0 || x == n - 1 || y == 0 || y == n - 1 || z == 0 || z == n - 1) store_periodic_images(out, n, x, y, z, v);
-    else out[(x + 1) + S * ((y + 1) + S * (long long)(z + 1))] = v;
+    return (x + 1) + (long long)sx * ((y + 1) + (long long)(n + 2) * (z + 1));
 }
 
-// Row cursor of a periodic (n+2)^3 output: the address of the row's valid cell at its first z, that
-// z, and flags (1: the row is inside the box, 2: it lies on an x or y face, so every cell of it has
-// ghost images).
+// Which periodic image of a coordinate exists: 0 none, 1 at +n (c == 0), 2 at -n (c == n-1).
+__device__ __forceinline__ int edge_code(int c, int n) { return c == 0 ? 1 : (c == n - 1 ? 2 : 0); }
+
+// Writes v at q (the valid cell) and at its periodic images, given the edge codes of x, y, z. The
+// images sit at constant offsets +-n, +-n*sx, +-n*sx*(n+2) from q, so this is a few predicated
+// stores. n == 1 (a cell that is both first and last) takes the general path.
+template <typename T>
+__device__ __forceinline__ void store_with_images(T* out, int n, int sx, T* q, int ex, int ey, int ez, T v)
+{
+    *q = v;
+    if ((ex | ey | ez) == 0) return;
+    if (n == 1) {
+        store_periodic_images(out, n, sx, 0, 0, 0, v);
+        return;
+    }
+    const long long ox = ex == 0 ? 0 : (ex == 1 ? n : -n);
+    const long long oy = ey == 0 ? 0 : (ey == 1 ? (long long)n * sx : -(long long)n * sx);
+    const long long sz = (long long)n * sx * (n + 2);
+    const long long oz = ez == 0 ? 0 : (ez == 1 ? sz : -sz);
+    if (ox) q[ox] = v;
+    if (oy) q[oy] = v;
+    if (ox && oy) q[ox + oy] = v;
+    if (oz) {
+        q[oz] = v;
+        if (ox) q[oz + ox] = v;
+        if (oy) q[oz + oy] = v;
+        if (ox && oy) q[oz + ox + oy] = v;
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void store_periodic(T* out, int n, int sx, int x, int y, int z, T v)
+{
+    store_with_images(out, n, sx, out + grown_index<T>(n, sx, x, y, z), edge_code(x, n), edge_code(y, n),
+                      edge_code(z, n), v);
+}
+
+// Row cursor of a periodic output for a thread's points x, x+1 (kPV of them) in one row: the
+// address of the first point's valid cell at the row's first plane z0, and the constant offsets of
+// the periodic images (0 when there is none): per point in x, and for the row in y.
+constexpr int kPV = 2;
 template <typename T>
 struct PeriodicRow {
     T* p;
     int z0;
-    int flags;
-    __device__ __forceinline__ bool active() const { return flags & 1; }
+    int yo;
+    int xo[kPV];
+    bool act;
+    __device__ __forceinline__ bool active() const { return act; }
 };
-template <typename T>
-__device__ __forceinline__ PeriodicRow<T> periodic_row(T* out, int n, int x, int y, int z0, bool active)
+__device__ __forceinline__ int image_offset(int c, int n, int stride)
 {
-    const long long S = n + 2;
+    return c == 0 ? n * stride : (c == n - 1 ? -n * stride : 0);
+}
+template <typename T>
+__device__ __forceinline__ PeriodicRow<T> periodic_row(T* out, int n, int sx, int x, int y, int z0, bool active)
+{
     PeriodicRow<T> r;
-    r.p = active ? out + (x + 1) + S * ((y + 1) + S * (long long)(z0 + 1)) : out;
+    r.p = active ? out + grown_index<T>(n, sx, x, y, z0) : out;
     r.z0 = z0;
-    r.flags = (active ? 1 : 0) | ((x == 0 || x == n - 1 || y == 0 || y == n - 1) ? 2 : 0);
+    r.act = active;
+    r.yo = image_offset(y, n, sx);
+#pragma unroll
+    for (int v = 0; v < kPV; v++) r.xo[v] = image_offset(x + v, n, 1);
     return r;
 }
-// boundary cell given by its address in the grown box: recover (x, y, z) and write the images
-template <typename T>
-__device__ __noinline__ void store_periodic_at(T* out, int n, T* q, T v)
+// Stores v at point (row, plane z0+zo, x+pv) and at its periodic images. ZE: the plane is the
+// first or last of the domain. A 1-cell box (every coordinate both first and last) takes the
+// general path.
+template <bool ZE, typename T>
+__device__ __forceinline__ void store_row(T* out, int n, int sx, const PeriodicRow<T>& r, int zo, int pv, T val)
 {
-    const long long S = n + 2, i = q - out;
-    const int x = (int)(i % S) - 1, y = (int)((i / S) % S) - 1, z = (int)(i / (S * S)) - 1;
-    store_periodic_images(out, n, x, y, z, v);
+    T* q = r.p + (long long)zo * sx * (n + 2) + pv;
+    if (n == 1) {
+        store_periodic_images(out, n, sx, 0, 0, 0, val);
+        return;
+    }
+    const int xo = r.xo[pv], yo = r.yo;
+    *q = val;
+    if (xo) q[xo] = val;
+    if (yo) {
+        q[yo] = val;
+        if (xo) q[yo + xo] = val;
+    }
+    if constexpr (ZE) {
+        const long long zs = (long long)n * sx * (n + 2);
+        T* qz = q + (r.z0 + zo == 0 ? zs : -zs);
+        *qz = val;
+        if (xo) qz[xo] = val;
+        if (yo) {
+            qz[yo] = val;
+            if (xo) qz[yo + xo] = val;
+        }
+    }
 }
 template <typename T>
-__device__ __forceinline__ void store_row(T* out, int n, const PeriodicRow<T>& r, int zo, T v)
+__device__ __forceinline__ T load_row(const PeriodicRow<T>& r, int n, int sx, int zo, int pv)
 {
-    const int z = r.z0 + zo;
-    T* q = r.p + (long long)zo * (n + 2) * (n + 2);
-    if ((r.flags & 2) || z == 0 || z == n - 1) store_periodic_at(out, n, q, v);
-    else *q = v;
-}
-template <typename T>
-__device__ __forceinline__ T load_row(const PeriodicRow<T>& r, int n, int zo)
-{
-    return r.p[(long long)zo * (n + 2) * (n + 2)];
+    return r.p[(long long)zo * sx * (n + 2) + pv];
 }
 
 // Scalars of one level's smoother.
 template <typename T>
 struct RelaxCoef {
-    int n;
+    int n, sx;           // edge and x pitch of the level
     int helm;
     T neg_lambda;        // Poisson form: -omega*h*h/6
     T beta, omega, diagB;
@@ -128,13 +194,16 @@ struct EpiRelax {
     T* out;
     RelaxCoef<T> k;
     using Row = PeriodicRow<T>;
-    __device__ __forceinline__ Row row(int x, int y, int z0, bool active) const { return periodic_row(out, k.n, x, y, z0, active); }
-    __device__ __forceinline__ T init(const Row&, int, const AuxCtx&) const { return T(0); }
-    __device__ __forceinline__ void finish(const Row& r, int zo, T acc, T c, const AuxCtx& ax) const
+    static constexpr bool kZEdge = true;
+    __device__ __forceinline__ Row row(int x, int y, int z0, bool active) const { return periodic_row(out, k.n, k.sx, x, y, z0, active); }
+    __device__ __forceinline__ bool z_edge(int z) const { return z == 0 || z == k.n - 1; }
+    __device__ __forceinline__ T init(const Row&, int, int, const AuxCtx&) const { return T(0); }
+    template <bool ZE>
+    __device__ __forceinline__ void finish(const Row& r, int zo, int pv, T acc, T c, const AuxCtx& ax) const
     {
         if (!r.active()) return;
         const T al = k.helm ? ax.get<T>(1) : T(0);
-        store_row(out, k.n, r, zo, relax_value(k, acc, c, ax.get<T>(0), al));
+        store_row<ZE>(out, k.n, k.sx, r, zo, pv, relax_value(k, acc, c, ax.get<T>(0), al));
     }
     __device__ __forceinline__ void end_warp() const {}
     __device__ __forceinline__ void end_block() const {}
@@ -144,16 +213,20 @@ struct EpiRelax {
 // u64 += (double) e_new, periodic images included. Auxiliary fields as in EpiRelax.
 struct EpiRelaxUpdate {
     double* u;
+    int usx;             // x pitch of u
     RelaxCoef<float> k;
     using Row = PeriodicRow<double>;
-    __device__ __forceinline__ Row row(int x, int y, int z0, bool active) const { return periodic_row(u, k.n, x, y, z0, active); }
-    __device__ __forceinline__ float init(const Row&, int, const AuxCtx&) const { return 0.f; }
-    __device__ __forceinline__ void finish(const Row& r, int zo, float acc, float c, const AuxCtx& ax) const
+    static constexpr bool kZEdge = true;
+    __device__ __forceinline__ Row row(int x, int y, int z0, bool active) const { return periodic_row(u, k.n, usx, x, y, z0, active); }
+    __device__ __forceinline__ bool z_edge(int z) const { return z == 0 || z == k.n - 1; }
+    __device__ __forceinline__ float init(const Row&, int, int, const AuxCtx&) const { return 0.f; }
+    template <bool ZE>
+    __device__ __forceinline__ void finish(const Row& r, int zo, int pv, float acc, float c, const AuxCtx& ax) const
     {
         if (!r.active()) return;
         const float al = k.helm ? ax.get<float>(1) : 0.f;
         const float e = relax_value(k, acc, c, ax.get<float>(0), al);
-        store_row(u, k.n, r, zo, dadd(load_row(r, k.n, zo), (double)e));
+        store_row<ZE>(u, k.n, usx, r, zo, pv, dadd(load_row(r, k.n, usx, zo, pv), (double)e));
     }
     __device__ __forceinline__ void end_warp() const {}
     __device__ __forceinline__ void end_block() const {}
@@ -168,13 +241,16 @@ struct EpiResnorm {
     double* result;
     double m;
     using Row = OutRow<T>;
+    static constexpr bool kZEdge = false;
     __device__ __forceinline__ Row row(int, int, int, bool active) const { return Row{nullptr, active}; }
-    __device__ __forceinline__ T init(const Row& r, int, const AuxCtx& ax) const
+    __device__ __forceinline__ bool z_edge(int) const { return false; }
+    __device__ __forceinline__ T init(const Row& r, int, int, const AuxCtx& ax) const
     {
         if (helm || !r.active) return T(0);
         return dsub(T(0), ax.get<T>(0));
     }
-    __device__ __forceinline__ void finish(const Row& r, int, T acc, T c, const AuxCtx& ax)
+    template <bool ZE>
+    __device__ __forceinline__ void finish(const Row& r, int, int, T acc, T c, const AuxCtx& ax)
     {
         if (!r.active) return;
         if (!helm) {
@@ -196,7 +272,7 @@ struct Res64Row {
     float* r;
 };
 struct EpiRes64 {
-    float* e32;          // (n+2)^3
+    float* e32;          // grown FP32 level (pitch k.sx)
     float* rhs32;        // n^3
     int helm;
     double beta;
@@ -204,19 +280,22 @@ struct EpiRes64 {
     double* result;
     double m;
     using Row = Res64Row;
+    static constexpr bool kZEdge = true;
     __device__ __forceinline__ Row row(int x, int y, int z0, bool active) const
     {
         Row r;
-        r.e = periodic_row(e32, k.n, x, y, z0, active);
+        r.e = periodic_row(e32, k.n, k.sx, x, y, z0, active);
         r.r = active ? rhs32 + x + (long long)k.n * (y + (long long)k.n * z0) : rhs32;
         return r;
     }
-    __device__ __forceinline__ double init(const Row& r, int, const AuxCtx& ax) const
+    __device__ __forceinline__ bool z_edge(int z) const { return z == 0 || z == k.n - 1; }
+    __device__ __forceinline__ double init(const Row& r, int, int, const AuxCtx& ax) const
     {
         if (helm || !r.e.active()) return 0.0;
         return dadd(0.0, ax.get<double>(0));
     }
-    __device__ __forceinline__ void finish(const Row& r, int zo, double acc, double c, const AuxCtx& ax)
+    template <bool ZE>
+    __device__ __forceinline__ void finish(const Row& r, int zo, int pv, double acc, double c, const AuxCtx& ax)
     {
         if (!r.e.active()) return;
         double res = acc;
@@ -228,8 +307,8 @@ struct EpiRes64 {
         }
         m = upd_abs(m, res);
         const float r32 = __double2float_rn(res);
-        r.r[(long long)zo * k.n * k.n] = r32;
-        store_row(e32, k.n, r.e, zo, relax_value(k, 0.f, 0.f, r32, al));
+        r.r[(long long)zo * k.n * k.n + pv] = r32;
+        store_row<ZE>(e32, k.n, k.sx, r.e, zo, pv, relax_value(k, 0.f, 0.f, r32, al));
     }
     __device__ __forceinline__ void end_warp() const { warp_max_atomic(m, result); }
     __device__ __forceinline__ void end_block() const { block_max_atomic(m, result); }
@@ -248,20 +327,20 @@ __global__ void __launch_bounds__(256) k_relax_first(const T* __restrict__ rhs, 
         long long q = i / n;
         int y = (int)(q % n), z = (int)(q / n);
         const T al = k.helm ? alpha[i] : T(0);
-        store_periodic(out, n, x, y, z, relax_value(k, T(0), T(0), rhs[i], al));
+        store_periodic(out, n, k.sx, x, y, z, relax_value(k, T(0), T(0), rhs[i], al));
     }
 }
 
 // exact coarsest-level solve: out = Ainv * rhs (one thread per cell, products summed in column order)
 template <typename T>
 __global__ void __launch_bounds__(256) k_bottom_direct(const T* __restrict__ ainv, const T* __restrict__ rhs, T* out,
-                                                       int n)
+                                                       int n, int sx)
 {
     const int N = n * n * n;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
         T acc = T(0);
         for (int j = 0; j < N; j++) acc = dadd(acc, dmul(ainv[(long long)i * N + j], rhs[j]));
-        store_periodic(out, n, i % n, (i / n) % n, i / (n * n), acc);
+        store_periodic(out, n, sx, i % n, (i / n) % n, i / (n * n), acc);
     }
 }
 
@@ -274,11 +353,11 @@ __global__ void __launch_bounds__(256) k_to_float(const double* __restrict__ a, 
 // coarse right-hand side: AvgDown(2) of the fine residual, children in Box([0,1]^3) order
 template <typename T>
 __global__ void __launch_bounds__(256) k_resid_restrict(const T* __restrict__ phi, const T* __restrict__ rhs,
-                                                        const T* __restrict__ alpha, T* rhs_c, int nf, int helm,
+                                                        const T* __restrict__ alpha, T* rhs_c, int nf, int sx, int helm,
                                                         Coefs<T> cf, T beta)
 {
     const int nc = nf / 2;
-    const long long S = nf + 2, S2 = S * S;
+    const long long Sy = sx, Sz = (long long)sx * (nf + 2);
     const long long total = (long long)nc * nc * nc;
     const long long stride = (long long)gridDim.x * blockDim.x;
     const T eighth = T(1.0 / 8);
@@ -291,20 +370,20 @@ __global__ void __launch_bounds__(256) k_resid_restrict(const T* __restrict__ ph
         for (int k = 0; k < 8; k++) {
             const int fx = 2 * cx + (k & 1), fy = 2 * cy + ((k >> 1) & 1), fz = 2 * cz + (k >> 2);
             const long long fi = fx + (long long)nf * (fy + (long long)nf * fz);
-            const long long gi = (fx + 1) + S * (fy + 1) + S2 * (fz + 1);
+            const long long gi = grown_index<T>(nf, sx, fx, fy, fz);
             T r;
             if (!helm) {
                 r = dadd(T(0), __ldg(rhs + fi));
 #pragma unroll
                 for (int j = 0; j < ShapeLap7::NT; j++) {
-                    const long long o = ShapeLap7::off(j, 0) + S * ShapeLap7::off(j, 1) + S2 * ShapeLap7::off(j, 2);
+                    const long long o = ShapeLap7::off(j, 0) + Sy * ShapeLap7::off(j, 1) + Sz * ShapeLap7::off(j, 2);
                     r = dadd(r, dmul(cf.c[j], __ldg(phi + gi + o)));
                 }
             } else {
                 T lp = T(0);
 #pragma unroll
                 for (int j = 0; j < ShapeLap7::NT; j++) {
-                    const long long o = ShapeLap7::off(j, 0) + S * ShapeLap7::off(j, 1) + S2 * ShapeLap7::off(j, 2);
+                    const long long o = ShapeLap7::off(j, 0) + Sy * ShapeLap7::off(j, 1) + Sz * ShapeLap7::off(j, 2);
                     lp = dadd(lp, dmul(cf.c[j], __ldg(phi + gi + o)));
                 }
                 r = dsub(__ldg(rhs + fi), dsub(dmul(__ldg(alpha + fi), __ldg(phi + gi)), dmul(beta, lp)));
@@ -317,45 +396,42 @@ __global__ void __launch_bounds__(256) k_resid_restrict(const T* __restrict__ ph
 
 // phi += 1.0 * delta_c(p/2) on the valid box, periodic images included
 template <typename T>
-__global__ void __launch_bounds__(256) k_prolong(T* phi, const T* __restrict__ delta_c, int nf)
+__global__ void __launch_bounds__(256) k_prolong(T* phi, const T* __restrict__ delta_c, int nf, int sxf, int sxc)
 {
     const int nc = nf / 2;
-    const long long S = nf + 2, Sc = nc + 2;
     const long long total = (long long)nf * nf * nf;
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
         int x = (int)(i % nf);
         long long q = i / nf;
         int y = (int)(q % nf), z = (int)(q / nf);
-        T d = __ldg(delta_c + (x / 2 + 1) + Sc * (y / 2 + 1) + Sc * Sc * (z / 2 + 1));
-        T v = dadd(phi[(x + 1) + S * (y + 1) + S * S * (z + 1)], dmul(T(1), d));
-        store_periodic(phi, nf, x, y, z, v);
+        T d = __ldg(delta_c + grown_index<T>(nc, sxc, x / 2, y / 2, z / 2));
+        T v = dadd(phi[grown_index<T>(nf, sxf, x, y, z)], dmul(T(1), d));
+        store_periodic(phi, nf, sxf, x, y, z, v);
     }
 }
 
-// n^3 <-> grown (n+2)^3 with periodic ghost images
+// n^3 <-> grown layout with periodic ghost images
 template <typename T>
-__global__ void __launch_bounds__(256) k_pack_in(const T* __restrict__ src, T* out, int n)
+__global__ void __launch_bounds__(256) k_pack_in(const T* __restrict__ src, T* out, int n, int sx)
 {
     const long long total = (long long)n * n * n;
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
         int x = (int)(i % n);
         long long q = i / n;
-        store_periodic(out, n, x, (int)(q % n), (int)(q / n), src[i]);
+        store_periodic(out, n, sx, x, (int)(q % n), (int)(q / n), src[i]);
     }
 }
 template <typename T>
-__global__ void __launch_bounds__(256) k_pack_out(const T* __restrict__ g, T* dst, int n)
+__global__ void __launch_bounds__(256) k_pack_out(const T* __restrict__ g, T* dst, int n, int sx)
 {
     const long long total = (long long)n * n * n;
-    const long long S = n + 2;
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
         int x = (int)(i % n);
         long long q = i / n;
-        int y = (int)(q % n), z = (int)(q / n);
-        dst[i] = g[(x + 1) + S * (y + 1) + S * S * (z + 1)];
+        dst[i] = g[grown_index<T>(n, sx, x, (int)(q % n), (int)(q / n))];
     }
 }
 
@@ -383,7 +459,9 @@ __global__ void __launch_bounds__(256) k_avgdown_plain(const T* __restrict__ f, 
 template <typename T>
 struct MGLevel {
     int n;
+    int sx;              // x pitch of the grown layout
     double h, hsqinv;
+    size_t grown_elems() const { return (size_t)sx * (n + 2) * (n + 2); }
     T* phi[2] = {nullptr, nullptr};
     T* rhs = nullptr;
     T* alpha = nullptr;
@@ -458,7 +536,7 @@ struct pb_mg {
     pb_mg_params p;
     std::vector<pb::MGLevel<double>> lv;    // FP64 hierarchy, index 0 = coarsest (precision FP64)
     std::vector<pb::MGLevel<float>> lv32;   // FP32 hierarchy including the finest grid (precision MIXED)
-    double* u64 = nullptr;                  // MIXED: FP64 solution, (n+2)^3 with periodic images
+    double* u64 = nullptr;                  // MIXED: FP64 solution, grown layout with periodic images
     double* f64 = nullptr;                  // MIXED: FP64 right-hand side, n^3
     double* alpha64 = nullptr;              // MIXED, Helmholtz: FP64 alpha, n^3
     double* ainv64 = nullptr;               // direct bottom solve: inverse of the coarsest operator
@@ -477,11 +555,13 @@ static inline double lambda_of(const pb_mg_params& p, double h) { return (p.omeg
 static inline bool is_mixed(const pb_mg* mg) { return mg->p.precision == PB_MG_MIXED; }
 static inline bool is_helm(const pb_mg* mg) { return mg->p.form == PB_MG_HELMHOLTZ; }
 
+// the grown layout as a box: x spans the pitch (padding columns included), y and z one ghost layer
 template <typename T>
 static Box3 grown_box(const MGLevel<T>& L)
 {
     Box3 b;
     for (int d = 0; d < 3; d++) { b.lo[d] = -1; b.hi[d] = L.n; }
+    b.hi[0] = L.sx - 2;
     return b;
 }
 template <typename T>
@@ -508,6 +588,7 @@ static RelaxCoef<T> relax_coef(const pb_mg* mg, const MGLevel<T>& L)
 {
     RelaxCoef<T> k;
     k.n = L.n;
+    k.sx = L.sx;
     k.helm = is_helm(mg);
     k.neg_lambda = (T)(-lambda_of(mg->p, L.h));
     k.beta = (T)mg->p.beta;
@@ -554,6 +635,7 @@ static int launch_relax_update(pb_mg* mg, MGLevel<float>& L, cudaStream_t st)
 {
     EpiRelaxUpdate epi;
     epi.u = mg->u64;
+    epi.usx = grown_pitch<double>(L.n);
     epi.k = relax_coef(mg, L);
     const double s = is_helm(mg) ? L.hsqinv : mg->p.omega / 6.0;
     return launch_star<ShapeLap7>(L.phi[L.cur], grown_box(L), valid_box(L), lap7_coefs<float>(s), epi, st,
@@ -587,6 +669,7 @@ static int launch_res64(pb_mg* mg, cudaStream_t st)
     epi.m = 0.0;
     MGLevel<double> G;
     G.n = L.n;
+    G.sx = grown_pitch<double>(L.n);
     G.h = L.h;
     G.hsqinv = L.hsqinv;
     const double s = is_helm(mg) ? L.hsqinv : -L.hsqinv;
@@ -603,7 +686,7 @@ static int relax_sweeps(pb_mg* mg, MGLevel<T>& L, int k, bool zero_start, cudaSt
         int e = launch_relax(mg, L, zero_start && s == 0, st);
         if (e != PB_OK) return e;
     }
-    if (zero_start && k == 0) PB_CUDA(cudaMemsetAsync(L.phi[L.cur], 0, sizeof(T) * (size_t)(L.n + 2) * (L.n + 2) * (L.n + 2), st));
+    if (zero_start && k == 0) PB_CUDA(cudaMemsetAsync(L.phi[L.cur], 0, sizeof(T) * L.grown_elems(), st));
     return PB_OK;
 }
 
@@ -629,12 +712,12 @@ static int vcycle(pb_mg* mg, std::vector<MGLevel<T>>& lv, int l, bool zero_start
         if ((e = relax_sweeps(mg, L, mg->p.nu1 - pre_done, zero_start && !pre_done, st)) != PB_OK) return e;
         const double s = is_helm(mg) ? L.hsqinv : -L.hsqinv;
         const long long nc3 = (long long)C.n * C.n * C.n;
-        k_resid_restrict<T><<<grid_for(nc3, 256), 256, 0, st>>>(L.phi[L.cur], L.rhs, L.alpha, C.rhs, L.n, is_helm(mg),
+        k_resid_restrict<T><<<grid_for(nc3, 256), 256, 0, st>>>(L.phi[L.cur], L.rhs, L.alpha, C.rhs, L.n, L.sx, is_helm(mg),
                                                                 lap7_coefs<T>(s), (T)mg->p.beta);
         PB_LAUNCH_CHECK();
         if ((e = vcycle(mg, lv, l - 1, true, 0, false, st)) != PB_OK) return e;
         const long long n3 = (long long)L.n * L.n * L.n;
-        k_prolong<T><<<grid_for(n3, 256), 256, 0, st>>>(L.phi[L.cur], C.phi[C.cur], L.n);
+        k_prolong<T><<<grid_for(n3, 256), 256, 0, st>>>(L.phi[L.cur], C.phi[C.cur], L.n, L.sx, C.sx);
         PB_LAUNCH_CHECK();
         if (!fuse_update) return relax_sweeps(mg, L, mg->p.nu2, false, st);
         if ((e = relax_sweeps(mg, L, mg->p.nu2 - 1, false, st)) != PB_OK) return e;
@@ -643,7 +726,7 @@ static int vcycle(pb_mg* mg, std::vector<MGLevel<T>>& lv, int l, bool zero_start
     }
     if (mg->p.bottom == PB_MG_BOTTOM_DIRECT) {
         const int N = L.n * L.n * L.n;
-        k_bottom_direct<T><<<(N + 255) / 256, 256, 0, st>>>(bottom_inverse<T>(mg), L.rhs, L.phi[0], L.n);
+        k_bottom_direct<T><<<(N + 255) / 256, 256, 0, st>>>(bottom_inverse<T>(mg), L.rhs, L.phi[0], L.n, L.sx);
         PB_LAUNCH_CHECK();
         L.cur = 0;
         return PB_OK;
@@ -721,9 +804,10 @@ static bool alloc_levels(const pb_mg_params* p, std::vector<MGLevel<T>>& lv)
     for (int l = 0; l <= p->levels; l++) {
         MGLevel<T>& L = lv[l];
         L.n = p->n >> (p->levels - l);
+        L.sx = grown_pitch<T>(L.n);
         L.h = (double)(1 << (p->levels - l)) / (double)p->n;
         L.hsqinv = 1. / (L.h * L.h);
-        const size_t g = sizeof(T) * (size_t)(L.n + 2) * (L.n + 2) * (L.n + 2);
+        const size_t g = sizeof(T) * L.grown_elems();
         const size_t c = sizeof(T) * (size_t)L.n * L.n * L.n;
         bool ok = cudaMalloc(&L.phi[0], g) == cudaSuccess && cudaMalloc(&L.phi[1], g) == cudaSuccess &&
                   cudaMalloc(&L.rhs, c) == cudaSuccess;
@@ -771,17 +855,18 @@ extern "C" {
 long long pb_mg_device_bytes(const pb_mg_params* p)
 {
     if (params_ok(p) != PB_OK) return -1;
-    const long long es = p->precision == PB_MG_MIXED ? 4 : 8;
+    const bool mixed = p->precision == PB_MG_MIXED;
+    const long long es = mixed ? 4 : 8;
     long long total = 0;
     for (int l = 0; l <= p->levels; l++) {
-        const long long n = p->n >> (p->levels - l);
-        const long long g = (n + 2) * (n + 2) * (n + 2);
-        total += 2 * g * es + n * n * n * es;
-        if (p->form == PB_MG_HELMHOLTZ) total += n * n * n * es;
+        const int n = p->n >> (p->levels - l);
+        const long long g = (long long)(mixed ? grown_pitch<float>(n) : grown_pitch<double>(n)) * (n + 2) * (n + 2);
+        total += 2 * g * es + (long long)n * n * n * es;
+        if (p->form == PB_MG_HELMHOLTZ) total += (long long)n * n * n * es;
     }
-    if (p->precision == PB_MG_MIXED) {
+    if (mixed) {
         const long long n = p->n;
-        total += (n + 2) * (n + 2) * (n + 2) * 8 + n * n * n * 8;
+        total += (long long)grown_pitch<double>(p->n) * (n + 2) * (n + 2) * 8 + n * n * n * 8;
         if (p->form == PB_MG_HELMHOLTZ) total += n * n * n * 8;
     }
     if (p->bottom == PB_MG_BOTTOM_DIRECT) {
@@ -803,10 +888,9 @@ int pb_mg_create(const pb_mg_params* p, pb_mg** out)
     bool ok;
     const long long n0 = p->n >> p->levels, N0 = n0 * n0 * n0;
     if (p->precision == PB_MG_MIXED) {
-        const size_t n = (size_t)p->n;
-        ok = alloc_levels(p, mg->lv32) && cudaMalloc(&mg->u64, 8 * (n + 2) * (n + 2) * (n + 2)) == cudaSuccess &&
-             cudaMalloc(&mg->f64, 8 * n * n * n) == cudaSuccess &&
-             cudaMemset(mg->u64, 0, 8 * (n + 2) * (n + 2) * (n + 2)) == cudaSuccess;
+        const size_t n = (size_t)p->n, ug = 8 * (size_t)grown_pitch<double>(p->n) * (n + 2) * (n + 2);
+        ok = alloc_levels(p, mg->lv32) && cudaMalloc(&mg->u64, ug) == cudaSuccess &&
+             cudaMalloc(&mg->f64, 8 * n * n * n) == cudaSuccess && cudaMemset(mg->u64, 0, ug) == cudaSuccess;
         if (ok && p->form == PB_MG_HELMHOLTZ) ok = cudaMalloc(&mg->alpha64, 8 * n * n * n) == cudaSuccess;
         if (ok && p->bottom == PB_MG_BOTTOM_DIRECT) ok = cudaMalloc(&mg->ainv32, sizeof(float) * N0 * N0) == cudaSuccess;
     } else {
@@ -878,13 +962,13 @@ int pb_mg_solve(pb_mg* mg, const double* rhs, double* phi, int* iters, double* h
     MGLevel<double>* T = mixed ? nullptr : &mg->lv.back();
     if (mixed) {
         PB_CUDA(cudaMemcpyAsync(mg->f64, rhs, sizeof(double) * n3, cudaMemcpyDeviceToDevice, st));
-        k_pack_in<double><<<grid_for(n3, 256), 256, 0, st>>>(phi, mg->u64, n);
+        k_pack_in<double><<<grid_for(n3, 256), 256, 0, st>>>(phi, mg->u64, n, grown_pitch<double>(n));
         PB_LAUNCH_CHECK();
         if ((e = launch_res64(mg, st)) != PB_OK) return e;
     } else {
         PB_CUDA(cudaMemcpyAsync(T->rhs, rhs, sizeof(double) * n3, cudaMemcpyDeviceToDevice, st));
         T->cur = 0;
-        k_pack_in<double><<<grid_for(n3, 256), 256, 0, st>>>(phi, T->phi[0], n);
+        k_pack_in<double><<<grid_for(n3, 256), 256, 0, st>>>(phi, T->phi[0], n, T->sx);
         PB_LAUNCH_CHECK();
         if ((e = launch_resnorm(mg, *T, st)) != PB_OK) return e;
     }
@@ -931,7 +1015,7 @@ int pb_mg_solve(pb_mg* mg, const double* rhs, double* phi, int* iters, double* h
         if (r < mg->p.tol * r0) break;
     }
     const double* src = mixed ? mg->u64 : T->phi[T->cur];
-    k_pack_out<double><<<grid_for(n3, 256), 256, 0, st>>>(src, phi, n);
+    k_pack_out<double><<<grid_for(n3, 256), 256, 0, st>>>(src, phi, n, grown_pitch<double>(n));
     PB_LAUNCH_CHECK();
     PB_CUDA(cudaStreamSynchronize(st));
     if (read_error_mg() > 0 || read_error_stencil() > 0) return PB_ERR_DEVICE;

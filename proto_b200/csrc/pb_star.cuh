@@ -1,12 +1,14 @@
 // Star-shaped stencil kernels (terms only on the axes, |offset| <= R) for sm_100a.
 //
 // Two kernels share the same epilogue interface:
-//   k_star_tma    : TMA-staged z-streaming, warp specialised. A CTA owns a 64 x TY column of output
-//                   points and a chunk of z. One producer warp brings planes of the source tile
-//                   (with an R-wide halo in x and y) into shared memory with cp.async.bulk.tensor,
-//                   through an NST-deep ring of full/empty mbarriers; consumer warps keep the z
-//                   neighbours of YB rows in a (2R+1)-deep register window and read x/y neighbours
-//                   from the centre plane in shared memory.
+//   k_star_tma    : TMA-staged z-streaming, warp specialised. A CTA owns a (64*XV) x TY column of
+//                   output points and a chunk of z. One producer warp brings planes of the source
+//                   tile (with an R-wide halo in x and y) into shared memory with
+//                   cp.async.bulk.tensor, through an NST-deep ring of full/empty mbarriers; each
+//                   consumer thread computes XV adjacent points in each of YB rows, keeps their z
+//                   neighbours in a (2R+1)-deep register window that rotates by renaming (the z
+//                   loop is unrolled by 2R+1), and reads the remaining x/y neighbours from the
+//                   centre plane in shared memory.
 //   k_star_simple : one thread per point, read-only cached global loads (small boxes, and any
 //                   box the TMA alignment rules exclude).
 //
@@ -14,6 +16,8 @@
 // (no FMA), so the result is bitwise the reference's Stencil::hostApply
 // (include/base/implem/Proto_StencilImplem.H:725-828 in the reference project).
 #pragma once
+#include <type_traits>
+
 #include "pb_internal.cuh"
 
 namespace pb {
@@ -55,16 +59,23 @@ struct StarGeom {
     int nst;    // TMA kernel: stages in the ring (>= 2R+1, <= 16)
 };
 
-constexpr int kStarTX = 64;
+constexpr int kStarTX = 64;   // consumer threads along x
 
-template <class S, typename T, int TY>
+template <class S, typename T, int TY, int XV>
 struct StarSmem {
     static constexpr int EV = 16 / (int)sizeof(T);                  // elements per 16 bytes
-    static constexpr int BX = ((kStarTX + 2 * S::R + (EV - 1)) + EV - 1) / EV * EV;
+    static constexpr int TXW = kStarTX * XV;                        // tile width in points
+    static constexpr int BX = ((TXW + 2 * S::R + (EV - 1)) + EV - 1) / EV * EV;
     static constexpr int BY = TY + 2 * S::R;
     static constexpr int PLANE_TX = BX * BY * (int)sizeof(T);       // bytes one TMA box delivers
     static constexpr int PLANE = (PLANE_TX + 127) / 128 * 128;
 };
+
+// CTAs per SM the register budget is sized for
+__host__ __device__ constexpr int star_min_blocks(int TY, int YB, int XV)
+{
+    return XV > 1 ? 2 : ((kStarTX * (TY / YB) + 32) <= 288 ? 3 : 2);
+}
 
 // Warp-wide max of a non-negative value followed by one atomic per warp (the warp-specialised
 // kernel's consumer warps finish independently).
@@ -104,8 +115,8 @@ __device__ inline void block_max_atomic(double v, double* result)
 
 // Auxiliary per-point fields an epilogue reads (e.g. the right-hand side of a relaxation): up to
 // two, each a field with its own element size and box. In the TMA kernel they travel through the
-// same pipeline as the source planes (one 64 x TY tile per output plane) or are read from global
-// memory; in the simple kernel they are read from global memory.
+// same pipeline as the source planes (one tile per output plane) or are read from global memory;
+// in the simple kernel they are read from global memory.
 struct AuxSpec {
     const void* base;
     int esize;                 // 8 or 4 bytes
@@ -124,40 +135,59 @@ struct AuxCtx {
     __device__ __forceinline__ A get(int k) const { return *reinterpret_cast<const A*>(p[k]); }
 };
 
-template <int TY>
+// shared-memory tile of one auxiliary field for one output plane: the tile's points plus room for
+// the 16-byte alignment shift of the field's x origin
+template <int TY, int XV>
 struct AuxTile {
-    static constexpr int width(int esize) { return esize == 8 ? kStarTX + 2 : kStarTX + 4; }   // room for a 16-byte pad
+    static constexpr int width(int esize) { return kStarTX * XV + 16 / esize; }
     static constexpr int bytes(int esize) { return ((width(esize) * TY * esize) + 127) / 128 * 128; }
 };
 
-// Warp-specialised TMA z-streaming star kernel. Threads: 64 x (TY/YB) consumers, each computing YB
-// rows of one x column, plus one producer warp that issues the TMA copies. Stage s of the NST-deep
-// ring holds source plane q (q % NST == s) and, when q - R is an output plane, the auxiliary tiles
-// of that plane; full[s] completes when its bytes land, empty[s] when every consumer warp is done
-// with it. Epilogues see one row at a time through a cursor set up once per row (Epi::Row). Waits
-// are bounded; on expiry the kernel flags DEV_WAIT_TIMEOUT and leaves.
-template <class S, typename T, int TY, int YB, class Epi>
-__global__ void __launch_bounds__(kStarTX * (TY / YB) + 32, (kStarTX * (TY / YB) + 32) <= 288 ? 3 : 2)
+// Runs step(integral_constant<PH>, zo + PH) for PH = P .. W-1 while zo + PH < nzl; false when a
+// step gave up (a bounded wait expired).
+template <int P, int W, class F>
+__device__ __forceinline__ bool run_phases(F& step, int zo, int nzl)
+{
+    if constexpr (P < W) {
+        if (zo + P >= nzl) return true;
+        if (!step(std::integral_constant<int, P>{}, zo + P)) return false;
+        return run_phases<P + 1, W>(step, zo, nzl);
+    } else {
+        return true;
+    }
+}
+
+// Warp-specialised TMA z-streaming star kernel. Threads: 64 x (TY/YB) consumers, each computing XV
+// adjacent points in each of YB rows, plus one producer warp that issues the TMA copies. Stage s
+// of the NST-deep ring holds source plane q (q % NST == s) and, when q - R is an output plane, the
+// auxiliary tiles of that plane; full[s] completes when its bytes land, empty[s] when every
+// consumer warp is done with it. Epilogues see points through a per-row cursor set up once
+// (Epi::Row). Epilogues that write periodic images (Epi::kZEdge) get a separate instantiation of
+// the step for the first and last plane of the domain (finish<true>), so interior planes carry no
+// z-image code. Waits are bounded; on expiry the kernel flags DEV_WAIT_TIMEOUT and leaves.
+template <class S, typename T, int TY, int YB, int XV, class Epi>
+__global__ void __launch_bounds__(kStarTX * (TY / YB) + 32, star_min_blocks(TY, YB, XV))
     k_star_tma(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CUtensorMap amap0,
                const __grid_constant__ CUtensorMap amap1, const StarGeom g, const AuxSpecs aux, const Coefs<T> cf,
                const Epi epi_in)
 {
-    using SM = StarSmem<S, T, TY>;
-    constexpr int R = S::R;
+    using SM = StarSmem<S, T, TY, XV>;
+    using AT = AuxTile<TY, XV>;
+    constexpr int R = S::R, W = 2 * R + 1;
     constexpr int NCW = kStarTX * (TY / YB) / 32;     // consumer warps
     static_assert(TY % YB == 0, "rows per thread must divide the tile");
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int NST = g.nst;                            // the launcher checks 2R+1 <= NST <= 16
     const bool aux_sm = aux.in_smem != 0;
-    const int aux_b0 = (aux_sm && aux.n > 0) ? AuxTile<TY>::bytes(aux.a[0].esize) : 0;
-    const int aux_b1 = (aux_sm && aux.n > 1) ? AuxTile<TY>::bytes(aux.a[1].esize) : 0;
+    const int aux_b0 = (aux_sm && aux.n > 0) ? AT::bytes(aux.a[0].esize) : 0;
+    const int aux_b1 = (aux_sm && aux.n > 1) ? AT::bytes(aux.a[1].esize) : 0;
     const int stage = SM::PLANE + aux_b0 + aux_b1;
     uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + NST * stage);
     uint64_t* empty = full + NST;
 
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
-    const int x0 = blockIdx.x * kStarTX, y0 = blockIdx.y * TY;
+    const int x0 = blockIdx.x * SM::TXW, y0 = blockIdx.y * TY;
     const int zb = blockIdx.z * g.zc;
     const int nzl = min(g.zc, g.nz - zb);
     if (nzl <= 0) return;
@@ -189,8 +219,8 @@ __global__ void __launch_bounds__(kStarTX * (TY / YB) + 32, (kStarTX * (TY / YB)
                 const bool with_aux = aux_sm && aux.n > 0 && zo >= 0 && zo < nzl;
                 uint32_t bytes = SM::PLANE_TX;
                 if (with_aux) {
-                    bytes += AuxTile<TY>::width(aux.a[0].esize) * TY * aux.a[0].esize;
-                    if (aux.n > 1) bytes += AuxTile<TY>::width(aux.a[1].esize) * TY * aux.a[1].esize;
+                    bytes += AT::width(aux.a[0].esize) * TY * aux.a[0].esize;
+                    if (aux.n > 1) bytes += AT::width(aux.a[1].esize) * TY * aux.a[1].esize;
                 }
                 mbar_arrive_expect_tx(&full[s], bytes);
                 tma_load_3d(st, &tmap, &full[s], xs, ys, zs0 + q);
@@ -217,27 +247,27 @@ __global__ void __launch_bounds__(kStarTX * (TY / YB) + 32, (kStarTX * (TY / YB)
     // ---- consumer warps ----
     Epi epi = epi_in;
     const int tx = tid & (kStarTX - 1), ty = tid / kStarTX;
-    const int x = x0 + tx;
+    const int x = x0 + tx * XV;                            // first of this thread's XV points
     const int yr0 = ty * YB;                               // first tile row of this thread
-    const bool xin = x < g.nx;
-    const int sc0 = (yr0 + R) * SM::BX + (tx + R + g.pad); // centre element of the first row
-    // per-row epilogue state, computed once; auxiliary-field addresses of row r are
-    // base + abase + r * arow (shared-memory tile or global field)
+    const bool xin = x < g.nx;                             // XV > 1: the launcher ensures nx % XV == 0
+    const int sc0 = (yr0 + R) * SM::BX + (tx * XV + R + g.pad);   // centre element of the first point
     typename Epi::Row rows[YB];
 #pragma unroll
     for (int r = 0; r < YB; r++) {
         const int y = y0 + yr0 + r;
         rows[r] = epi.row(x, y, zb, xin && (y < g.ny));
     }
+    // auxiliary-field address of row r, point v: base + abase + r * arow + v * esize
     long long abase0, abase1, astep0 = 0, astep1 = 0;
     int arow0, arow1;
+    const int es0 = aux.a[0].esize, es1 = aux.a[1].esize;
     {
         const AuxSpec& a0 = aux.a[0];
         const AuxSpec& a1 = aux.a[1];
         if (aux_sm) {
-            const int w0 = AuxTile<TY>::width(a0.esize), w1 = AuxTile<TY>::width(a1.esize);
-            abase0 = ((long long)yr0 * w0 + tx + a0.ox % (16 / a0.esize)) * a0.esize;
-            abase1 = ((long long)yr0 * w1 + tx + a1.ox % (16 / a1.esize)) * a1.esize;
+            const int w0 = AT::width(a0.esize), w1 = AT::width(a1.esize);
+            abase0 = ((long long)yr0 * w0 + tx * XV + a0.ox % (16 / a0.esize)) * a0.esize;
+            abase1 = ((long long)yr0 * w1 + tx * XV + a1.ox % (16 / a1.esize)) * a1.esize;
             arow0 = w0 * a0.esize;
             arow1 = w1 * a1.esize;
         } else {
@@ -250,64 +280,91 @@ __global__ void __launch_bounds__(kStarTX * (TY / YB) + 32, (kStarTX * (TY / YB)
             astep1 = (long long)a1.Sx * a1.Sy * a1.esize;
         }
     }
-    uint32_t fph = 0;                                      // parity bits of the next full-wait per slot
+    T win[YB][XV][W];
     bool ok = true;
-    T win[YB][2 * R + 1];
-    // window: planes 0 .. 2R-1
+    // window: planes 0 .. 2R-1 (slots 0 .. 2R-1 of the ring, first use: parity 0)
 #pragma unroll
     for (int q = 0; q < 2 * R; q++) {
-        ok &= mbar_wait(&full[q], (fph >> q) & 1);
-        fph ^= 1u << q;
+        ok &= mbar_wait(&full[q], 0);
         const T* pl = reinterpret_cast<const T*>(smem_raw + q * stage);
 #pragma unroll
-        for (int r = 0; r < YB; r++) win[r][q] = pl[sc0 + r * SM::BX];
+        for (int r = 0; r < YB; r++)
+#pragma unroll
+            for (int v = 0; v < XV; v++) win[r][v][q] = pl[sc0 + r * SM::BX + v];
     }
     __syncwarp();
     // planes 0 .. R-1 only fed the window
     if (lane == 0)
         for (int q = 0; q < R; q++) mbar_arrive(&empty[q]);
-    int sn = 2 * R % NST, scs = R % NST;                   // slots of the newest and the centre plane
     ok = __all_sync(0xffffffffu, ok);
-    for (int zo = 0; zo < nzl && ok; zo++) {
-        ok = __all_sync(0xffffffffu, mbar_wait(&full[sn], (fph >> sn) & 1));
-        fph ^= 1u << sn;
-        const T* pn = reinterpret_cast<const T*>(smem_raw + sn * stage);
-#pragma unroll
-        for (int r = 0; r < YB; r++) win[r][2 * R] = pn[sc0 + r * SM::BX];
-        const unsigned char* stc = smem_raw + scs * stage;
-        const T* pc = reinterpret_cast<const T*>(stc);
-        const unsigned char* ab0 = (aux_sm ? stc + SM::PLANE : reinterpret_cast<const unsigned char*>(aux.a[0].base) + zo * astep0) + abase0;
-        const unsigned char* ab1 = (aux_sm ? stc + SM::PLANE + aux_b0 : reinterpret_cast<const unsigned char*>(aux.a[1].base) + zo * astep1) + abase1;
-#pragma unroll
-        for (int r = 0; r < YB; r++) {
-            AuxCtx ax;
-            ax.p[0] = ab0 + r * arow0;
-            ax.p[1] = ab1 + r * arow1;
-            T acc = epi.init(rows[r], zo, ax);
-#pragma unroll
-            for (int j = 0; j < S::NT; j++) {
-                const int ox = S::off(j, 0), oy = S::off(j, 1), oz = S::off(j, 2);
-                T v;
-                if (oz != 0) v = win[r][R + oz];
-                else if (ox == 0 && oy == 0) v = win[r][R];
-                else if (ox == 0 && r + oy >= 0 && r + oy < YB) v = win[r + oy][R];   // another row of this thread
-                else v = pc[sc0 + (r + oy) * SM::BX + ox];
-                acc = dadd(acc, dmul(cf.c[j], v));
-            }
-            epi.finish(rows[r], zo, acc, win[r][R], ax);
-        }
+    int sn = 2 * R;        // slot of the newest plane (NST > 2R)
+    uint32_t pn = 0;       // its phase parity
+    int scs = R;           // slot of the centre plane
+
+    // One z step. PH = zo mod (2R+1) names the window slots, so the window rotates by renaming;
+    // ZE: this plane is the first or last of the domain (periodic z images).
+    auto step_ze = [&](auto PHc, auto ZEc, int zo) -> bool {
+        constexpr int PH = decltype(PHc)::value;
+        constexpr bool ZE = decltype(ZEc)::value;
+        constexpr int IN = (PH + 2 * R) % W, IC = (PH + R) % W;
+        if (!__all_sync(0xffffffffu, mbar_wait(&full[sn], pn))) return false;
+        const T* pnew = reinterpret_cast<const T*>(smem_raw + sn * stage);
 #pragma unroll
         for (int r = 0; r < YB; r++)
 #pragma unroll
-            for (int k = 0; k < 2 * R; k++) win[r][k] = win[r][k + 1];
+            for (int v = 0; v < XV; v++) win[r][v][IN] = pnew[sc0 + r * SM::BX + v];
+        const unsigned char* stc = smem_raw + scs * stage;
+        const T* pc = reinterpret_cast<const T*>(stc);
+        const unsigned char* ab0 =
+            (aux_sm ? stc + SM::PLANE : reinterpret_cast<const unsigned char*>(aux.a[0].base) + zo * astep0) + abase0;
+        const unsigned char* ab1 =
+            (aux_sm ? stc + SM::PLANE + aux_b0 : reinterpret_cast<const unsigned char*>(aux.a[1].base) + zo * astep1) +
+            abase1;
+#pragma unroll
+        for (int r = 0; r < YB; r++) {
+#pragma unroll
+            for (int v = 0; v < XV; v++) {
+                AuxCtx ax;
+                ax.p[0] = ab0 + r * arow0 + v * es0;
+                ax.p[1] = ab1 + r * arow1 + v * es1;
+                T acc = epi.init(rows[r], zo, v, ax);
+#pragma unroll
+                for (int j = 0; j < S::NT; j++) {
+                    const int ox = S::off(j, 0), oy = S::off(j, 1), oz = S::off(j, 2);
+                    T val;
+                    if (oz != 0) val = win[r][v][(IC + oz + W) % W];
+                    else if (ox == 0 && oy == 0) val = win[r][v][IC];
+                    else if (oy == 0 && v + ox >= 0 && v + ox < XV) val = win[r][v + ox][IC];   // this thread's point
+                    else if (ox == 0 && r + oy >= 0 && r + oy < YB) val = win[r + oy][v][IC];   // this thread's row
+                    else val = pc[sc0 + (r + oy) * SM::BX + v + ox];
+                    acc = dadd(acc, dmul(cf.c[j], val));
+                }
+                epi.template finish<ZE>(rows[r], zo, v, acc, win[r][v][IC], ax);
+            }
+        }
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty[scs]);
-        if (++sn == NST) sn = 0;
+        if (++sn == NST) {
+            sn = 0;
+            pn ^= 1;
+        }
         if (++scs == NST) scs = 0;
+        return true;
+    };
+    auto step = [&](auto PHc, int zo) -> bool {
+        if constexpr (Epi::kZEdge) {
+            if (epi.z_edge(zb + zo)) return step_ze(PHc, std::true_type{}, zo);
+        }
+        return step_ze(PHc, std::false_type{}, zo);
+    };
+    if (ok) {
+        for (int zo = 0; zo < nzl; zo += W)
+            if (!run_phases<0, W>(step, zo, nzl)) break;
     }
     epi.end_warp();
 }
 
+// One thread per point (small boxes and any box the TMA rules exclude).
 template <class S, typename T, class Epi>
 __global__ void __launch_bounds__(256) k_star_simple(const T* __restrict__ src, const StarGeom g, const AuxSpecs aux,
                                                      const Coefs<T> cf, const Epi epi_in)
@@ -328,18 +385,28 @@ __global__ void __launch_bounds__(256) k_star_simple(const T* __restrict__ src, 
         ax.p[1] = reinterpret_cast<const unsigned char*>(aux.a[1].base) +
                   ((x + aux.a[1].ox) + (long long)aux.a[1].Sx * ((y + aux.a[1].oy) + (long long)aux.a[1].Sy * (z + aux.a[1].oz))) * aux.a[1].esize;
         const typename Epi::Row row = epi.row(x, y, z, true);
-        T acc = epi.init(row, 0, ax);
+        T acc = epi.init(row, 0, 0, ax);
 #pragma unroll
         for (int j = 0; j < S::NT; j++) {
             const long long o = S::off(j, 0) + Sx * S::off(j, 1) + Sxy * S::off(j, 2);
             acc = dadd(acc, dmul(cf.c[j], __ldg(src + base + o)));
         }
-        epi.finish(row, 0, acc, __ldg(src + base), ax);
+        bool ze = false;
+        if constexpr (Epi::kZEdge) ze = epi.z_edge(z);
+        if (ze) epi.template finish<true>(row, 0, 0, acc, __ldg(src + base), ax);
+        else epi.template finish<false>(row, 0, 0, acc, __ldg(src + base), ax);
     }
     epi.end_block();
 }
 
 // ---- basic epilogues ---------------------------------------------------------------------------
+// Epilogue interface (both kernels):
+//   Row                      per-row cursor type
+//   kZEdge                   whether some planes need separate handling (then z_edge(z) says which)
+//   row(x, y, z0, active)    cursor of the row of points x .. x+XV-1 at y, starting at plane z0
+//   init(row, zo, v, ax)     accumulator start for point v of the row at plane z0+zo
+//   finish<ZE>(row, zo, v, acc, c, ax)   consume the stencil sum (c = the source's centre value)
+//   end_warp() / end_block() after the TMA / simple kernel's last point
 // Output addressing for a field on a box: index-box point (x,y,z) -> (x+dx) + Dx*(y+dy) + Dxy*(z+dz)
 struct OutMap {
     long long dx, dy, dz, Dx, Dxy;
@@ -360,15 +427,18 @@ struct EpiStore {
     OutMap m;
     int accumulate;
     using Row = OutRow<T>;
+    static constexpr bool kZEdge = false;
     __device__ __forceinline__ Row row(int x, int y, int z0, bool active) const { return Row{dst + m.at(x, y, z0), active}; }
-    __device__ __forceinline__ T init(const Row& r, int zo, const AuxCtx&) const
+    __device__ __forceinline__ T init(const Row& r, int zo, int v, const AuxCtx&) const
     {
-        return (accumulate && r.active) ? r.p[zo * m.Dxy] : T(0);
+        return (accumulate && r.active) ? r.p[zo * m.Dxy + v] : T(0);
     }
-    __device__ __forceinline__ void finish(const Row& r, int zo, T acc, T, const AuxCtx&) const
+    template <bool ZE>
+    __device__ __forceinline__ void finish(const Row& r, int zo, int v, T acc, T, const AuxCtx&) const
     {
-        if (r.active) r.p[zo * m.Dxy] = acc;
+        if (r.active) r.p[zo * m.Dxy + v] = acc;
     }
+    __device__ __forceinline__ bool z_edge(int) const { return false; }
     __device__ __forceinline__ void end_warp() const {}
     __device__ __forceinline__ void end_block() const {}
 };
@@ -381,12 +451,15 @@ struct EpiAxpby {
     T a, b;
     int euler;
     using Row = OutRow<T>;
+    static constexpr bool kZEdge = false;
     __device__ __forceinline__ Row row(int x, int y, int z0, bool active) const { return Row{dst + m.at(x, y, z0), active}; }
-    __device__ __forceinline__ T init(const Row&, int, const AuxCtx&) const { return T(0); }
-    __device__ __forceinline__ void finish(const Row& r, int zo, T acc, T u, const AuxCtx&) const
+    __device__ __forceinline__ T init(const Row&, int, int, const AuxCtx&) const { return T(0); }
+    template <bool ZE>
+    __device__ __forceinline__ void finish(const Row& r, int zo, int v, T acc, T u, const AuxCtx&) const
     {
-        if (r.active) r.p[zo * m.Dxy] = euler ? dadd(u, dmul(a, acc)) : dadd(dmul(a, acc), dmul(b, u));
+        if (r.active) r.p[zo * m.Dxy + v] = euler ? dadd(u, dmul(a, acc)) : dadd(dmul(a, acc), dmul(b, u));
     }
+    __device__ __forceinline__ bool z_edge(int) const { return false; }
     __device__ __forceinline__ void end_warp() const {}
     __device__ __forceinline__ void end_block() const {}
 };

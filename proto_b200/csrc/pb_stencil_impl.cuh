@@ -24,9 +24,11 @@ struct StarTune {
     int mode = AUTO;
     long long min_tma_points = 1 << 18;   // smaller boxes are launch/latency bound: simple kernel
     int zc = 0;                          // z chunk per CTA; 0 = occupancy-based heuristic
-    int ty = 8;                          // CTA tile height (rows of 64 points)
-    int yb = 2;                          // rows per consumer thread; (ty, yb) in {(4,1), (8,1), (8,2), (16,4)}
-    int nst = 0;                         // ring depth; 0 = 2R+4
+    int ty = 8;                          // CTA tile height
+    int yb = 2;                          // rows per consumer thread
+    int xv = 2;                          // adjacent x points per consumer thread; (ty, yb, xv) in
+                                         // {(8,1,1), (8,2,1), (8,2,2), (4,2,2)}
+    int nst = 0;                         // ring depth; 0 = as deep as two CTAs per SM allow (<= 2R+4)
     int aux_smem = 1;                    // stage auxiliary fields through shared memory by TMA
 };
 StarTune& default_star_tune();
@@ -58,17 +60,16 @@ inline AuxSpec aux_spec(const void* base, const Box3& fb, const Box3& ib, int es
 }
 
 // ---- star launch (shared with the multigrid module) -------------------------------------------
-template <class S, typename T, int TY, int YB, class Epi>
+template <class S, typename T, int TY, int YB, int XV, class Epi>
 int launch_star_tma(const T* src, StarGeom g, const Coefs<T>& cf, const Epi& epi, cudaStream_t st, int zc,
                     AuxSpecs aux, int nst)
 {
     constexpr int R = S::R;
     constexpr int EV = 16 / (int)sizeof(T);
     constexpr int NTHR = kStarTX * (TY / YB) + 32;
-    using SM = StarSmem<S, T, TY>;
-    if (nst <= 0) nst = 2 * R + 4;
-    if (nst < 2 * R + 1 || nst > 16) return PB_ERR_ARG;
-    g.nst = nst;
+    using SM = StarSmem<S, T, TY, XV>;
+    using AT = AuxTile<TY, XV>;
+    if (XV > 1 && g.nx % XV != 0) return PB_ERR_ARG;
     g.pad = (g.ox - R) % EV;
     CUtensorMap map, amap[2];
     int e = encode_tmap_3d(&map, src, (int)sizeof(T), g.Sx, g.Sy, g.Sz, SM::BX, SM::BY, 1);
@@ -80,15 +81,24 @@ int launch_star_tma(const T* src, StarGeom g, const Coefs<T>& cf, const Epi& epi
         for (int k = 0; k < aux.n && aux.in_smem; k++) {
             const AuxSpec& a = aux.a[k];
             if (a.ox < 0 || (a.esize != 4 && a.esize != 8) ||
-                encode_tmap_3d(&amap[k], a.base, a.esize, a.Sx, a.Sy, a.Sz, AuxTile<TY>::width(a.esize), TY, 1) != PB_OK)
+                encode_tmap_3d(&amap[k], a.base, a.esize, a.Sx, a.Sy, a.Sz, AT::width(a.esize), TY, 1) != PB_OK)
                 aux.in_smem = 0;
-            else aux_bytes += AuxTile<TY>::bytes(a.esize);
+            else aux_bytes += AT::bytes(a.esize);
         }
         if (!aux.in_smem) aux_bytes = 0;
     }
-    const size_t smem = (size_t)nst * (SM::PLANE + aux_bytes) + 2 * nst * sizeof(uint64_t);
+    const size_t stage = (size_t)SM::PLANE + aux_bytes;
+    if (nst <= 0) {
+        // deepest ring (up to 2R+4 planes) that still lets the CTAs the registers allow share an SM
+        const int per_sm = star_min_blocks(TY, YB, XV);
+        nst = 2 * R + 4;
+        while (nst > 2 * R + 1 && (size_t)per_sm * (nst * stage + 16 * nst + 1024) > 227 * 1024) nst--;
+    }
+    if (nst < 2 * R + 1 || nst > 16) return PB_ERR_ARG;
+    g.nst = nst;
+    const size_t smem = (size_t)nst * stage + 2 * nst * sizeof(uint64_t);
     if (smem > 220 * 1024) return PB_ERR_ARG;
-    auto kern = k_star_tma<S, T, TY, YB, Epi>;
+    auto kern = k_star_tma<S, T, TY, YB, XV, Epi>;
     static int occ = 0;
     static bool attr_set = false;
     if (!attr_set) {
@@ -103,7 +113,7 @@ int launch_star_tma(const T* src, StarGeom g, const Coefs<T>& cf, const Epi& epi
         if (occ < 1) occ = 1;
         occ_smem = smem;
     }
-    const long long tiles = (long long)((g.nx + kStarTX - 1) / kStarTX) * ((g.ny + TY - 1) / TY);
+    const long long tiles = (long long)((g.nx + SM::TXW - 1) / SM::TXW) * ((g.ny + TY - 1) / TY);
     if (zc <= 0) {
         // Pick the z chunk that best balances whole waves against the 2R+1 planes of halo each
         // CTA streams beyond its own: efficiency = (waves / ceil(waves)) * zc / (zc + 2R + 2).
@@ -122,7 +132,7 @@ int launch_star_tma(const T* src, StarGeom g, const Coefs<T>& cf, const Epi& epi
     }
     if (zc > g.nz) zc = g.nz;
     g.zc = zc;
-    dim3 grid((g.nx + kStarTX - 1) / kStarTX, (g.ny + TY - 1) / TY, (g.nz + zc - 1) / zc);
+    dim3 grid((g.nx + SM::TXW - 1) / SM::TXW, (g.ny + TY - 1) / TY, (g.nz + zc - 1) / zc);
     kern<<<grid, NTHR, smem, st>>>(map, amap[0], amap[1], g, aux, cf, epi);
     PB_LAUNCH_CHECK();
     return PB_OK;
@@ -158,10 +168,11 @@ int launch_star(const T* src, const Box3& srcBox, const Box3& ib, const Coefs<T>
     if (tune.mode == StarTune::TMA) use_tma = g.ox >= S::R && tma_available();
     if (use_tma) {
         int e;
-        if (tune.ty == 4) e = launch_star_tma<S, T, 4, 1>(src, g, cf, epi, st, tune.zc, aux, tune.nst);
-        else if (tune.ty == 16) e = launch_star_tma<S, T, 16, 4>(src, g, cf, epi, st, tune.zc, aux, tune.nst);
-        else if (tune.yb == 1) e = launch_star_tma<S, T, 8, 1>(src, g, cf, epi, st, tune.zc, aux, tune.nst);
-        else e = launch_star_tma<S, T, 8, 2>(src, g, cf, epi, st, tune.zc, aux, tune.nst);
+        const bool pairs = tune.xv == 2 && g.nx % 2 == 0;   // two x points per thread need an even extent
+        if (pairs && tune.ty == 4) e = launch_star_tma<S, T, 4, 2, 2>(src, g, cf, epi, st, tune.zc, aux, tune.nst);
+        else if (pairs) e = launch_star_tma<S, T, 8, 2, 2>(src, g, cf, epi, st, tune.zc, aux, tune.nst);
+        else if (tune.yb == 1) e = launch_star_tma<S, T, 8, 1, 1>(src, g, cf, epi, st, tune.zc, aux, tune.nst);
+        else e = launch_star_tma<S, T, 8, 2, 1>(src, g, cf, epi, st, tune.zc, aux, tune.nst);
         if (e == PB_OK || tune.mode == StarTune::TMA) return e;
     }
     const int threads = 256;

@@ -58,15 +58,17 @@ def test_argument_errors():
 
 def test_launch_shape_knobs_validate():
     L = pb.lib()
-    L.pb_star_tune_set.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_longlong]
-    assert L.pb_star_tune_set(0, 0, 8, 3, -1) == -1          # rows per thread must divide the tile
-    assert L.pb_star_tune_set(0, 0, 12, 1, -1) == -1
-    assert L.pb_star_tune_set(3, 0, 8, 2, -1) == -1
+    L.pb_star_tune_set.argtypes = [ctypes.c_int] * 5 + [ctypes.c_longlong]
+    assert L.pb_star_tune_set(0, 0, 8, 3, 1, -1) == -1        # rows per thread must divide the tile
+    assert L.pb_star_tune_set(0, 0, 12, 1, 1, -1) == -1
+    assert L.pb_star_tune_set(0, 0, 8, 1, 2, -1) == -1
+    assert L.pb_star_tune_set(0, 0, 8, 2, 3, -1) == -1
+    assert L.pb_star_tune_set(3, 0, 8, 2, 2, -1) == -1
     assert L.pb_star_tune_ring(2, 1) == -1                    # fewer planes than a 7-point window
     assert L.pb_star_tune_ring(17, 1) == -1
     assert L.pb_star_tune_ring(0, 2) == -1
-    for ty, yb in ((4, 1), (8, 1), (16, 4), (8, 2)):
-        assert L.pb_star_tune_set(0, 0, ty, yb, -1) == 0
+    for ty, yb, xv in ((8, 1, 1), (8, 2, 1), (4, 2, 2), (8, 2, 2)):
+        assert L.pb_star_tune_set(0, 0, ty, yb, xv, -1) == 0
     assert L.pb_star_tune_ring(0, 1) == 0
 
 

@@ -209,6 +209,10 @@ int pb_mg_solve(pb_mg* mg, const double* rhs, double* phi, int* iters, double* h
 int pb_mg_relax(pb_mg* mg, int sweeps, void* stream);
 /* Kernel launches one V-cycle plus its residual norm issues for these parameters. */
 int pb_mg_launches_per_cycle(const pb_mg_params* p);
+/* Process-wide: the levels of edge <= 'edge' below the finest grid run their part of each V-cycle
+ * as one single-CTA kernel instead of one launch per sweep (same arithmetic, same results);
+ * 0 turns this off. Default 16. Applies to solvers created and cycles captured afterwards. */
+int pb_mg_coarse_edge(int edge);
 
 #ifdef __cplusplus
 }

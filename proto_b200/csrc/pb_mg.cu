@@ -195,6 +195,7 @@ struct EpiRelax {
     RelaxCoef<T> k;
     using Row = PeriodicRow<T>;
     static constexpr bool kZEdge = true;
+    static constexpr int kAux = 2;
     __device__ __forceinline__ Row row(int x, int y, int z0, bool active) const { return periodic_row(out, k.n, k.sx, x, y, z0, active); }
     __device__ __forceinline__ bool z_edge(int z) const { return z == 0 || z == k.n - 1; }
     __device__ __forceinline__ T init(const Row&, int, int, const AuxCtx&) const { return T(0); }
@@ -210,13 +211,15 @@ struct EpiRelax {
 };
 
 // Last FP32 post-smoothing sweep of a mixed-precision cycle, fused with the FP64 correction:
-// u64 += (double) e_new, periodic images included. Auxiliary fields as in EpiRelax.
+// u64 += (double) e_new, periodic images included. Auxiliary fields 0 = u64 itself (its old value
+// arrives through the pipeline instead of a dependent load), 1 = rho, 2 = alpha (Helmholtz).
 struct EpiRelaxUpdate {
     double* u;
     int usx;             // x pitch of u
     RelaxCoef<float> k;
     using Row = PeriodicRow<double>;
     static constexpr bool kZEdge = true;
+    static constexpr int kAux = 3;
     __device__ __forceinline__ Row row(int x, int y, int z0, bool active) const { return periodic_row(u, k.n, usx, x, y, z0, active); }
     __device__ __forceinline__ bool z_edge(int z) const { return z == 0 || z == k.n - 1; }
     __device__ __forceinline__ float init(const Row&, int, int, const AuxCtx&) const { return 0.f; }
@@ -224,9 +227,9 @@ struct EpiRelaxUpdate {
     __device__ __forceinline__ void finish(const Row& r, int zo, int pv, float acc, float c, const AuxCtx& ax) const
     {
         if (!r.active()) return;
-        const float al = k.helm ? ax.get<float>(1) : 0.f;
-        const float e = relax_value(k, acc, c, ax.get<float>(0), al);
-        store_row<ZE>(u, k.n, usx, r, zo, pv, dadd(load_row(r, k.n, usx, zo, pv), (double)e));
+        const float al = k.helm ? ax.get<float>(2) : 0.f;
+        const float e = relax_value(k, acc, c, ax.get<float>(1), al);
+        store_row<ZE>(u, k.n, usx, r, zo, pv, dadd(ax.get<double>(0), (double)e));
     }
     __device__ __forceinline__ void end_warp() const {}
     __device__ __forceinline__ void end_block() const {}
@@ -242,6 +245,7 @@ struct EpiResnorm {
     double m;
     using Row = OutRow<T>;
     static constexpr bool kZEdge = false;
+    static constexpr int kAux = 2;
     __device__ __forceinline__ Row row(int, int, int, bool active) const { return Row{nullptr, active}; }
     __device__ __forceinline__ bool z_edge(int) const { return false; }
     __device__ __forceinline__ T init(const Row& r, int, int, const AuxCtx& ax) const
@@ -281,6 +285,7 @@ struct EpiRes64 {
     double m;
     using Row = Res64Row;
     static constexpr bool kZEdge = true;
+    static constexpr int kAux = 2;
     __device__ __forceinline__ Row row(int x, int y, int z0, bool active) const
     {
         Row r;
@@ -350,66 +355,73 @@ __global__ void __launch_bounds__(256) k_to_float(const double* __restrict__ a, 
         b[i] = __double2float_rn(a[i]);
 }
 
-// coarse right-hand side: AvgDown(2) of the fine residual, children in Box([0,1]^3) order
+// One fine cell's residual for the restriction: rho + L(phi, -1/h^2) (Poisson form, cf scaled by
+// -1/h^2) or rho - (alpha*phi - beta*L(phi, 1/h^2)) (Helmholtz form, cf scaled by 1/h^2).
+template <typename T>
+__device__ __forceinline__ T fine_residual(const T* phi, long long gi, long long Sy, long long Sz, T rho, T al,
+                                           int helm, const Coefs<T>& cf, T beta)
+{
+    if (!helm) {
+        T r = dadd(T(0), rho);
+#pragma unroll
+        for (int j = 0; j < ShapeLap7::NT; j++) {
+            const long long o = ShapeLap7::off(j, 0) + Sy * ShapeLap7::off(j, 1) + Sz * ShapeLap7::off(j, 2);
+            r = dadd(r, dmul(cf.c[j], phi[gi + o]));
+        }
+        return r;
+    }
+    T lp = T(0);
+#pragma unroll
+    for (int j = 0; j < ShapeLap7::NT; j++) {
+        const long long o = ShapeLap7::off(j, 0) + Sy * ShapeLap7::off(j, 1) + Sz * ShapeLap7::off(j, 2);
+        lp = dadd(lp, dmul(cf.c[j], phi[gi + o]));
+    }
+    return dsub(rho, dsub(dmul(al, phi[gi]), dmul(beta, lp)));
+}
+
+// coarse right-hand side: AvgDown(2) of the fine residual, children in Box([0,1]^3) order.
+// Block (32, 8): one thread per coarse cell of a (cx, cy) tile; blockIdx.z = cz.
 template <typename T>
 __global__ void __launch_bounds__(256) k_resid_restrict(const T* __restrict__ phi, const T* __restrict__ rhs,
                                                         const T* __restrict__ alpha, T* rhs_c, int nf, int sx, int helm,
                                                         Coefs<T> cf, T beta)
 {
     const int nc = nf / 2;
+    const int cx = blockIdx.x * 32 + threadIdx.x, cy = blockIdx.y * 8 + threadIdx.y, cz = blockIdx.z;
+    if (cx >= nc || cy >= nc) return;
     const long long Sy = sx, Sz = (long long)sx * (nf + 2);
-    const long long total = (long long)nc * nc * nc;
-    const long long stride = (long long)gridDim.x * blockDim.x;
     const T eighth = T(1.0 / 8);
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
-        int cx = (int)(i % nc);
-        long long q = i / nc;
-        int cy = (int)(q % nc), cz = (int)(q / nc);
-        T acc = T(0);
+    T acc = T(0);
 #pragma unroll
-        for (int k = 0; k < 8; k++) {
-            const int fx = 2 * cx + (k & 1), fy = 2 * cy + ((k >> 1) & 1), fz = 2 * cz + (k >> 2);
-            const long long fi = fx + (long long)nf * (fy + (long long)nf * fz);
-            const long long gi = grown_index<T>(nf, sx, fx, fy, fz);
-            T r;
-            if (!helm) {
-                r = dadd(T(0), __ldg(rhs + fi));
-#pragma unroll
-                for (int j = 0; j < ShapeLap7::NT; j++) {
-                    const long long o = ShapeLap7::off(j, 0) + Sy * ShapeLap7::off(j, 1) + Sz * ShapeLap7::off(j, 2);
-                    r = dadd(r, dmul(cf.c[j], __ldg(phi + gi + o)));
-                }
-            } else {
-                T lp = T(0);
-#pragma unroll
-                for (int j = 0; j < ShapeLap7::NT; j++) {
-                    const long long o = ShapeLap7::off(j, 0) + Sy * ShapeLap7::off(j, 1) + Sz * ShapeLap7::off(j, 2);
-                    lp = dadd(lp, dmul(cf.c[j], __ldg(phi + gi + o)));
-                }
-                r = dsub(__ldg(rhs + fi), dsub(dmul(__ldg(alpha + fi), __ldg(phi + gi)), dmul(beta, lp)));
-            }
-            acc = dadd(acc, dmul(eighth, r));
-        }
-        rhs_c[i] = acc;
+    for (int k = 0; k < 8; k++) {
+        const int fx = 2 * cx + (k & 1), fy = 2 * cy + ((k >> 1) & 1), fz = 2 * cz + (k >> 2);
+        const long long fi = fx + (long long)nf * (fy + (long long)nf * fz);
+        const T al = helm ? __ldg(alpha + fi) : T(0);
+        const T r = fine_residual(phi, grown_index<T>(nf, sx, fx, fy, fz), Sy, Sz, __ldg(rhs + fi), al, helm, cf, beta);
+        acc = dadd(acc, dmul(eighth, r));
     }
+    rhs_c[cx + (long long)nc * (cy + (long long)nc * cz)] = acc;
 }
+static inline dim3 restrict_grid(int nf) { return dim3((nf / 2 + 31) / 32, (nf / 2 + 7) / 8, nf / 2); }
 
-// phi += 1.0 * delta_c(p/2) on the valid box, periodic images included
+// phi += 1.0 * delta_c(p/2) on the valid box, periodic images included. Block (32, 8): a thread
+// owns the two fine cells of one coarse cell in x.
 template <typename T>
 __global__ void __launch_bounds__(256) k_prolong(T* phi, const T* __restrict__ delta_c, int nf, int sxf, int sxc)
 {
     const int nc = nf / 2;
-    const long long total = (long long)nf * nf * nf;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
-        int x = (int)(i % nf);
-        long long q = i / nf;
-        int y = (int)(q % nf), z = (int)(q / nf);
-        T d = __ldg(delta_c + grown_index<T>(nc, sxc, x / 2, y / 2, z / 2));
-        T v = dadd(phi[grown_index<T>(nf, sxf, x, y, z)], dmul(T(1), d));
-        store_periodic(phi, nf, sxf, x, y, z, v);
+    const int cx = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
+    if (cx >= nc || y >= nf) return;
+    const T d = delta_c[grown_index<T>(nc, sxc, cx, y / 2, z / 2)];
+    const int ey = edge_code(y, nf), ez = edge_code(z, nf);
+#pragma unroll
+    for (int v = 0; v < 2; v++) {
+        const int x = 2 * cx + v;
+        T* q = phi + grown_index<T>(nf, sxf, x, y, z);
+        store_with_images(phi, nf, sxf, q, edge_code(x, nf), ey, ez, dadd(*q, dmul(T(1), d)));
     }
 }
+static inline dim3 prolong_grid(int nf) { return dim3((nf / 2 + 31) / 32, (nf + 7) / 8, nf); }
 
 // n^3 <-> grown layout with periodic ghost images
 template <typename T>
@@ -455,6 +467,145 @@ __global__ void __launch_bounds__(256) k_avgdown_plain(const T* __restrict__ f, 
     }
 }
 
+
+// ---- coarse levels as one kernel ---------------------------------------------------------------
+// The levels at and below a small edge run their whole part of the V-cycle inside one CTA: every
+// sweep, restriction and prolongation is a block-strided loop followed by __syncthreads, with the
+// same per-cell arithmetic (and the same buffer ping-pong) as the one-launch-per-step path, so the
+// results are identical; only the launches go away.
+constexpr int kMaxCoarse = 8;
+constexpr int kCoarseThreads = 1024;
+template <typename T>
+struct CoarseLevel {
+    T* phi[2];
+    T* rhs;
+    const T* alpha;
+    RelaxCoef<T> k;          // n, sx and the smoother's scalars
+    Coefs<T> crelax;         // L(., omega/6) (Poisson form) or L(., 1/h^2) (Helmholtz form)
+    Coefs<T> cres;           // L(., -1/h^2) (Poisson form) or L(., 1/h^2) (Helmholtz form)
+};
+template <typename T>
+struct CoarseArgs {
+    CoarseLevel<T> lv[kMaxCoarse];   // 0 = coarsest
+    int top;                         // finest level handled here (entered from zero)
+    int nu1, nu2, nu_bottom, direct;
+    const T* ainv;
+    T beta;
+};
+
+template <typename T>
+__device__ void coarse_relax(const CoarseLevel<T>& L, int cur, bool first)
+{
+    const int n = L.k.n, sx = L.k.sx;
+    const long long Sy = sx, Sz = (long long)sx * (n + 2);
+    const T* src = L.phi[cur];
+    T* dst = L.phi[1 - cur];
+    for (int i = threadIdx.x; i < n * n * n; i += blockDim.x) {
+        const int x = i % n, y = (i / n) % n, z = i / (n * n);
+        const T al = L.k.helm ? L.alpha[i] : T(0);
+        T v;
+        if (first) {
+            v = relax_value(L.k, T(0), T(0), L.rhs[i], al);
+        } else {
+            const long long g = grown_index<T>(n, sx, x, y, z);
+            T acc = T(0);
+#pragma unroll
+            for (int j = 0; j < ShapeLap7::NT; j++) {
+                const long long o = ShapeLap7::off(j, 0) + Sy * ShapeLap7::off(j, 1) + Sz * ShapeLap7::off(j, 2);
+                acc = dadd(acc, dmul(L.crelax.c[j], src[g + o]));
+            }
+            v = relax_value(L.k, acc, src[g], L.rhs[i], al);
+        }
+        store_periodic(dst, n, sx, x, y, z, v);
+    }
+    __syncthreads();
+}
+template <typename T>
+__device__ void coarse_zero(const CoarseLevel<T>& L, int cur)
+{
+    const long long m = (long long)L.k.sx * (L.k.n + 2) * (L.k.n + 2);
+    for (long long i = threadIdx.x; i < m; i += blockDim.x) L.phi[cur][i] = T(0);
+    __syncthreads();
+}
+// returns the buffer index holding the result
+template <typename T>
+__device__ int coarse_sweeps(const CoarseLevel<T>& L, int cur, int k, bool zero_start)
+{
+    for (int s = 0; s < k; s++) {
+        coarse_relax(L, cur, zero_start && s == 0);
+        cur = 1 - cur;
+    }
+    if (zero_start && k == 0) coarse_zero(L, cur);
+    return cur;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kCoarseThreads) k_coarse_cycle(const CoarseArgs<T> a)
+{
+    int cur[kMaxCoarse];
+    // down: pre-smoothing from zero, residual restriction
+    for (int l = a.top; l > 0; l--) {
+        const CoarseLevel<T>& L = a.lv[l];
+        CoarseLevel<T> const& C = a.lv[l - 1];
+        cur[l] = coarse_sweeps(L, 0, a.nu1, true);
+        const int nf = L.k.n, nc = nf / 2, sx = L.k.sx;
+        const long long Sy = sx, Sz = (long long)sx * (nf + 2);
+        const T* phi = L.phi[cur[l]];
+        for (int i = threadIdx.x; i < nc * nc * nc; i += blockDim.x) {
+            const int cx = i % nc, cy = (i / nc) % nc, cz = i / (nc * nc);
+            T acc = T(0);
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                const int fx = 2 * cx + (k & 1), fy = 2 * cy + ((k >> 1) & 1), fz = 2 * cz + (k >> 2);
+                const int fi = fx + nf * (fy + nf * fz);
+                const T al = L.k.helm ? L.alpha[fi] : T(0);
+                const T r = fine_residual(phi, grown_index<T>(nf, sx, fx, fy, fz), Sy, Sz, L.rhs[fi], al, L.k.helm,
+                                          L.cres, a.beta);
+                acc = dadd(acc, dmul(T(1.0 / 8), r));
+            }
+            C.rhs[i] = acc;
+        }
+        __syncthreads();
+    }
+    // bottom
+    {
+        const CoarseLevel<T>& B = a.lv[0];
+        if (a.direct) {
+            const int n = B.k.n, N = n * n * n;
+            for (int i = threadIdx.x; i < N; i += blockDim.x) {
+                T acc = T(0);
+                for (int j = 0; j < N; j++) acc = dadd(acc, dmul(a.ainv[(long long)i * N + j], B.rhs[j]));
+                store_periodic(B.phi[0], n, B.k.sx, i % n, (i / n) % n, i / (n * n), acc);
+            }
+            __syncthreads();
+            cur[0] = 0;
+        } else {
+            cur[0] = coarse_sweeps(B, 0, a.nu_bottom, true);
+        }
+    }
+    // up: prolongation, post-smoothing
+    for (int l = 1; l <= a.top; l++) {
+        const CoarseLevel<T>& L = a.lv[l];
+        const CoarseLevel<T>& C = a.lv[l - 1];
+        const int nf = L.k.n, nc = nf / 2;
+        T* phi = L.phi[cur[l]];
+        const T* d = C.phi[cur[l - 1]];
+        for (int i = threadIdx.x; i < nf * nf * nf; i += blockDim.x) {
+            const int x = i % nf, y = (i / nf) % nf, z = i / (nf * nf);
+            const T dv = d[grown_index<T>(nc, C.k.sx, x / 2, y / 2, z / 2)];
+            const long long g = grown_index<T>(nf, L.k.sx, x, y, z);
+            store_periodic(phi, nf, L.k.sx, x, y, z, dadd(phi[g], dmul(T(1), dv)));
+        }
+        __syncthreads();
+        cur[l] = coarse_sweeps(L, cur[l], a.nu2, false);
+    }
+    // leave the result in buffer 0 of the top level
+    if (cur[a.top] == 1) {
+        const CoarseLevel<T>& L = a.lv[a.top];
+        const long long m = (long long)L.k.sx * (L.k.n + 2) * (L.k.n + 2);
+        for (long long i = threadIdx.x; i < m; i += blockDim.x) L.phi[0][i] = L.phi[1][i];
+    }
+}
 
 template <typename T>
 struct MGLevel {
@@ -638,8 +789,17 @@ static int launch_relax_update(pb_mg* mg, MGLevel<float>& L, cudaStream_t st)
     epi.usx = grown_pitch<double>(L.n);
     epi.k = relax_coef(mg, L);
     const double s = is_helm(mg) ? L.hsqinv : mg->p.omega / 6.0;
+    const AuxSpecs lvl = level_aux(mg, L.rhs, L.alpha, L);
+    MGLevel<double> G;
+    G.n = L.n;
+    G.sx = epi.usx;
+    AuxSpecs a = lvl;
+    a.n = lvl.n + 1;
+    a.a[0] = aux_spec(mg->u64, grown_box(G), valid_box(G), 8);
+    a.a[1] = lvl.a[0];
+    a.a[2] = lvl.a[1];
     return launch_star<ShapeLap7>(L.phi[L.cur], grown_box(L), valid_box(L), lap7_coefs<float>(s), epi, st,
-                                  default_star_tune(), level_aux(mg, L.rhs, L.alpha, L));
+                                  default_star_tune(), a);
 }
 
 static int launch_resnorm(pb_mg* mg, MGLevel<double>& L, cudaStream_t st)
@@ -697,6 +857,49 @@ const double* bottom_inverse<double>(const pb_mg* mg) { return mg->ainv64; }
 template <>
 const float* bottom_inverse<float>(const pb_mg* mg) { return mg->ainv32; }
 
+// Coarse levels at or below this edge run as one kernel (0: one launch per step everywhere).
+static int g_coarse_edge = 16;
+
+// Highest level index whose part of the cycle runs as one kernel, or -1.
+static int fused_top(const pb_mg_params& p)
+{
+    if (g_coarse_edge <= 0) return -1;
+    int ft = -1;
+    for (int l = 0; l < p.levels && l < kMaxCoarse; l++)
+        if ((p.n >> (p.levels - l)) <= g_coarse_edge) ft = l;
+    return ft;
+}
+
+template <typename T>
+static int launch_coarse_cycle(pb_mg* mg, std::vector<MGLevel<T>>& lv, int top, cudaStream_t st)
+{
+    CoarseArgs<T> a;
+    memset(&a, 0, sizeof(a));
+    const bool helm = is_helm(mg);
+    for (int l = 0; l <= top; l++) {
+        MGLevel<T>& L = lv[l];
+        CoarseLevel<T>& c = a.lv[l];
+        c.phi[0] = L.phi[0];
+        c.phi[1] = L.phi[1];
+        c.rhs = L.rhs;
+        c.alpha = L.alpha;
+        c.k = relax_coef(mg, L);
+        c.crelax = lap7_coefs<T>(helm ? L.hsqinv : mg->p.omega / 6.0);
+        c.cres = lap7_coefs<T>(helm ? L.hsqinv : -L.hsqinv);
+    }
+    a.top = top;
+    a.nu1 = mg->p.nu1;
+    a.nu2 = mg->p.nu2;
+    a.nu_bottom = mg->p.nu_bottom;
+    a.direct = mg->p.bottom == PB_MG_BOTTOM_DIRECT;
+    a.ainv = bottom_inverse<T>(mg);
+    a.beta = (T)mg->p.beta;
+    k_coarse_cycle<T><<<1, kCoarseThreads, 0, st>>>(a);
+    PB_LAUNCH_CHECK();
+    for (int l = 0; l <= top; l++) lv[l].cur = 0;
+    return PB_OK;
+}
+
 // V-cycle on level l of hierarchy lv. pre_done: the first pre-smoothing sweep already ran (the
 // mixed-precision residual pass does it); fuse_update: the last post-smoothing sweep adds its
 // result to the FP64 solution instead of storing it.
@@ -706,18 +909,17 @@ static int vcycle(pb_mg* mg, std::vector<MGLevel<T>>& lv, int l, bool zero_start
 {
     MGLevel<T>& L = lv[l];
     if (zero_start) L.cur = 0;
+    if (zero_start && l == fused_top(mg->p)) return launch_coarse_cycle(mg, lv, l, st);
     int e;
     if (l > 0) {
         MGLevel<T>& C = lv[l - 1];
         if ((e = relax_sweeps(mg, L, mg->p.nu1 - pre_done, zero_start && !pre_done, st)) != PB_OK) return e;
         const double s = is_helm(mg) ? L.hsqinv : -L.hsqinv;
-        const long long nc3 = (long long)C.n * C.n * C.n;
-        k_resid_restrict<T><<<grid_for(nc3, 256), 256, 0, st>>>(L.phi[L.cur], L.rhs, L.alpha, C.rhs, L.n, L.sx, is_helm(mg),
-                                                                lap7_coefs<T>(s), (T)mg->p.beta);
+        k_resid_restrict<T><<<restrict_grid(L.n), dim3(32, 8), 0, st>>>(L.phi[L.cur], L.rhs, L.alpha, C.rhs, L.n, L.sx,
+                                                                       is_helm(mg), lap7_coefs<T>(s), (T)mg->p.beta);
         PB_LAUNCH_CHECK();
         if ((e = vcycle(mg, lv, l - 1, true, 0, false, st)) != PB_OK) return e;
-        const long long n3 = (long long)L.n * L.n * L.n;
-        k_prolong<T><<<grid_for(n3, 256), 256, 0, st>>>(L.phi[L.cur], C.phi[C.cur], L.n, L.sx, C.sx);
+        k_prolong<T><<<prolong_grid(L.n), dim3(32, 8), 0, st>>>(L.phi[L.cur], C.phi[C.cur], L.n, L.sx, C.sx);
         PB_LAUNCH_CHECK();
         if (!fuse_update) return relax_sweeps(mg, L, mg->p.nu2, false, st);
         if ((e = relax_sweeps(mg, L, mg->p.nu2 - 1, false, st)) != PB_OK) return e;
@@ -1035,10 +1237,20 @@ int pb_mg_launches_per_cycle(const pb_mg_params* p)
     if (params_ok(p) != PB_OK) return -1;
     // levels top..1: nu1 + nu2 sweeps, one restriction, one prolongation; the bottom solve; one norm
     // (mixed: the first pre-sweep and the last post-sweep fuse into the residual and update passes,
-    // and the residual pass replaces the norm)
+    // and the residual pass replaces the norm). Levels at or below the fused edge: one launch.
+    const int per = p->nu1 + p->nu2 + 2;
+    const int mixed = p->precision == PB_MG_MIXED ? 1 : 0;
+    const int ft = fused_top(*p);
+    if (ft >= 0) return (p->levels - ft) * per - mixed + 1 + 1;
     const int bottom = p->bottom == PB_MG_BOTTOM_DIRECT ? 1 : p->nu_bottom;
-    if (p->precision == PB_MG_MIXED) return p->levels * (p->nu1 + p->nu2 + 2) - 1 + bottom + 1;
-    return p->levels * (p->nu1 + p->nu2 + 2) + bottom + 1;
+    return p->levels * per - mixed + bottom + 1;
+}
+
+int pb_mg_coarse_edge(int edge)
+{
+    if (edge < 0) return PB_ERR_ARG;
+    g_coarse_edge = edge;
+    return PB_OK;
 }
 
 } // extern "C"

@@ -114,7 +114,8 @@ __device__ inline void block_max_atomic(double v, double* result)
 }
 
 // Auxiliary per-point fields an epilogue reads (e.g. the right-hand side of a relaxation): up to
-// two, each a field with its own element size and box. In the TMA kernel they travel through the
+// three (Epi::kAux says how many the epilogue reads), each a field with its own element size and
+// box. In the TMA kernel they travel through the
 // same pipeline as the source planes (one tile per output plane) or are read from global memory;
 // in the simple kernel they are read from global memory.
 struct AuxSpec {
@@ -123,14 +124,15 @@ struct AuxSpec {
     int Sx, Sy, Sz;            // extents of the field
     int ox, oy, oz;            // field-local coordinates of index point (0,0,0)
 };
+constexpr int kMaxAux = 3;
 struct AuxSpecs {
     int n;
     int in_smem;               // TMA kernel: 1 stages the tiles through shared memory, 0 reads global memory
-    AuxSpec a[2];
+    AuxSpec a[kMaxAux];
 };
 // What an epilogue sees: per auxiliary field, the address of this point's value.
 struct AuxCtx {
-    const void* p[2];
+    const void* p[kMaxAux];
     template <typename A>
     __device__ __forceinline__ A get(int k) const { return *reinterpret_cast<const A*>(p[k]); }
 };
@@ -168,20 +170,26 @@ __device__ __forceinline__ bool run_phases(F& step, int zo, int nzl)
 template <class S, typename T, int TY, int YB, int XV, class Epi>
 __global__ void __launch_bounds__(kStarTX * (TY / YB) + 32, star_min_blocks(TY, YB, XV))
     k_star_tma(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CUtensorMap amap0,
-               const __grid_constant__ CUtensorMap amap1, const StarGeom g, const AuxSpecs aux, const Coefs<T> cf,
-               const Epi epi_in)
+               const __grid_constant__ CUtensorMap amap1, const __grid_constant__ CUtensorMap amap2,
+               const StarGeom g, const AuxSpecs aux, const Coefs<T> cf, const Epi epi_in)
 {
     using SM = StarSmem<S, T, TY, XV>;
     using AT = AuxTile<TY, XV>;
     constexpr int R = S::R, W = 2 * R + 1;
+    constexpr int NA = Epi::kAux;                     // auxiliary fields the epilogue reads
     constexpr int NCW = kStarTX * (TY / YB) / 32;     // consumer warps
     static_assert(TY % YB == 0, "rows per thread must divide the tile");
+    static_assert(NA <= kMaxAux, "too many auxiliary fields");
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int NST = g.nst;                            // the launcher checks 2R+1 <= NST <= 16
-    const bool aux_sm = aux.in_smem != 0;
-    const int aux_b0 = (aux_sm && aux.n > 0) ? AT::bytes(aux.a[0].esize) : 0;
-    const int aux_b1 = (aux_sm && aux.n > 1) ? AT::bytes(aux.a[1].esize) : 0;
-    const int stage = SM::PLANE + aux_b0 + aux_b1;
+    const bool aux_sm = NA > 0 && aux.in_smem != 0;
+    // byte offset of each auxiliary tile within a stage (aux.n <= NA fields are present)
+    int aoff[kMaxAux + 1];
+    aoff[0] = SM::PLANE;
+#pragma unroll
+    for (int k = 0; k < kMaxAux; k++)
+        aoff[k + 1] = aoff[k] + ((aux_sm && k < NA && k < aux.n) ? AT::bytes(aux.a[k].esize) : 0);
+    const int stage = aoff[NA];
     uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + NST * stage);
     uint64_t* empty = full + NST;
 
@@ -216,22 +224,23 @@ __global__ void __launch_bounds__(kStarTX * (TY / YB) + 32, star_min_blocks(TY, 
                 }
                 unsigned char* st = smem_raw + s * stage;
                 const int zo = q - R;
-                const bool with_aux = aux_sm && aux.n > 0 && zo >= 0 && zo < nzl;
+                const bool with_aux = aux_sm && zo >= 0 && zo < nzl;
                 uint32_t bytes = SM::PLANE_TX;
                 if (with_aux) {
-                    bytes += AT::width(aux.a[0].esize) * TY * aux.a[0].esize;
-                    if (aux.n > 1) bytes += AT::width(aux.a[1].esize) * TY * aux.a[1].esize;
+#pragma unroll
+                    for (int k = 0; k < NA; k++)
+                        if (k < aux.n) bytes += AT::width(aux.a[k].esize) * TY * aux.a[k].esize;
                 }
                 mbar_arrive_expect_tx(&full[s], bytes);
                 tma_load_3d(st, &tmap, &full[s], xs, ys, zs0 + q);
                 if (with_aux) {
-                    const AuxSpec& a0 = aux.a[0];
-                    tma_load_3d(st + SM::PLANE, &amap0, &full[s], a0.ox + x0 - (a0.ox % (16 / a0.esize)), a0.oy + y0,
-                                a0.oz + zb + zo);
-                    if (aux.n > 1) {
-                        const AuxSpec& a1 = aux.a[1];
-                        tma_load_3d(st + SM::PLANE + aux_b0, &amap1, &full[s], a1.ox + x0 - (a1.ox % (16 / a1.esize)),
-                                    a1.oy + y0, a1.oz + zb + zo);
+#pragma unroll
+                    for (int k = 0; k < NA; k++) {
+                        if (k >= aux.n) break;
+                        const AuxSpec& a = aux.a[k];
+                        const CUtensorMap* am = k == 0 ? &amap0 : (k == 1 ? &amap1 : &amap2);
+                        tma_load_3d(st + aoff[k], am, &full[s], a.ox + x0 - (a.ox % (16 / a.esize)), a.oy + y0,
+                                    a.oz + zb + zo);
                     }
                 }
                 if (++s == NST) s = 0;
@@ -258,26 +267,22 @@ __global__ void __launch_bounds__(kStarTX * (TY / YB) + 32, star_min_blocks(TY, 
         rows[r] = epi.row(x, y, zb, xin && (y < g.ny));
     }
     // auxiliary-field address of row r, point v: base + abase + r * arow + v * esize
-    long long abase0, abase1, astep0 = 0, astep1 = 0;
-    int arow0, arow1;
-    const int es0 = aux.a[0].esize, es1 = aux.a[1].esize;
-    {
-        const AuxSpec& a0 = aux.a[0];
-        const AuxSpec& a1 = aux.a[1];
+    long long abase[kMaxAux], astep[kMaxAux];
+    int arow[kMaxAux], es[kMaxAux];
+#pragma unroll
+    for (int k = 0; k < NA; k++) {
+        const AuxSpec& a = aux.a[k];
+        es[k] = a.esize;
+        astep[k] = 0;
         if (aux_sm) {
-            const int w0 = AT::width(a0.esize), w1 = AT::width(a1.esize);
-            abase0 = ((long long)yr0 * w0 + tx * XV + a0.ox % (16 / a0.esize)) * a0.esize;
-            abase1 = ((long long)yr0 * w1 + tx * XV + a1.ox % (16 / a1.esize)) * a1.esize;
-            arow0 = w0 * a0.esize;
-            arow1 = w1 * a1.esize;
+            const int w = AT::width(a.esize);
+            abase[k] = ((long long)yr0 * w + tx * XV + a.ox % (16 / a.esize)) * a.esize;
+            arow[k] = w * a.esize;
         } else {
             const int y = y0 + yr0;
-            abase0 = ((x + a0.ox) + (long long)a0.Sx * ((y + a0.oy) + (long long)a0.Sy * (zb + a0.oz))) * a0.esize;
-            abase1 = ((x + a1.ox) + (long long)a1.Sx * ((y + a1.oy) + (long long)a1.Sy * (zb + a1.oz))) * a1.esize;
-            arow0 = a0.Sx * a0.esize;
-            arow1 = a1.Sx * a1.esize;
-            astep0 = (long long)a0.Sx * a0.Sy * a0.esize;
-            astep1 = (long long)a1.Sx * a1.Sy * a1.esize;
+            abase[k] = ((x + a.ox) + (long long)a.Sx * ((y + a.oy) + (long long)a.Sy * (zb + a.oz))) * a.esize;
+            arow[k] = a.Sx * a.esize;
+            astep[k] = (long long)a.Sx * a.Sy * a.esize;
         }
     }
     T win[YB][XV][W];
@@ -315,18 +320,18 @@ __global__ void __launch_bounds__(kStarTX * (TY / YB) + 32, star_min_blocks(TY, 
             for (int v = 0; v < XV; v++) win[r][v][IN] = pnew[sc0 + r * SM::BX + v];
         const unsigned char* stc = smem_raw + scs * stage;
         const T* pc = reinterpret_cast<const T*>(stc);
-        const unsigned char* ab0 =
-            (aux_sm ? stc + SM::PLANE : reinterpret_cast<const unsigned char*>(aux.a[0].base) + zo * astep0) + abase0;
-        const unsigned char* ab1 =
-            (aux_sm ? stc + SM::PLANE + aux_b0 : reinterpret_cast<const unsigned char*>(aux.a[1].base) + zo * astep1) +
-            abase1;
+        const unsigned char* ab[kMaxAux];
+#pragma unroll
+        for (int k = 0; k < NA; k++)
+            ab[k] = (aux_sm ? stc + aoff[k] : reinterpret_cast<const unsigned char*>(aux.a[k].base) + zo * astep[k]) +
+                    abase[k];
 #pragma unroll
         for (int r = 0; r < YB; r++) {
 #pragma unroll
             for (int v = 0; v < XV; v++) {
                 AuxCtx ax;
-                ax.p[0] = ab0 + r * arow0 + v * es0;
-                ax.p[1] = ab1 + r * arow1 + v * es1;
+#pragma unroll
+                for (int k = 0; k < NA; k++) ax.p[k] = ab[k] + r * arow[k] + v * es[k];
                 T acc = epi.init(rows[r], zo, v, ax);
 #pragma unroll
                 for (int j = 0; j < S::NT; j++) {
@@ -380,10 +385,12 @@ __global__ void __launch_bounds__(256) k_star_simple(const T* __restrict__ src, 
         int z = (int)(r / g.ny);
         long long base = (x + g.ox) + Sx * (y + g.oy) + Sxy * (z + g.oz);
         AuxCtx ax;
-        ax.p[0] = reinterpret_cast<const unsigned char*>(aux.a[0].base) +
-                  ((x + aux.a[0].ox) + (long long)aux.a[0].Sx * ((y + aux.a[0].oy) + (long long)aux.a[0].Sy * (z + aux.a[0].oz))) * aux.a[0].esize;
-        ax.p[1] = reinterpret_cast<const unsigned char*>(aux.a[1].base) +
-                  ((x + aux.a[1].ox) + (long long)aux.a[1].Sx * ((y + aux.a[1].oy) + (long long)aux.a[1].Sy * (z + aux.a[1].oz))) * aux.a[1].esize;
+#pragma unroll
+        for (int k = 0; k < Epi::kAux; k++) {
+            const AuxSpec& a = aux.a[k];
+            ax.p[k] = reinterpret_cast<const unsigned char*>(a.base) +
+                      ((x + a.ox) + (long long)a.Sx * ((y + a.oy) + (long long)a.Sy * (z + a.oz))) * a.esize;
+        }
         const typename Epi::Row row = epi.row(x, y, z, true);
         T acc = epi.init(row, 0, 0, ax);
 #pragma unroll
@@ -403,6 +410,7 @@ __global__ void __launch_bounds__(256) k_star_simple(const T* __restrict__ src, 
 // Epilogue interface (both kernels):
 //   Row                      per-row cursor type
 //   kZEdge                   whether some planes need separate handling (then z_edge(z) says which)
+//   kAux                     how many auxiliary fields init/finish read (AuxCtx::get<A>(k), k < kAux)
 //   row(x, y, z0, active)    cursor of the row of points x .. x+XV-1 at y, starting at plane z0
 //   init(row, zo, v, ax)     accumulator start for point v of the row at plane z0+zo
 //   finish<ZE>(row, zo, v, acc, c, ax)   consume the stencil sum (c = the source's centre value)
@@ -428,6 +436,7 @@ struct EpiStore {
     int accumulate;
     using Row = OutRow<T>;
     static constexpr bool kZEdge = false;
+    static constexpr int kAux = 0;
     __device__ __forceinline__ Row row(int x, int y, int z0, bool active) const { return Row{dst + m.at(x, y, z0), active}; }
     __device__ __forceinline__ T init(const Row& r, int zo, int v, const AuxCtx&) const
     {
@@ -452,6 +461,7 @@ struct EpiAxpby {
     int euler;
     using Row = OutRow<T>;
     static constexpr bool kZEdge = false;
+    static constexpr int kAux = 0;
     __device__ __forceinline__ Row row(int x, int y, int z0, bool active) const { return Row{dst + m.at(x, y, z0), active}; }
     __device__ __forceinline__ T init(const Row&, int, int, const AuxCtx&) const { return T(0); }
     template <bool ZE>

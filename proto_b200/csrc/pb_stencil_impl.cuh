@@ -71,7 +71,7 @@ int launch_star_tma(const T* src, StarGeom g, const Coefs<T>& cf, const Epi& epi
     using AT = AuxTile<TY, XV>;
     if (XV > 1 && g.nx % XV != 0) return PB_ERR_ARG;
     g.pad = (g.ox - R) % EV;
-    CUtensorMap map, amap[2];
+    CUtensorMap map, amap[kMaxAux];
     int e = encode_tmap_3d(&map, src, (int)sizeof(T), g.Sx, g.Sy, g.Sz, SM::BX, SM::BY, 1);
     if (e != PB_OK) return e;
     memset(amap, 0, sizeof(amap));
@@ -133,7 +133,7 @@ int launch_star_tma(const T* src, StarGeom g, const Coefs<T>& cf, const Epi& epi
     if (zc > g.nz) zc = g.nz;
     g.zc = zc;
     dim3 grid((g.nx + SM::TXW - 1) / SM::TXW, (g.ny + TY - 1) / TY, (g.nz + zc - 1) / zc);
-    kern<<<grid, NTHR, smem, st>>>(map, amap[0], amap[1], g, aux, cf, epi);
+    kern<<<grid, NTHR, smem, st>>>(map, amap[0], amap[1], amap[2], g, aux, cf, epi);
     PB_LAUNCH_CHECK();
     return PB_OK;
 }
@@ -155,8 +155,9 @@ int launch_star(const T* src, const Box3& srcBox, const Box3& ib, const Coefs<T>
     g.zc = g.nz;
     g.pad = 0;
     g.nst = 0;
+    if (aux.n > Epi::kAux) return PB_ERR_ARG;
     // unused auxiliary slots point at something harmless (their addresses are formed, never read)
-    for (int k = aux.n; k < 2; k++) {
+    for (int k = aux.n; k < kMaxAux; k++) {
         aux.a[k] = AuxSpec{};
         aux.a[k].base = src;
         aux.a[k].esize = (int)sizeof(T);

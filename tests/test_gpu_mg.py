@@ -134,3 +134,27 @@ def test_levels_zero_direct_is_exact(pb, port):
     n2, h2 = port.mg_cs(N, 0, 4, 4, 10, 2.0 / 3.0, 1.0, None, 3, 1e-10, rho.reshape(-1).copy(), p2, bottom=1)
     assert it == n2 and hist == list(h2)
     assert np.array_equal(phi, p2)
+
+
+@pytest.mark.parametrize("edge", [0, 16, 32])
+def test_coarse_levels_as_one_kernel_bitwise(pb, port, edge):
+    """Coarse levels run as one single-CTA kernel (edge 16, 32) or one launch per step (0): the
+    same arithmetic either way, so the history and solution are bitwise the C port's."""
+    L = pb.lib()
+    N, lev = 64, 4
+    alpha = W.helmholtz_alpha(N, seed=3)
+    rhs = -W.poisson_rho(N, seed=1)
+    try:
+        assert L.pb_mg_coarse_edge(edge) == 0
+        it, hist, phi = _gpu_solve(pb, N, lev, pb.MG_FP64, max_iter=8, alpha=alpha, rhs=rhs, bottom=1)
+        it2, hist2, phi2 = _gpu_solve(pb, N, lev, pb.MG_FP64, max_iter=8)
+    finally:
+        L.pb_mg_coarse_edge(16)
+    p1 = np.zeros(N ** 3)
+    n1, h1 = port.mg_cs(N, lev, 4, 4, 10, 2.0 / 3.0, 1.0, alpha.reshape(-1).copy(), 8, 1e-10,
+                        rhs.reshape(-1).copy(), p1, bottom=1)
+    assert it == n1 and hist == list(h1) and np.array_equal(phi, p1)
+    p2 = np.zeros(N ** 3)
+    n2, h2 = port.mg_cs(N, lev, 4, 4, 10, 2.0 / 3.0, 1.0, None, 8, 1e-10,
+                        W.poisson_rho(N, seed=1).reshape(-1).copy(), p2)
+    assert it2 == n2 and hist2 == list(h2) and np.array_equal(phi2, p2)

@@ -75,9 +75,10 @@ int pb_stencil_apply_f32(const pb_stencil* s, const float* src, pb_box src_box,
  * above min_tma_points cells, one thread per point below), 1 forces the TMA kernel, 2 the
  * one-thread-per-point kernel; zc is the z extent per CTA (0: chosen from the occupancy so that
  * whole waves of CTAs fill the SMs); ty the CTA tile height, yb the rows and xv the adjacent x
- * points each consumer thread computes: (ty, yb, xv) one of (8,1,1), (8,2,1), (8,2,2), (4,2,2)
- * (xv = 2 applies to boxes of even x extent; others use xv = 1). min_tma_points < 0 keeps the
- * current threshold. */
+ * points each consumer thread computes: (ty, yb, xv) one of (8,1,1), (8,2,1), (8,2,2), (4,2,2),
+ * or (8,2,0), the default, which uses xv = 1 for Stencil::apply and xv = 2 for the multigrid
+ * sweeps (xv = 2 applies to boxes of even x extent; others use xv = 1). min_tma_points < 0 keeps
+ * the current threshold. */
 int pb_star_tune_set(int mode, int zc, int ty, int yb, int xv, long long min_tma_points);
 /* Depth of the TMA kernel's shared-memory ring (0: up to 2R+4 planes, as deep as two CTAs per SM
  * allow; else 2R+1..16) and whether

@@ -491,6 +491,36 @@ struct CoarseArgs {
     int nu1, nu2, nu_bottom, direct;
     const T* ainv;
     T beta;
+    int in_smem;                     // 1: the levels live in shared memory during the cycle
+};
+
+// Shared-memory arena of the coarse cycle: per level two grown buffers, rho and (Helmholtz)
+// alpha, each 16-byte aligned. Returns the bytes needed; fills the element offsets when asked.
+template <typename T>
+static size_t coarse_smem_layout(const CoarseArgs<T>& a, int helm, long long (*off)[4])
+{
+    size_t total = 0;
+    auto take = [&](size_t elems) {
+        const size_t o = total;
+        total += (elems * sizeof(T) + 15) / 16 * 16;
+        return (long long)(o / sizeof(T));
+    };
+    for (int l = 0; l <= a.top; l++) {
+        const CoarseLevel<T>& L = a.lv[l];
+        const size_t g = (size_t)L.k.sx * (L.k.n + 2) * (L.k.n + 2), c = (size_t)L.k.n * L.k.n * L.k.n;
+        const long long o0 = take(g), o1 = take(g), o2 = take(c), o3 = helm ? take(c) : -1;
+        if (off) {
+            off[l][0] = o0;
+            off[l][1] = o1;
+            off[l][2] = o2;
+            off[l][3] = o3;
+        }
+    }
+    return total;
+}
+
+struct CoarseOffsets {
+    long long o[kMaxCoarse][4];      // element offsets of phi0, phi1, rho, alpha per level
 };
 
 template <typename T>
@@ -540,13 +570,42 @@ __device__ int coarse_sweeps(const CoarseLevel<T>& L, int cur, int k, bool zero_
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kCoarseThreads) k_coarse_cycle(const CoarseArgs<T> a)
+__global__ void __launch_bounds__(kCoarseThreads) k_coarse_cycle(const CoarseArgs<T> ga, const CoarseOffsets off)
 {
+    extern __shared__ __align__(16) unsigned char coarse_smem[];
+    // level descriptors, shared by the block (in shared-memory mode they point into the arena)
+    __shared__ CoarseLevel<T> lvs[kMaxCoarse];
+    if (threadIdx.x == 0) {
+        T* base = reinterpret_cast<T*>(coarse_smem);
+        for (int l = 0; l <= ga.top; l++) {
+            CoarseLevel<T> L = ga.lv[l];
+            if (ga.in_smem) {
+                L.phi[0] = base + off.o[l][0];
+                L.phi[1] = base + off.o[l][1];
+                L.rhs = base + off.o[l][2];
+                if (L.k.helm) L.alpha = base + off.o[l][3];
+            }
+            lvs[l] = L;
+        }
+    }
+    __syncthreads();
+    if (ga.in_smem) {
+        // rho of the entry level and every alpha come in
+        for (int l = 0; l <= ga.top; l++) {
+            const int n3 = ga.lv[l].k.n * ga.lv[l].k.n * ga.lv[l].k.n;
+            if (l == ga.top)
+                for (int i = threadIdx.x; i < n3; i += blockDim.x) lvs[l].rhs[i] = ga.lv[l].rhs[i];
+            if (ga.lv[l].k.helm)
+                for (int i = threadIdx.x; i < n3; i += blockDim.x) const_cast<T*>(lvs[l].alpha)[i] = ga.lv[l].alpha[i];
+        }
+        __syncthreads();
+    }
+    const CoarseArgs<T>& a = ga;
     int cur[kMaxCoarse];
     // down: pre-smoothing from zero, residual restriction
     for (int l = a.top; l > 0; l--) {
-        const CoarseLevel<T>& L = a.lv[l];
-        CoarseLevel<T> const& C = a.lv[l - 1];
+        const CoarseLevel<T>& L = lvs[l];
+        CoarseLevel<T> const& C = lvs[l - 1];
         cur[l] = coarse_sweeps(L, 0, a.nu1, true);
         const int nf = L.k.n, nc = nf / 2, sx = L.k.sx;
         const long long Sy = sx, Sz = (long long)sx * (nf + 2);
@@ -569,7 +628,7 @@ __global__ void __launch_bounds__(kCoarseThreads) k_coarse_cycle(const CoarseArg
     }
     // bottom
     {
-        const CoarseLevel<T>& B = a.lv[0];
+        const CoarseLevel<T>& B = lvs[0];
         if (a.direct) {
             const int n = B.k.n, N = n * n * n;
             for (int i = threadIdx.x; i < N; i += blockDim.x) {
@@ -585,8 +644,8 @@ __global__ void __launch_bounds__(kCoarseThreads) k_coarse_cycle(const CoarseArg
     }
     // up: prolongation, post-smoothing
     for (int l = 1; l <= a.top; l++) {
-        const CoarseLevel<T>& L = a.lv[l];
-        const CoarseLevel<T>& C = a.lv[l - 1];
+        const CoarseLevel<T>& L = lvs[l];
+        const CoarseLevel<T>& C = lvs[l - 1];
         const int nf = L.k.n, nc = nf / 2;
         T* phi = L.phi[cur[l]];
         const T* d = C.phi[cur[l - 1]];
@@ -599,11 +658,12 @@ __global__ void __launch_bounds__(kCoarseThreads) k_coarse_cycle(const CoarseArg
         __syncthreads();
         cur[l] = coarse_sweeps(L, cur[l], a.nu2, false);
     }
-    // leave the result in buffer 0 of the top level
-    if (cur[a.top] == 1) {
-        const CoarseLevel<T>& L = a.lv[a.top];
+    // leave the result in buffer 0 of the top level (in global memory)
+    if (a.in_smem || cur[a.top] == 1) {
+        const CoarseLevel<T>& L = lvs[a.top];
         const long long m = (long long)L.k.sx * (L.k.n + 2) * (L.k.n + 2);
-        for (long long i = threadIdx.x; i < m; i += blockDim.x) L.phi[0][i] = L.phi[1][i];
+        const T* src = L.phi[cur[a.top]];
+        for (long long i = threadIdx.x; i < m; i += blockDim.x) ga.lv[a.top].phi[0][i] = src[i];
     }
 }
 
@@ -774,7 +834,7 @@ static int launch_relax(pb_mg* mg, MGLevel<T>& L, bool first, cudaStream_t st)
         epi.k = k;
         const double s = is_helm(mg) ? L.hsqinv : mg->p.omega / 6.0;
         int e = launch_star<ShapeLap7>(L.phi[L.cur], grown_box(L), valid_box(L), lap7_coefs<T>(s), epi, st,
-                                       default_star_tune(), level_aux(mg, L.rhs, L.alpha, L));
+                                       default_star_tune(), level_aux(mg, L.rhs, L.alpha, L), 2);
         if (e != PB_OK) return e;
     }
     L.cur = 1 - L.cur;
@@ -799,7 +859,7 @@ static int launch_relax_update(pb_mg* mg, MGLevel<float>& L, cudaStream_t st)
     a.a[1] = lvl.a[0];
     a.a[2] = lvl.a[1];
     return launch_star<ShapeLap7>(L.phi[L.cur], grown_box(L), valid_box(L), lap7_coefs<float>(s), epi, st,
-                                  default_star_tune(), a);
+                                  default_star_tune(), a, 2);
 }
 
 static int launch_resnorm(pb_mg* mg, MGLevel<double>& L, cudaStream_t st)
@@ -811,7 +871,7 @@ static int launch_resnorm(pb_mg* mg, MGLevel<double>& L, cudaStream_t st)
     epi.result = mg->d_res;
     epi.m = 0.0;
     return launch_star<ShapeLap7>(L.phi[L.cur], grown_box(L), valid_box(L), lap7_coefs<double>(L.hsqinv), epi, st,
-                                  default_star_tune(), level_aux(mg, L.rhs, L.alpha, L));
+                                  default_star_tune(), level_aux(mg, L.rhs, L.alpha, L), 2);
 }
 
 // MIXED: FP64 residual of u64 + norm + FP32 right-hand side + first FP32 sweep of the finest level
@@ -834,7 +894,7 @@ static int launch_res64(pb_mg* mg, cudaStream_t st)
     G.hsqinv = L.hsqinv;
     const double s = is_helm(mg) ? L.hsqinv : -L.hsqinv;
     int e = launch_star<ShapeLap7>((const double*)mg->u64, grown_box(G), valid_box(G), lap7_coefs<double>(s), epi, st,
-                                   default_star_tune(), level_aux(mg, (const double*)mg->f64, (const double*)mg->alpha64, G));
+                                   default_star_tune(), level_aux(mg, (const double*)mg->f64, (const double*)mg->alpha64, G), 2);
     L.cur = 1;
     return e;
 }
@@ -894,7 +954,16 @@ static int launch_coarse_cycle(pb_mg* mg, std::vector<MGLevel<T>>& lv, int top, 
     a.direct = mg->p.bottom == PB_MG_BOTTOM_DIRECT;
     a.ainv = bottom_inverse<T>(mg);
     a.beta = (T)mg->p.beta;
-    k_coarse_cycle<T><<<1, kCoarseThreads, 0, st>>>(a);
+    CoarseOffsets off;
+    memset(&off, 0, sizeof(off));
+    const size_t smem = coarse_smem_layout(a, helm, off.o);
+    static bool attr = false;
+    if (!attr) {
+        PB_CUDA(cudaFuncSetAttribute(k_coarse_cycle<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+        attr = true;
+    }
+    a.in_smem = smem <= 216 * 1024 ? 1 : 0;   // the descriptor table takes a little static shared memory
+    k_coarse_cycle<T><<<1, kCoarseThreads, a.in_smem ? smem : 0, st>>>(a, off);
     PB_LAUNCH_CHECK();
     for (int l = 0; l <= top; l++) lv[l].cur = 0;
     return PB_OK;

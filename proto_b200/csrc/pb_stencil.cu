@@ -172,10 +172,11 @@ StarTune& default_star_tune() { return g_default_tune; }
 
 // Launch-shape knobs of the star kernels (used by the autotuner and by profiling sweeps):
 // mode 0 auto / 1 TMA only / 2 simple only; zc z-chunk (0 heuristic); (ty, yb, xv) CTA tile height,
-// rows per consumer thread and adjacent x points per consumer thread.
+// rows per consumer thread and adjacent x points per consumer thread (xv 0: one point per thread
+// for Stencil::apply, two for the multigrid sweeps).
 extern "C" int pb_star_tune_set(int mode, int zc, int ty, int yb, int xv, long long min_tma_points)
 {
-    const bool shape_ok = (ty == 8 && yb == 1 && xv == 1) || (ty == 8 && yb == 2 && (xv == 1 || xv == 2)) ||
+    const bool shape_ok = (ty == 8 && yb == 1 && xv == 1) || (ty == 8 && yb == 2 && xv >= 0 && xv <= 2) ||
                           (ty == 4 && yb == 2 && xv == 2);
     if (mode < 0 || mode > 2 || zc < 0 || !shape_ok) return PB_ERR_ARG;
     pb::StarTune& t = pb::default_star_tune();

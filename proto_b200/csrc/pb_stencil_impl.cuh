@@ -26,8 +26,9 @@ struct StarTune {
     int zc = 0;                          // z chunk per CTA; 0 = occupancy-based heuristic
     int ty = 8;                          // CTA tile height
     int yb = 2;                          // rows per consumer thread
-    int xv = 2;                          // adjacent x points per consumer thread; (ty, yb, xv) in
-                                         // {(8,1,1), (8,2,1), (8,2,2), (4,2,2)}
+    int xv = 0;                          // adjacent x points per consumer thread; (ty, yb, xv) in
+                                         // {(8,1,1), (8,2,1), (8,2,2), (4,2,2)}; 0 = the caller's
+                                         // default with ty 8, yb 2
     int nst = 0;                         // ring depth; 0 = as deep as two CTAs per SM allow (<= 2R+4)
     int aux_smem = 1;                    // stage auxiliary fields through shared memory by TMA
 };
@@ -140,7 +141,7 @@ int launch_star_tma(const T* src, StarGeom g, const Coefs<T>& cf, const Epi& epi
 
 template <class S, typename T, class Epi>
 int launch_star(const T* src, const Box3& srcBox, const Box3& ib, const Coefs<T>& cf, const Epi& epi,
-                cudaStream_t st, const StarTune& tune, AuxSpecs aux = no_aux())
+                cudaStream_t st, const StarTune& tune, AuxSpecs aux = no_aux(), int xv_default = 1)
 {
     StarGeom g;
     g.nx = (int)bsize(ib, 0);
@@ -169,7 +170,8 @@ int launch_star(const T* src, const Box3& srcBox, const Box3& ib, const Coefs<T>
     if (tune.mode == StarTune::TMA) use_tma = g.ox >= S::R && tma_available();
     if (use_tma) {
         int e;
-        const bool pairs = tune.xv == 2 && g.nx % 2 == 0;   // two x points per thread need an even extent
+        const int xv = tune.xv ? tune.xv : xv_default;
+        const bool pairs = xv == 2 && g.nx % 2 == 0;         // two x points per thread need an even extent
         if (pairs && tune.ty == 4) e = launch_star_tma<S, T, 4, 2, 2>(src, g, cf, epi, st, tune.zc, aux, tune.nst);
         else if (pairs) e = launch_star_tma<S, T, 8, 2, 2>(src, g, cf, epi, st, tune.zc, aux, tune.nst);
         else if (tune.yb == 1) e = launch_star_tma<S, T, 8, 1, 1>(src, g, cf, epi, st, tune.zc, aux, tune.nst);

@@ -136,12 +136,13 @@ def test_levels_zero_direct_is_exact(pb, port):
     assert np.array_equal(phi, p2)
 
 
-@pytest.mark.parametrize("edge", [0, 16, 32])
-def test_coarse_levels_as_one_kernel_bitwise(pb, port, edge):
-    """Coarse levels run as one single-CTA kernel (edge 16, 32) or one launch per step (0): the
-    same arithmetic either way, so the history and solution are bitwise the C port's."""
+@pytest.mark.parametrize("edge,lev", [(0, 4), (16, 4), (32, 4), (8, 3), (16, 3)])
+def test_coarse_levels_as_one_kernel_bitwise(pb, port, edge, lev):
+    """Coarse levels run as one single-CTA kernel (edge 8..32; coarsest 4^3 or 8^3, exact or
+    relaxed bottom) or one launch per step (0): the same arithmetic either way, so the history
+    and solution are bitwise the C port's."""
     L = pb.lib()
-    N, lev = 64, 4
+    N = 64
     alpha = W.helmholtz_alpha(N, seed=3)
     rhs = -W.poisson_rho(N, seed=1)
     try:

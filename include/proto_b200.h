@@ -215,6 +215,49 @@ int pb_mg_launches_per_cycle(const pb_mg_params* p);
  * 0 turns this off. Default 16. Applies to solvers created and cycles captured afterwards. */
 int pb_mg_coarse_edge(int edge);
 
+/* ---- Serving engine (no counterpart in the reference, which solves one grid at a time) ----------
+ * Periodic Poisson/Helmholtz solves of different edges, solved together: each admitted solve keeps
+ * its hierarchy on the device; one pb_serve_step runs one mixed-precision V-cycle (FP32 cycle,
+ * FP64 residual, correction and norm) for every in-flight solve, each cycle phase one launch for
+ * all of them, the whole step one CUDA graph. Solves are admitted between steps while slots and
+ * the HBM budget allow, and retired when their max-norm residual drops below tol times the first
+ * one. Per solve the arithmetic is pb_mg's PB_MG_MIXED solver's (constant alpha, levels = every
+ * halving, bottom = nu_bottom sweeps), so each result is the same alone and in any mix.
+ * An edge must halve down to <= 16 (n = m * 2^k with m <= 16). */
+enum { PB_SERVE_WAITING = 0, PB_SERVE_ACTIVE = 1, PB_SERVE_DONE = 2, PB_SERVE_FAILED = 3 };
+typedef struct {
+    long long hbm_budget;   /* bytes of solver hierarchies the engine may hold                     */
+    int max_active;         /* solves in flight (1..256)                                           */
+    int nu1, nu2, nu_bottom;
+    double omega;
+    double tol;             /* relative max-norm residual                                          */
+    int max_cycles;         /* a solve still above tol after this many cycles is retired as failed */
+} pb_serve_params;
+typedef struct {
+    int n;                  /* edge                                                                */
+    int form;               /* PB_MG_POISSON (L_h u = rhs) / PB_MG_HELMHOLTZ (alpha u - beta L_h u = rhs) */
+    double alpha, beta;     /* Helmholtz scalars                                                   */
+    const double* rhs;      /* host, n^3 (x fastest); read when the solve is admitted              */
+    double* out;            /* host, n^3; receives the solution (initial guess zero)               */
+} pb_serve_request;
+typedef struct pb_serve pb_serve;
+int pb_serve_create(const pb_serve_params* p, pb_serve** out);
+int pb_serve_destroy(pb_serve* sv);
+/* Queues a request; rhs and out must stay valid until its ticket completes. PB_ERR_BUDGET if one
+ * solve of this edge alone exceeds the budget. */
+int pb_serve_submit(pb_serve* sv, const pb_serve_request* q, long long* ticket);
+/* Admits what fits, runs one cycle for every in-flight solve, retires the finished ones (their
+ * results are in their out buffers when this returns). active / waiting may be NULL. */
+int pb_serve_step(pb_serve* sv, int* active, int* waiting);
+/* Tickets completed since the last poll (up to cap). */
+int pb_serve_poll(pb_serve* sv, long long* tickets, int cap, int* n);
+/* state PB_SERVE_*, cycles run, last relative residual. */
+int pb_serve_status(const pb_serve* sv, long long ticket, int* state, int* cycles, double* rel_res);
+/* Bytes of hierarchies held (in use and cached for reuse). */
+long long pb_serve_device_bytes(const pb_serve* sv);
+/* Bytes one solve of edge n holds (-1 if n is not servable). */
+long long pb_serve_request_bytes(int n);
+
 #ifdef __cplusplus
 }
 #endif

@@ -16,6 +16,7 @@ __all__ = ["ProtoError", "lib", "Box", "Stencil", "Level", "Multigrid", "MGParam
            "interp_constant", "device_check", "OP_ADD", "OP_SUB", "OP_MUL", "OP_DIV", "OP_ASSIGN",
            "RED_MAX", "RED_MIN", "RED_ABS", "RED_SUM", "RED_SUMABS", "RED_SUMSQ", "EPI_AXPBY", "EPI_EULER",
            "MG_POISSON", "MG_HELMHOLTZ", "MG_FP64", "MG_MIXED", "MG_BOTTOM_RELAX", "MG_BOTTOM_DIRECT",
+           "Serve", "SERVE_WAITING", "SERVE_ACTIVE", "SERVE_DONE", "SERVE_FAILED",
            "header_functions"]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -28,6 +29,7 @@ EPI_AXPBY, EPI_EULER = 1, 2
 MG_POISSON, MG_HELMHOLTZ = 0, 1
 MG_FP64, MG_MIXED = 0, 1
 MG_BOTTOM_RELAX, MG_BOTTOM_DIRECT = 0, 1
+SERVE_WAITING, SERVE_ACTIVE, SERVE_DONE, SERVE_FAILED = 0, 1, 2, 3
 
 _c_int, _c_dbl, _c_flt, _vp, _c_ll = ctypes.c_int, ctypes.c_double, ctypes.c_float, ctypes.c_void_p, ctypes.c_longlong
 
@@ -40,6 +42,15 @@ class pb_mg_params(ctypes.Structure):
     _fields_ = [("n", _c_int), ("levels", _c_int), ("nu1", _c_int), ("nu2", _c_int), ("nu_bottom", _c_int),
                 ("omega", _c_dbl), ("beta", _c_dbl), ("form", _c_int), ("precision", _c_int),
                 ("max_iter", _c_int), ("tol", _c_dbl), ("bottom", _c_int)]
+
+
+class pb_serve_params(ctypes.Structure):
+    _fields_ = [("hbm_budget", _c_ll), ("max_active", _c_int), ("nu1", _c_int), ("nu2", _c_int),
+                ("nu_bottom", _c_int), ("omega", _c_dbl), ("tol", _c_dbl), ("max_cycles", _c_int)]
+
+
+class pb_serve_request(ctypes.Structure):
+    _fields_ = [("n", _c_int), ("form", _c_int), ("alpha", _c_dbl), ("beta", _c_dbl), ("rhs", _vp), ("out", _vp)]
 
 
 class ProtoError(RuntimeError):
@@ -66,6 +77,10 @@ def lib():
         L.pb_mg_device_bytes.restype = _c_ll
         L.pb_mg_device_bytes.argtypes = [ctypes.POINTER(pb_mg_params)]
         L.pb_mg_launches_per_cycle.argtypes = [ctypes.POINTER(pb_mg_params)]
+        L.pb_serve_device_bytes.restype = _c_ll
+        L.pb_serve_request_bytes.restype = _c_ll
+        L.pb_serve_status.argtypes = [_vp, _c_ll, ctypes.POINTER(_c_int), ctypes.POINTER(_c_int),
+                                      ctypes.POINTER(_c_dbl)]
         for name in ("pb_stencil_apply_f64", "pb_stencil_apply_f32", "pb_stencil_apply_fused_f64",
                      "pb_boxdata_op_f64", "pb_boxdata_scalar_f64", "pb_boxdata_copy_f64", "pb_forall_axpby_f64",
                      "pb_reduce_f64", "pb_reduce_async_f64", "pb_interp_constant_f64"):
@@ -314,4 +329,68 @@ class Multigrid:
     def __del__(self):
         if getattr(self, "_h", None) and _LIB is not None:
             _LIB.pb_mg_destroy(self._h)
+            self._h = None
+
+
+class Serve:
+    """Serving engine (pb_serve_*): in-flight solves advance together, one V-cycle per step.
+
+    Requests carry host numpy float64 arrays (rhs read at admission, out written at completion);
+    the engine keeps references until the request completes."""
+
+    def __init__(self, hbm_budget, max_active=64, nu1=4, nu2=4, nu_bottom=10, omega=2.0 / 3.0, tol=1e-8,
+                 max_cycles=100):
+        self.params = pb_serve_params(int(hbm_budget), max_active, nu1, nu2, nu_bottom, omega, tol, max_cycles)
+        h = _vp()
+        _check(lib().pb_serve_create(ctypes.byref(self.params), ctypes.byref(h)), "pb_serve_create")
+        self._h = h
+        self._keep = {}
+
+    @staticmethod
+    def request_bytes(n):
+        return lib().pb_serve_request_bytes(_c_int(n))
+
+    def submit(self, n, rhs, out, form=MG_POISSON, alpha=0.0, beta=1.0):
+        import numpy as np
+        assert rhs.dtype == np.float64 and out.dtype == np.float64 and rhs.size == n ** 3 and out.size == n ** 3
+        assert rhs.flags["C_CONTIGUOUS"] and out.flags["C_CONTIGUOUS"]
+        q = pb_serve_request(n, form, alpha, beta, rhs.ctypes.data, out.ctypes.data)
+        t = _c_ll()
+        _check(lib().pb_serve_submit(self._h, ctypes.byref(q), ctypes.byref(t)), "pb_serve_submit")
+        self._keep[t.value] = (rhs, out)
+        return t.value
+
+    def step(self):
+        a, w = _c_int(), _c_int()
+        _check(lib().pb_serve_step(self._h, ctypes.byref(a), ctypes.byref(w)), "pb_serve_step")
+        return a.value, w.value
+
+    def poll(self, cap=4096):
+        buf = (_c_ll * cap)()
+        n = _c_int()
+        _check(lib().pb_serve_poll(self._h, buf, _c_int(cap), ctypes.byref(n)), "pb_serve_poll")
+        done = [buf[i] for i in range(n.value)]
+        for t in done:
+            self._keep.pop(t, None)
+        return done
+
+    def status(self, ticket):
+        st, cy, rr = _c_int(), _c_int(), _c_dbl()
+        _check(lib().pb_serve_status(self._h, _c_ll(ticket), ctypes.byref(st), ctypes.byref(cy), ctypes.byref(rr)),
+               "pb_serve_status")
+        return st.value, cy.value, rr.value
+
+    def device_bytes(self):
+        return lib().pb_serve_device_bytes(self._h)
+
+    def run_until_idle(self, max_steps=100000):
+        for _ in range(max_steps):
+            a, w = self.step()
+            if a == 0 and w == 0:
+                return
+        raise RuntimeError("serve: not idle after %d steps" % max_steps)
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _LIB is not None:
+            _LIB.pb_serve_destroy(self._h)
             self._h = None

@@ -24,648 +24,12 @@
 #include <vector>
 
 #include "pb_internal.cuh"
+#include "pb_mg_kernels.cuh"
 #include "pb_stencil_impl.cuh"
 
 namespace pb {
 
 PB_DEFINE_ERROR_READER(read_error_mg)
-
-// A level is one periodic n^3 box held with a one-cell ghost layer: cell (x, y, z), -1 <= x,y,z <= n,
-// sits at (x+1) + sx*((y+1) + (n+2)*(z+1)). The x pitch sx >= n+2 is n+2 rounded up to 16 bytes,
-// so every row starts on a 16-byte boundary (a TMA requirement); columns past n+1 are padding.
-template <typename T>
-constexpr int grown_pitch(int n)
-{
-    return (n + 2 + (16 / (int)sizeof(T)) - 1) / (16 / (int)sizeof(T)) * (16 / (int)sizeof(T));
-}
-
-// Writes v to the valid cell (x,y,z) and to every ghost cell that is a periodic image of it.
-// Out of line: only cells on the box boundary call it, and keeping its index arrays out of the
-// fused stencil kernels keeps their register count low.
-template <typename T>
-__device__ __noinline__ void store_periodic_images(T* out, int n, int sx, int x, int y, int z, T v)
-{
-    const long long Sy = sx, Sz = (long long)sx * (n + 2);
-    int xs[3], ys[3], zs[3];
-    int nx = 1, ny = 1, nz = 1;
-    xs[0] = x + 1;
-    ys[0] = y + 1;
-    zs[0] = z + 1;
-    if (x == 0) xs[nx++] = n + 1;
-    if (x == n - 1) xs[nx++] = 0;
-    if (y == 0) ys[ny++] = n + 1;
-    if (y == n - 1) ys[ny++] = 0;
-    if (z == 0) zs[nz++] = n + 1;
-    if (z == n - 1) zs[nz++] = 0;
-    for (int k = 0; k < nz; k++)
-        for (int j = 0; j < ny; j++)
-            for (int i = 0; i < nx; i++) out[xs[i] + Sy * ys[j] + Sz * zs[k]] = v;
-}
-
-template <typename T>
-__device__ __forceinline__ long long grown_index(int n, int sx, int x, int y, int z)
-{
-    return (x + 1) + (long long)sx * ((y + 1) + (long long)(n + 2) * (z + 1));
-}
-
-// Which periodic image of a coordinate exists: 0 none, 1 at +n (c == 0), 2 at -n (c == n-1).
-__device__ __forceinline__ int edge_code(int c, int n) { return c == 0 ? 1 : (c == n - 1 ? 2 : 0); }
-
-// Writes v at q (the valid cell) and at its periodic images, given the edge codes of x, y, z. The
-// images sit at constant offsets +-n, +-n*sx, +-n*sx*(n+2) from q, so this is a few predicated
-// stores. n == 1 (a cell that is both first and last) takes the general path.
-template <typename T>
-__device__ __forceinline__ void store_with_images(T* out, int n, int sx, T* q, int ex, int ey, int ez, T v)
-{
-    *q = v;
-    if ((ex | ey | ez) == 0) return;
-    if (n == 1) {
-        store_periodic_images(out, n, sx, 0, 0, 0, v);
-        return;
-    }
-    const long long ox = ex == 0 ? 0 : (ex == 1 ? n : -n);
-    const long long oy = ey == 0 ? 0 : (ey == 1 ? (long long)n * sx : -(long long)n * sx);
-    const long long sz = (long long)n * sx * (n + 2);
-    const long long oz = ez == 0 ? 0 : (ez == 1 ? sz : -sz);
-    if (ox) q[ox] = v;
-    if (oy) q[oy] = v;
-    if (ox && oy) q[ox + oy] = v;
-    if (oz) {
-        q[oz] = v;
-        if (ox) q[oz + ox] = v;
-        if (oy) q[oz + oy] = v;
-        if (ox && oy) q[oz + ox + oy] = v;
-    }
-}
-
-template <typename T>
-__device__ __forceinline__ void store_periodic(T* out, int n, int sx, int x, int y, int z, T v)
-{
-    store_with_images(out, n, sx, out + grown_index<T>(n, sx, x, y, z), edge_code(x, n), edge_code(y, n),
-                      edge_code(z, n), v);
-}
-
-// Row cursor of a periodic output for a thread's points x, x+1 (kPV of them) in one row: the
-// address of the first point's valid cell at the row's first plane z0, and the constant offsets of
-// the periodic images (0 when there is none): per point in x, and for the row in y.
-constexpr int kPV = 2;
-template <typename T>
-struct PeriodicRow {
-    T* p;
-    int z0;
-    int yo;
-    int xo[kPV];
-    bool act;
-    __device__ __forceinline__ bool active() const { return act; }
-};
-__device__ __forceinline__ int image_offset(int c, int n, int stride)
-{
-    return c == 0 ? n * stride : (c == n - 1 ? -n * stride : 0);
-}
-template <typename T>
-__device__ __forceinline__ PeriodicRow<T> periodic_row(T* out, int n, int sx, int x, int y, int z0, bool active)
-{
-    PeriodicRow<T> r;
-    r.p = active ? out + grown_index<T>(n, sx, x, y, z0) : out;
-    r.z0 = z0;
-    r.act = active;
-    r.yo = image_offset(y, n, sx);
-#pragma unroll
-    for (int v = 0; v < kPV; v++) r.xo[v] = image_offset(x + v, n, 1);
-    return r;
-}
-// Stores v at point (row, plane z0+zo, x+pv) and at its periodic images. ZE: the plane is the
-// first or last of the domain. A 1-cell box (every coordinate both first and last) takes the
-// general path.
-template <bool ZE, typename T>
-__device__ __forceinline__ void store_row(T* out, int n, int sx, const PeriodicRow<T>& r, int zo, int pv, T val)
-{
-    T* q = r.p + (long long)zo * sx * (n + 2) + pv;
-    if (n == 1) {
-        store_periodic_images(out, n, sx, 0, 0, 0, val);
-        return;
-    }
-    const int xo = r.xo[pv], yo = r.yo;
-    *q = val;
-    if (xo) q[xo] = val;
-    if (yo) {
-        q[yo] = val;
-        if (xo) q[yo + xo] = val;
-    }
-    if constexpr (ZE) {
-        const long long zs = (long long)n * sx * (n + 2);
-        T* qz = q + (r.z0 + zo == 0 ? zs : -zs);
-        *qz = val;
-        if (xo) qz[xo] = val;
-        if (yo) {
-            qz[yo] = val;
-            if (xo) qz[yo + xo] = val;
-        }
-    }
-}
-template <typename T>
-__device__ __forceinline__ T load_row(const PeriodicRow<T>& r, int n, int sx, int zo, int pv)
-{
-    return r.p[(long long)zo * sx * (n + 2) + pv];
-}
-
-// Scalars of one level's smoother.
-template <typename T>
-struct RelaxCoef {
-    int n, sx;           // edge and x pitch of the level
-    int helm;
-    T neg_lambda;        // Poisson form: -omega*h*h/6
-    T beta, omega, diagB;
-};
-
-// One Jacobi sweep value from the stencil sum acc (L(phi, omega/6) for the Poisson form,
-// L(phi, 1/h^2) for the Helmholtz form), the centre value c, rho and alpha.
-template <typename T>
-__device__ __forceinline__ T relax_value(const RelaxCoef<T>& k, T acc, T c, T rho, T al)
-{
-    if (!k.helm) return dadd(c, dadd(acc, dmul(k.neg_lambda, rho)));
-    const T r = dsub(rho, dsub(dmul(al, c), dmul(k.beta, acc)));
-    return dadd(c, ddiv(dmul(k.omega, r), dadd(al, k.diagB)));
-}
-
-// relax epilogue: auxiliary field 0 = rho, 1 = alpha (Helmholtz)
-template <typename T>
-struct EpiRelax {
-    T* out;
-    RelaxCoef<T> k;
-    using Row = PeriodicRow<T>;
-    static constexpr bool kZEdge = true;
-    static constexpr int kAux = 2;
-    __device__ __forceinline__ Row row(int x, int y, int z0, bool active) const { return periodic_row(out, k.n, k.sx, x, y, z0, active); }
-    __device__ __forceinline__ bool z_edge(int z) const { return z == 0 || z == k.n - 1; }
-    __device__ __forceinline__ T init(const Row&, int, int, const AuxCtx&) const { return T(0); }
-    template <bool ZE>
-    __device__ __forceinline__ void finish(const Row& r, int zo, int pv, T acc, T c, const AuxCtx& ax) const
-    {
-        if (!r.active()) return;
-        const T al = k.helm ? ax.get<T>(1) : T(0);
-        store_row<ZE>(out, k.n, k.sx, r, zo, pv, relax_value(k, acc, c, ax.get<T>(0), al));
-    }
-    __device__ __forceinline__ void end_warp() const {}
-    __device__ __forceinline__ void end_block() const {}
-};
-
-// Last FP32 post-smoothing sweep of a mixed-precision cycle, fused with the FP64 correction:
-// u64 += (double) e_new, periodic images included. Auxiliary fields 0 = u64 itself (its old value
-// arrives through the pipeline instead of a dependent load), 1 = rho, 2 = alpha (Helmholtz).
-struct EpiRelaxUpdate {
-    double* u;
-    int usx;             // x pitch of u
-    RelaxCoef<float> k;
-    using Row = PeriodicRow<double>;
-    static constexpr bool kZEdge = true;
-    static constexpr int kAux = 3;
-    __device__ __forceinline__ Row row(int x, int y, int z0, bool active) const { return periodic_row(u, k.n, usx, x, y, z0, active); }
-    __device__ __forceinline__ bool z_edge(int z) const { return z == 0 || z == k.n - 1; }
-    __device__ __forceinline__ float init(const Row&, int, int, const AuxCtx&) const { return 0.f; }
-    template <bool ZE>
-    __device__ __forceinline__ void finish(const Row& r, int zo, int pv, float acc, float c, const AuxCtx& ax) const
-    {
-        if (!r.active()) return;
-        const float al = k.helm ? ax.get<float>(2) : 0.f;
-        const float e = relax_value(k, acc, c, ax.get<float>(1), al);
-        store_row<ZE>(u, k.n, usx, r, zo, pv, dadd(ax.get<double>(0), (double)e));
-    }
-    __device__ __forceinline__ void end_warp() const {}
-    __device__ __forceinline__ void end_block() const {}
-};
-
-// residual max-norm epilogue: Poisson acc starts at (0 - rho) with L(phi, 1/h^2); Helmholtz
-// r = rho - (alpha*phi - beta*L(phi, 1/h^2)). Auxiliary fields as in EpiRelax.
-template <typename T>
-struct EpiResnorm {
-    int helm;
-    T beta;
-    double* result;
-    double m;
-    using Row = OutRow<T>;
-    static constexpr bool kZEdge = false;
-    static constexpr int kAux = 2;
-    __device__ __forceinline__ Row row(int, int, int, bool active) const { return Row{nullptr, active}; }
-    __device__ __forceinline__ bool z_edge(int) const { return false; }
-    __device__ __forceinline__ T init(const Row& r, int, int, const AuxCtx& ax) const
-    {
-        if (helm || !r.active) return T(0);
-        return dsub(T(0), ax.get<T>(0));
-    }
-    template <bool ZE>
-    __device__ __forceinline__ void finish(const Row& r, int, int, T acc, T c, const AuxCtx& ax)
-    {
-        if (!r.active) return;
-        if (!helm) {
-            m = upd_abs(m, (double)acc);
-        } else {
-            const T res = dsub(ax.get<T>(0), dsub(dmul(ax.get<T>(1), c), dmul(beta, acc)));
-            m = upd_abs(m, (double)res);
-        }
-    }
-    __device__ __forceinline__ void end_warp() const { warp_max_atomic(m, result); }
-    __device__ __forceinline__ void end_block() const { block_max_atomic(m, result); }
-};
-
-// Mixed precision, one pass over the FP64 state u (auxiliary fields: 0 = f, 1 = alpha):
-//   r = (0 + f) + L(u, -1/h^2)  |  r = f - (alpha*u - beta*L(u, 1/h^2))   (FP64)
-//   norm = max |r|; rhs32 = float(r); first FP32 sweep of the next cycle from e = 0 into e32.
-struct Res64Row {
-    PeriodicRow<float> e;
-    float* r;
-};
-struct EpiRes64 {
-    float* e32;          // grown FP32 level (pitch k.sx)
-    float* rhs32;        // n^3
-    int helm;
-    double beta;
-    RelaxCoef<float> k;
-    double* result;
-    double m;
-    using Row = Res64Row;
-    static constexpr bool kZEdge = true;
-    static constexpr int kAux = 2;
-    __device__ __forceinline__ Row row(int x, int y, int z0, bool active) const
-    {
-        Row r;
-        r.e = periodic_row(e32, k.n, k.sx, x, y, z0, active);
-        r.r = active ? rhs32 + x + (long long)k.n * (y + (long long)k.n * z0) : rhs32;
-        return r;
-    }
-    __device__ __forceinline__ bool z_edge(int z) const { return z == 0 || z == k.n - 1; }
-    __device__ __forceinline__ double init(const Row& r, int, int, const AuxCtx& ax) const
-    {
-        if (helm || !r.e.active()) return 0.0;
-        return dadd(0.0, ax.get<double>(0));
-    }
-    template <bool ZE>
-    __device__ __forceinline__ void finish(const Row& r, int zo, int pv, double acc, double c, const AuxCtx& ax)
-    {
-        if (!r.e.active()) return;
-        double res = acc;
-        float al = 0.f;
-        if (helm) {
-            const double a64 = ax.get<double>(1);
-            res = dsub(ax.get<double>(0), dsub(dmul(a64, c), dmul(beta, acc)));
-            al = __double2float_rn(a64);
-        }
-        m = upd_abs(m, res);
-        const float r32 = __double2float_rn(res);
-        r.r[(long long)zo * k.n * k.n + pv] = r32;
-        store_row<ZE>(e32, k.n, k.sx, r.e, zo, pv, relax_value(k, 0.f, 0.f, r32, al));
-    }
-    __device__ __forceinline__ void end_warp() const { warp_max_atomic(m, result); }
-    __device__ __forceinline__ void end_block() const { block_max_atomic(m, result); }
-};
-
-// first sweep from phi == 0 (every read of phi would return +0.0)
-template <typename T>
-__global__ void __launch_bounds__(256) k_relax_first(const T* __restrict__ rhs, const T* __restrict__ alpha, T* out,
-                                                     RelaxCoef<T> k)
-{
-    const int n = k.n;
-    const long long total = (long long)n * n * n;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
-        int x = (int)(i % n);
-        long long q = i / n;
-        int y = (int)(q % n), z = (int)(q / n);
-        const T al = k.helm ? alpha[i] : T(0);
-        store_periodic(out, n, k.sx, x, y, z, relax_value(k, T(0), T(0), rhs[i], al));
-    }
-}
-
-// exact coarsest-level solve: out = Ainv * rhs (one thread per cell, products summed in column order)
-template <typename T>
-__global__ void __launch_bounds__(256) k_bottom_direct(const T* __restrict__ ainv, const T* __restrict__ rhs, T* out,
-                                                       int n, int sx)
-{
-    const int N = n * n * n;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
-        T acc = T(0);
-        for (int j = 0; j < N; j++) acc = dadd(acc, dmul(ainv[(long long)i * N + j], rhs[j]));
-        store_periodic(out, n, sx, i % n, (i / n) % n, i / (n * n), acc);
-    }
-}
-
-__global__ void __launch_bounds__(256) k_to_float(const double* __restrict__ a, float* b, long long n)
-{
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        b[i] = __double2float_rn(a[i]);
-}
-
-// One fine cell's residual for the restriction: rho + L(phi, -1/h^2) (Poisson form, cf scaled by
-// -1/h^2) or rho - (alpha*phi - beta*L(phi, 1/h^2)) (Helmholtz form, cf scaled by 1/h^2).
-template <typename T>
-__device__ __forceinline__ T fine_residual(const T* phi, long long gi, long long Sy, long long Sz, T rho, T al,
-                                           int helm, const Coefs<T>& cf, T beta)
-{
-    if (!helm) {
-        T r = dadd(T(0), rho);
-#pragma unroll
-        for (int j = 0; j < ShapeLap7::NT; j++) {
-            const long long o = ShapeLap7::off(j, 0) + Sy * ShapeLap7::off(j, 1) + Sz * ShapeLap7::off(j, 2);
-            r = dadd(r, dmul(cf.c[j], phi[gi + o]));
-        }
-        return r;
-    }
-    T lp = T(0);
-#pragma unroll
-    for (int j = 0; j < ShapeLap7::NT; j++) {
-        const long long o = ShapeLap7::off(j, 0) + Sy * ShapeLap7::off(j, 1) + Sz * ShapeLap7::off(j, 2);
-        lp = dadd(lp, dmul(cf.c[j], phi[gi + o]));
-    }
-    return dsub(rho, dsub(dmul(al, phi[gi]), dmul(beta, lp)));
-}
-
-// coarse right-hand side: AvgDown(2) of the fine residual, children in Box([0,1]^3) order.
-// Block (32, 8): one thread per coarse cell of a (cx, cy) tile; blockIdx.z = cz.
-template <typename T>
-__global__ void __launch_bounds__(256) k_resid_restrict(const T* __restrict__ phi, const T* __restrict__ rhs,
-                                                        const T* __restrict__ alpha, T* rhs_c, int nf, int sx, int helm,
-                                                        Coefs<T> cf, T beta)
-{
-    const int nc = nf / 2;
-    const int cx = blockIdx.x * 32 + threadIdx.x, cy = blockIdx.y * 8 + threadIdx.y, cz = blockIdx.z;
-    if (cx >= nc || cy >= nc) return;
-    const long long Sy = sx, Sz = (long long)sx * (nf + 2);
-    const T eighth = T(1.0 / 8);
-    T acc = T(0);
-#pragma unroll
-    for (int k = 0; k < 8; k++) {
-        const int fx = 2 * cx + (k & 1), fy = 2 * cy + ((k >> 1) & 1), fz = 2 * cz + (k >> 2);
-        const long long fi = fx + (long long)nf * (fy + (long long)nf * fz);
-        const T al = helm ? __ldg(alpha + fi) : T(0);
-        const T r = fine_residual(phi, grown_index<T>(nf, sx, fx, fy, fz), Sy, Sz, __ldg(rhs + fi), al, helm, cf, beta);
-        acc = dadd(acc, dmul(eighth, r));
-    }
-    rhs_c[cx + (long long)nc * (cy + (long long)nc * cz)] = acc;
-}
-static inline dim3 restrict_grid(int nf) { return dim3((nf / 2 + 31) / 32, (nf / 2 + 7) / 8, nf / 2); }
-
-// phi += 1.0 * delta_c(p/2) on the valid box, periodic images included. Block (32, 8): a thread
-// owns the two fine cells of one coarse cell in x.
-template <typename T>
-__global__ void __launch_bounds__(256) k_prolong(T* phi, const T* __restrict__ delta_c, int nf, int sxf, int sxc)
-{
-    const int nc = nf / 2;
-    const int cx = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
-    if (cx >= nc || y >= nf) return;
-    const T d = delta_c[grown_index<T>(nc, sxc, cx, y / 2, z / 2)];
-    const int ey = edge_code(y, nf), ez = edge_code(z, nf);
-#pragma unroll
-    for (int v = 0; v < 2; v++) {
-        const int x = 2 * cx + v;
-        T* q = phi + grown_index<T>(nf, sxf, x, y, z);
-        store_with_images(phi, nf, sxf, q, edge_code(x, nf), ey, ez, dadd(*q, dmul(T(1), d)));
-    }
-}
-static inline dim3 prolong_grid(int nf) { return dim3((nf / 2 + 31) / 32, (nf + 7) / 8, nf); }
-
-// n^3 <-> grown layout with periodic ghost images
-template <typename T>
-__global__ void __launch_bounds__(256) k_pack_in(const T* __restrict__ src, T* out, int n, int sx)
-{
-    const long long total = (long long)n * n * n;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
-        int x = (int)(i % n);
-        long long q = i / n;
-        store_periodic(out, n, sx, x, (int)(q % n), (int)(q / n), src[i]);
-    }
-}
-template <typename T>
-__global__ void __launch_bounds__(256) k_pack_out(const T* __restrict__ g, T* dst, int n, int sx)
-{
-    const long long total = (long long)n * n * n;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
-        int x = (int)(i % n);
-        long long q = i / n;
-        dst[i] = g[grown_index<T>(n, sx, x, (int)(q % n), (int)(q / n))];
-    }
-}
-
-// AvgDown(2) of a plain n^3 field (coarse-level alpha)
-template <typename T>
-__global__ void __launch_bounds__(256) k_avgdown_plain(const T* __restrict__ f, T* c, int nf)
-{
-    const int nc = nf / 2;
-    const long long total = (long long)nc * nc * nc;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
-        int cx = (int)(i % nc);
-        long long q = i / nc;
-        int cy = (int)(q % nc), cz = (int)(q / nc);
-        T acc = T(0);
-        for (int k = 0; k < 8; k++) {
-            int fx = 2 * cx + (k & 1), fy = 2 * cy + ((k >> 1) & 1), fz = 2 * cz + (k >> 2);
-            acc = dadd(acc, dmul(T(1.0 / 8), f[fx + (long long)nf * (fy + (long long)nf * fz)]));
-        }
-        c[i] = acc;
-    }
-}
-
-
-// ---- coarse levels as one kernel ---------------------------------------------------------------
-// The levels at and below a small edge run their whole part of the V-cycle inside one CTA: every
-// sweep, restriction and prolongation is a block-strided loop followed by __syncthreads, with the
-// same per-cell arithmetic (and the same buffer ping-pong) as the one-launch-per-step path, so the
-// results are identical; only the launches go away.
-constexpr int kMaxCoarse = 8;
-constexpr int kCoarseThreads = 1024;
-template <typename T>
-struct CoarseLevel {
-    T* phi[2];
-    T* rhs;
-    const T* alpha;
-    RelaxCoef<T> k;          // n, sx and the smoother's scalars
-    Coefs<T> crelax;         // L(., omega/6) (Poisson form) or L(., 1/h^2) (Helmholtz form)
-    Coefs<T> cres;           // L(., -1/h^2) (Poisson form) or L(., 1/h^2) (Helmholtz form)
-};
-template <typename T>
-struct CoarseArgs {
-    CoarseLevel<T> lv[kMaxCoarse];   // 0 = coarsest
-    int top;                         // finest level handled here (entered from zero)
-    int nu1, nu2, nu_bottom, direct;
-    const T* ainv;
-    T beta;
-    int in_smem;                     // 1: the levels live in shared memory during the cycle
-};
-
-// Shared-memory arena of the coarse cycle: per level two grown buffers, rho and (Helmholtz)
-// alpha, each 16-byte aligned. Returns the bytes needed; fills the element offsets when asked.
-template <typename T>
-static size_t coarse_smem_layout(const CoarseArgs<T>& a, int helm, long long (*off)[4])
-{
-    size_t total = 0;
-    auto take = [&](size_t elems) {
-        const size_t o = total;
-        total += (elems * sizeof(T) + 15) / 16 * 16;
-        return (long long)(o / sizeof(T));
-    };
-    for (int l = 0; l <= a.top; l++) {
-        const CoarseLevel<T>& L = a.lv[l];
-        const size_t g = (size_t)L.k.sx * (L.k.n + 2) * (L.k.n + 2), c = (size_t)L.k.n * L.k.n * L.k.n;
-        const long long o0 = take(g), o1 = take(g), o2 = take(c), o3 = helm ? take(c) : -1;
-        if (off) {
-            off[l][0] = o0;
-            off[l][1] = o1;
-            off[l][2] = o2;
-            off[l][3] = o3;
-        }
-    }
-    return total;
-}
-
-struct CoarseOffsets {
-    long long o[kMaxCoarse][4];      // element offsets of phi0, phi1, rho, alpha per level
-};
-
-template <typename T>
-__device__ void coarse_relax(const CoarseLevel<T>& L, int cur, bool first)
-{
-    const int n = L.k.n, sx = L.k.sx;
-    const long long Sy = sx, Sz = (long long)sx * (n + 2);
-    const T* src = L.phi[cur];
-    T* dst = L.phi[1 - cur];
-    for (int i = threadIdx.x; i < n * n * n; i += blockDim.x) {
-        const int x = i % n, y = (i / n) % n, z = i / (n * n);
-        const T al = L.k.helm ? L.alpha[i] : T(0);
-        T v;
-        if (first) {
-            v = relax_value(L.k, T(0), T(0), L.rhs[i], al);
-        } else {
-            const long long g = grown_index<T>(n, sx, x, y, z);
-            T acc = T(0);
-#pragma unroll
-            for (int j = 0; j < ShapeLap7::NT; j++) {
-                const long long o = ShapeLap7::off(j, 0) + Sy * ShapeLap7::off(j, 1) + Sz * ShapeLap7::off(j, 2);
-                acc = dadd(acc, dmul(L.crelax.c[j], src[g + o]));
-            }
-            v = relax_value(L.k, acc, src[g], L.rhs[i], al);
-        }
-        store_periodic(dst, n, sx, x, y, z, v);
-    }
-    __syncthreads();
-}
-template <typename T>
-__device__ void coarse_zero(const CoarseLevel<T>& L, int cur)
-{
-    const long long m = (long long)L.k.sx * (L.k.n + 2) * (L.k.n + 2);
-    for (long long i = threadIdx.x; i < m; i += blockDim.x) L.phi[cur][i] = T(0);
-    __syncthreads();
-}
-// returns the buffer index holding the result
-template <typename T>
-__device__ int coarse_sweeps(const CoarseLevel<T>& L, int cur, int k, bool zero_start)
-{
-    for (int s = 0; s < k; s++) {
-        coarse_relax(L, cur, zero_start && s == 0);
-        cur = 1 - cur;
-    }
-    if (zero_start && k == 0) coarse_zero(L, cur);
-    return cur;
-}
-
-template <typename T>
-__global__ void __launch_bounds__(kCoarseThreads) k_coarse_cycle(const CoarseArgs<T> ga, const CoarseOffsets off)
-{
-    extern __shared__ __align__(16) unsigned char coarse_smem[];
-    // level descriptors, shared by the block (in shared-memory mode they point into the arena)
-    __shared__ CoarseLevel<T> lvs[kMaxCoarse];
-    if (threadIdx.x == 0) {
-        T* base = reinterpret_cast<T*>(coarse_smem);
-        for (int l = 0; l <= ga.top; l++) {
-            CoarseLevel<T> L = ga.lv[l];
-            if (ga.in_smem) {
-                L.phi[0] = base + off.o[l][0];
-                L.phi[1] = base + off.o[l][1];
-                L.rhs = base + off.o[l][2];
-                if (L.k.helm) L.alpha = base + off.o[l][3];
-            }
-            lvs[l] = L;
-        }
-    }
-    __syncthreads();
-    if (ga.in_smem) {
-        // rho of the entry level and every alpha come in
-        for (int l = 0; l <= ga.top; l++) {
-            const int n3 = ga.lv[l].k.n * ga.lv[l].k.n * ga.lv[l].k.n;
-            if (l == ga.top)
-                for (int i = threadIdx.x; i < n3; i += blockDim.x) lvs[l].rhs[i] = ga.lv[l].rhs[i];
-            if (ga.lv[l].k.helm)
-                for (int i = threadIdx.x; i < n3; i += blockDim.x) const_cast<T*>(lvs[l].alpha)[i] = ga.lv[l].alpha[i];
-        }
-        __syncthreads();
-    }
-    const CoarseArgs<T>& a = ga;
-    int cur[kMaxCoarse];
-    // down: pre-smoothing from zero, residual restriction
-    for (int l = a.top; l > 0; l--) {
-        const CoarseLevel<T>& L = lvs[l];
-        CoarseLevel<T> const& C = lvs[l - 1];
-        cur[l] = coarse_sweeps(L, 0, a.nu1, true);
-        const int nf = L.k.n, nc = nf / 2, sx = L.k.sx;
-        const long long Sy = sx, Sz = (long long)sx * (nf + 2);
-        const T* phi = L.phi[cur[l]];
-        for (int i = threadIdx.x; i < nc * nc * nc; i += blockDim.x) {
-            const int cx = i % nc, cy = (i / nc) % nc, cz = i / (nc * nc);
-            T acc = T(0);
-#pragma unroll
-            for (int k = 0; k < 8; k++) {
-                const int fx = 2 * cx + (k & 1), fy = 2 * cy + ((k >> 1) & 1), fz = 2 * cz + (k >> 2);
-                const int fi = fx + nf * (fy + nf * fz);
-                const T al = L.k.helm ? L.alpha[fi] : T(0);
-                const T r = fine_residual(phi, grown_index<T>(nf, sx, fx, fy, fz), Sy, Sz, L.rhs[fi], al, L.k.helm,
-                                          L.cres, a.beta);
-                acc = dadd(acc, dmul(T(1.0 / 8), r));
-            }
-            C.rhs[i] = acc;
-        }
-        __syncthreads();
-    }
-    // bottom
-    {
-        const CoarseLevel<T>& B = lvs[0];
-        if (a.direct) {
-            const int n = B.k.n, N = n * n * n;
-            for (int i = threadIdx.x; i < N; i += blockDim.x) {
-                T acc = T(0);
-                for (int j = 0; j < N; j++) acc = dadd(acc, dmul(a.ainv[(long long)i * N + j], B.rhs[j]));
-                store_periodic(B.phi[0], n, B.k.sx, i % n, (i / n) % n, i / (n * n), acc);
-            }
-            __syncthreads();
-            cur[0] = 0;
-        } else {
-            cur[0] = coarse_sweeps(B, 0, a.nu_bottom, true);
-        }
-    }
-    // up: prolongation, post-smoothing
-    for (int l = 1; l <= a.top; l++) {
-        const CoarseLevel<T>& L = lvs[l];
-        const CoarseLevel<T>& C = lvs[l - 1];
-        const int nf = L.k.n, nc = nf / 2;
-        T* phi = L.phi[cur[l]];
-        const T* d = C.phi[cur[l - 1]];
-        for (int i = threadIdx.x; i < nf * nf * nf; i += blockDim.x) {
-            const int x = i % nf, y = (i / nf) % nf, z = i / (nf * nf);
-            const T dv = d[grown_index<T>(nc, C.k.sx, x / 2, y / 2, z / 2)];
-            const long long g = grown_index<T>(nf, L.k.sx, x, y, z);
-            store_periodic(phi, nf, L.k.sx, x, y, z, dadd(phi[g], dmul(T(1), dv)));
-        }
-        __syncthreads();
-        cur[l] = coarse_sweeps(L, cur[l], a.nu2, false);
-    }
-    // leave the result in buffer 0 of the top level (in global memory)
-    if (a.in_smem || cur[a.top] == 1) {
-        const CoarseLevel<T>& L = lvs[a.top];
-        const long long m = (long long)L.k.sx * (L.k.n + 2) * (L.k.n + 2);
-        const T* src = L.phi[cur[a.top]];
-        for (long long i = threadIdx.x; i < m; i += blockDim.x) ga.lv[a.top].phi[0][i] = src[i];
-    }
-}
 
 template <typename T>
 struct MGLevel {
@@ -781,18 +145,6 @@ static Box3 valid_box(const MGLevel<T>& L)
     Box3 b;
     for (int d = 0; d < 3; d++) { b.lo[d] = 0; b.hi[d] = L.n - 1; }
     return b;
-}
-// 7-point coefficients times s (the reference's Stencil * scale: coefficient*s unless s == 1)
-template <typename T>
-static Coefs<T> lap7_coefs(double s)
-{
-    Coefs<T> cf;
-    for (int j = 0; j < 13; j++) cf.c[j] = T(0);
-    for (int j = 0; j < 7; j++) {
-        const double c = (j == 0) ? -6.0 : 1.0;
-        cf.c[j] = (T)((s != 1.0) ? c * s : c);
-    }
-    return cf;
 }
 template <typename T>
 static RelaxCoef<T> relax_coef(const pb_mg* mg, const MGLevel<T>& L)

@@ -1,0 +1,733 @@
+// Serving engine (C ABI: pb_serve_*): a stream of periodic Poisson/Helmholtz solves of different
+// grid sizes, solved together. Each admitted solve keeps its hierarchy resident on the device (FP64
+// solution and right-hand side, FP32 levels) for its whole life; admission is bounded by an HBM
+// budget and a slot count. One step runs one mixed-precision V-cycle for every in-flight solve:
+// each phase of the cycle (a sweep at one depth, a restriction, a prolongation, the coarse-level
+// cycle, the FP64 residual pass) is one launch covering all solves, and the whole step is one CUDA
+// graph, captured once per hierarchy depth and replayed while solves arrive and retire (the kernels
+// read their work lists from device memory). Converged solves are copied out and their slots and
+// memory reused.
+//
+// Per solve the arithmetic is the single-solve mixed-precision solver's (pb_mg with PB_MG_MIXED,
+// a constant alpha field, levels = the number of halvings, coarse levels of edge <= 16 fused), so
+// a result is the same alone and in any mix, and the same as that solver's.
+//
+// Reference counterpart: none (the reference runs one solve at a time, LevelMultigridSolver::solve,
+// include/utils/implem/Proto_LevelMultigridSolverImplem.H:85-123).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <vector>
+
+#include "pb_internal.cuh"
+#include "pb_serve_kernels.cuh"
+#include "pb_stencil_impl.cuh"
+
+namespace pb {
+
+PB_DEFINE_ERROR_READER(read_error_serve)
+
+// One device-resident hierarchy (reused across solves of the same edge).
+struct SvHier {
+    int n = 0;
+    int nlev = 0;                       // levels, top first
+    std::vector<int> edge, sx;          // per level
+    std::vector<float*> phi0, phi1, rhs, alpha;   // alpha: coarse levels only (Helmholtz)
+    double* u64 = nullptr;              // grown, pitch sxd
+    double* f64 = nullptr;              // n^3 (also the staging buffer of the result)
+    int sxd = 0;
+    size_t bytes = 0;
+};
+
+struct SvSolve {
+    long long ticket = 0;
+    pb_serve_request req{};
+    int state = PB_SERVE_WAITING;
+    int slot = -1;
+    SvHier* h = nullptr;
+    int depth = 0;                      // batched levels (the top one and every edge > 16)
+    std::vector<float> alpha_lv;        // per level: the FP32 alpha the single-solve solver has there
+    int cycles = 0;
+    double r0 = 0, r = 0;
+    bool fresh = false;                 // admitted, first residual pass pending
+};
+
+} // namespace pb
+
+using namespace pb;
+
+struct pb_serve {
+    pb_serve_params p{};
+    int device = 0;
+    cudaStream_t st = nullptr;
+    long long next_ticket = 1;
+    std::map<long long, SvSolve> solves;
+    std::deque<long long> waiting;
+    std::vector<long long> slots;       // slot -> ticket (0: free)
+    std::vector<long long> completed;   // tickets done since the last poll
+    std::multimap<int, SvHier*> cache;  // idle hierarchies by edge
+    size_t held = 0;                    // bytes of all hierarchies (busy and idle)
+    // phase lists (device + host mirror)
+    int max_phases = 0;
+    SvItem* d_items = nullptr;
+    SvPhaseHeader* d_hdr = nullptr;
+    std::vector<SvItem> h_items;
+    std::vector<SvPhaseHeader> h_hdr;
+    CoarseArgs<float>* d_cargs = nullptr;
+    CoarseOffsets* d_coffs = nullptr;
+    int* d_ccount = nullptr;
+    std::vector<CoarseArgs<float>> h_cargs;
+    std::vector<CoarseOffsets> h_coffs;
+    double* d_norms = nullptr;          // per slot: residual norm of the step
+    double* d_r0 = nullptr;             // per slot: first residual norm
+    double* h_norms = nullptr;          // pinned
+    double* h_r0 = nullptr;             // pinned
+    // graphs by depth
+    std::map<int, cudaGraphExec_t> graphs;
+    bool lists_dirty = true;
+    int depth_now = 0;
+    int grid = 0;                       // persistent grid of the phase kernels
+    size_t coarse_smem = 0;
+};
+
+namespace {
+
+constexpr int kCoarseEdge = 16;
+constexpr int kMaxDepth = 12;
+// phases per depth (down: up to nu1 sweeps + restrict; up: prolong + nu2 sweeps) plus K1 slots
+int phases_for(const pb_serve_params& p) { return kMaxDepth * (p.nu1 + p.nu2 + 2) + 2; }
+
+bool edge_ok(int n)
+{
+    if (n < 2 || n % 2 != 0) return false;   // the top level is batched, so it must coarsen once
+    int e = n;
+    while (e > kCoarseEdge && e % 2 == 0) e /= 2;
+    return e <= kCoarseEdge;
+}
+
+void hier_free(SvHier* h)
+{
+    for (size_t l = 0; l < h->phi0.size(); l++) {
+        cudaFree(h->phi0[l]);
+        cudaFree(h->phi1[l]);
+        cudaFree(h->rhs[l]);
+        cudaFree(h->alpha[l]);
+    }
+    cudaFree(h->u64);
+    cudaFree(h->f64);
+    delete h;
+}
+
+size_t hier_bytes(int n)
+{
+    size_t b = 0;
+    for (int e = n;; e /= 2) {
+        const size_t g = (size_t)grown_pitch<float>(e) * (e + 2) * (e + 2), c = (size_t)e * e * e;
+        b += 4 * (2 * g + c) + (e <= kCoarseEdge ? 4 * c : 0);
+        if (e % 2 != 0 || e == 1) break;
+    }
+    b += 8 * (size_t)grown_pitch<double>(n) * (n + 2) * (n + 2) + 8 * (size_t)n * n * n;
+    return b;
+}
+
+SvHier* hier_alloc(int n)
+{
+    SvHier* h = new SvHier;
+    h->n = n;
+    bool ok = true;
+    for (int e = n;; e /= 2) {
+        h->edge.push_back(e);
+        h->sx.push_back(grown_pitch<float>(e));
+        const size_t g = sizeof(float) * (size_t)h->sx.back() * (e + 2) * (e + 2), c = sizeof(float) * (size_t)e * e * e;
+        float *a = nullptr, *b = nullptr, *r = nullptr, *al = nullptr;
+        ok = ok && cudaMalloc(&a, g) == cudaSuccess && cudaMalloc(&b, g) == cudaSuccess && cudaMalloc(&r, c) == cudaSuccess;
+        if (ok && e <= kCoarseEdge) ok = cudaMalloc(&al, c) == cudaSuccess;
+        if (ok) ok = cudaMemset(a, 0, g) == cudaSuccess && cudaMemset(b, 0, g) == cudaSuccess;
+        h->phi0.push_back(a);
+        h->phi1.push_back(b);
+        h->rhs.push_back(r);
+        h->alpha.push_back(al);
+        if (e % 2 != 0 || e == 1) break;
+    }
+    h->nlev = (int)h->edge.size();
+    h->sxd = grown_pitch<double>(n);
+    const size_t gd = sizeof(double) * (size_t)h->sxd * (n + 2) * (n + 2);
+    ok = ok && cudaMalloc(&h->u64, gd) == cudaSuccess && cudaMalloc(&h->f64, sizeof(double) * (size_t)n * n * n) == cudaSuccess;
+    h->bytes = hier_bytes(n);
+    if (!ok) {
+        cudaGetLastError();
+        hier_free(h);
+        return nullptr;
+    }
+    return h;
+}
+
+int batched_depth(const SvHier* h)
+{
+    int d = 1;
+    while (d < h->nlev && h->edge[d] > kCoarseEdge) d++;
+    return d;
+}
+
+// Per-level FP32 alpha of a constant field: the top level holds float(alpha), each coarser level the
+// 2^3 average of the one above (eight products 0.125*a summed in order, each rounded to FP32, as
+// the averaging kernel does; for a non-dyadic a the sum is not exactly a).
+std::vector<float> level_alphas(double alpha, int nlev)
+{
+    std::vector<float> v(nlev);
+    v[0] = (float)alpha;
+    for (int l = 1; l < nlev; l++) {
+        float acc = 0.f;
+        for (int k = 0; k < 8; k++) acc = acc + 0.125f * v[l - 1];
+        v[l] = acc;
+    }
+    return v;
+}
+
+// Smoother scalars of the level at depth d of an n-edge hierarchy (the single-solve solver's).
+RelaxCoef<float> level_coef(const pb_serve_params& p, const pb_serve_request& q, int n, int e, int sx, int d)
+{
+    const double h = (double)(1 << d) / (double)n, hsqinv = 1. / (h * h);
+    RelaxCoef<float> k;
+    k.n = e;
+    k.sx = sx;
+    k.helm = q.form == PB_MG_HELMHOLTZ;
+    k.neg_lambda = (float)(-mg_lambda(p.omega, h));
+    k.beta = (float)q.beta;
+    k.omega = (float)p.omega;
+    k.diagB = (float)(6.0 * q.beta * hsqinv);
+    return k;
+}
+
+double level_hsqinv(int n, int d)
+{
+    const double h = (double)(1 << d) / (double)n;
+    return 1. / (h * h);
+}
+
+} // namespace
+
+// ---- work lists ------------------------------------------------------------------------------------
+// Phase order of one step (D = deepest batched depth among the active solves):
+//   down d = 0..D-1 : sweeps (depth 0: nu1-1, the first ran in the residual pass; deeper: a sweep
+//                     from zero then nu1-1), restriction to d+1
+//   coarse          : the fused coarse cycle of every solve (one CTA each)
+//   up d = D-1..0   : prolongation from d+1, sweeps (depth 0: nu2-1 then the fused update)
+//   K1              : FP64 residual, norm, FP32 right-hand side and first sweep of the next step
+// Phase slots are laid out in that order; the graph for depth D launches exactly these slots.
+namespace {
+
+struct PhaseSlot {
+    int op;
+    int depth;
+};
+
+std::vector<PhaseSlot> phase_plan(const pb_serve_params& p, int D)
+{
+    std::vector<PhaseSlot> v;
+    for (int d = 0; d < D; d++) {
+        if (d == 0) {
+            for (int s = 1; s < p.nu1; s++) v.push_back({SV_RELAX, d});
+        } else {
+            v.push_back({SV_RELAX_FIRST, d});
+            for (int s = 1; s < p.nu1; s++) v.push_back({SV_RELAX, d});
+        }
+        v.push_back({SV_RESTRICT, d});
+    }
+    v.push_back({-1, -1});   // coarse
+    for (int d = D - 1; d >= 0; d--) {
+        v.push_back({SV_PROLONG, d});
+        const int sweeps = d == 0 ? p.nu2 - 1 : p.nu2;
+        for (int s = 0; s < sweeps; s++) v.push_back({SV_RELAX, d});
+        if (d == 0) v.push_back({SV_UPDATE, 0});
+    }
+    v.push_back({SV_K1, 0});
+    return v;
+}
+
+// buffer index holding a level's current solution just before each phase, following the
+// single-solve solver's ping-pong: depth 0 starts at 1 (the residual pass wrote phi[1]), deeper
+// levels start from zero (their first sweep writes phi[1])
+void add_item(std::vector<SvItem>& items, long long& total, SvItem it)
+{
+    it.unit0 = total;
+    total += ((long long)it.units + kSvUnit - 1) / kSvUnit * kSvUnit;
+    items.push_back(it);
+}
+
+} // namespace
+
+static int build_lists(pb_serve* sv)
+{
+    const pb_serve_params& p = sv->p;
+    int D = 0;
+    std::vector<SvSolve*> act;
+    for (long long t : sv->slots)
+        if (t) {
+            SvSolve& s = sv->solves[t];
+            act.push_back(&s);
+            D = std::max(D, s.depth);
+        }
+    sv->depth_now = D;
+    const std::vector<PhaseSlot> plan = phase_plan(p, std::max(D, 1));
+    const int cap = (int)p.max_active;
+    sv->h_items.assign((size_t)sv->max_phases * cap, SvItem{});
+    sv->h_hdr.assign(sv->max_phases, SvPhaseHeader{0, 0});
+    // per solve: the buffer index of each level's current solution as the plan advances
+    std::vector<std::vector<int>> cur(act.size());
+    for (size_t a = 0; a < act.size(); a++) {
+        cur[a].assign(act[a]->h->nlev, 0);
+        cur[a][0] = 1;
+    }
+    for (size_t ph = 0; ph < plan.size(); ph++) {
+        const PhaseSlot& ps = plan[ph];
+        if (ps.op < 0) continue;   // coarse: its own argument table
+        std::vector<SvItem> items;
+        long long total = 0;
+        for (size_t a = 0; a < act.size(); a++) {
+            SvSolve& s = *act[a];
+            SvHier& h = *s.h;
+            const int d = ps.depth;
+            if (d >= s.depth) continue;
+            const int n = h.n, e = h.edge[d], sxl = h.sx[d];
+            SvItem it{};
+            it.k = level_coef(p, s.req, n, e, sxl, d);
+            const bool helm = s.req.form == PB_MG_HELMHOLTZ;
+            it.alpha = s.alpha_lv[d];
+            it.beta = (float)s.req.beta;
+            it.alpha64 = s.req.alpha;
+            it.beta64 = s.req.beta;
+            it.slot = s.slot;
+            it.sxd = h.sxd;
+            it.u64 = h.u64;
+            it.f64 = h.f64;
+            float* ph_[2] = {h.phi0[d], h.phi1[d]};
+            int& c = cur[a][d];
+            switch (ps.op) {
+            case SV_RELAX:
+            case SV_UPDATE:
+                it.in = ph_[c];
+                it.out = ph_[1 - c];
+                it.rhs = h.rhs[d];
+                it.c = lap7_coefs<float>(helm ? level_hsqinv(n, d) : p.omega / 6.0);
+                it.units = e * e * e;
+                if (ps.op == SV_RELAX) c = 1 - c;
+                break;
+            case SV_RELAX_FIRST:
+                c = 0;
+                it.out = ph_[1];
+                it.rhs = h.rhs[d];
+                it.units = e * e * e;
+                c = 1;
+                break;
+            case SV_RESTRICT: {
+                it.in = ph_[c];
+                it.out = h.rhs[d + 1];
+                it.rhs = h.rhs[d];
+                const double hs = level_hsqinv(n, d);
+                it.c = lap7_coefs<float>(helm ? hs : -hs);
+                it.units = (e / 2) * (e / 2) * (e / 2);
+                break;
+            }
+            case SV_PROLONG: {
+                it.in = ph_[c];
+                const int dc = d + 1;
+                // the coarse part leaves its entry level's result in phi[0]
+                const int cc = dc >= s.depth ? 0 : cur[a][dc];
+                it.delta = cc ? h.phi1[dc] : h.phi0[dc];
+                it.sxc = h.sx[dc];
+                it.units = e * e * e;
+                break;
+            }
+            case SV_K1: {
+                it.in = h.phi1[0];
+                it.out = h.rhs[0];
+                const double hs = level_hsqinv(n, 0);
+                it.c64 = lap7_coefs<double>(helm ? hs : -hs);
+                it.units = e * e * e;
+                c = 1;
+                break;
+            }
+            }
+            add_item(items, total, it);
+        }
+        std::copy(items.begin(), items.end(), sv->h_items.begin() + ph * cap);
+        sv->h_hdr[ph] = SvPhaseHeader{(long long)items.size(), total};
+    }
+    // the residual pass for freshly admitted solves (slot max_phases-1)
+    {
+        const int ph = sv->max_phases - 1;
+        std::vector<SvItem> items;
+        long long total = 0;
+        for (size_t a = 0; a < act.size(); a++) {
+            SvSolve& s = *act[a];
+            if (!s.fresh) continue;
+            SvHier& h = *s.h;
+            const bool helm = s.req.form == PB_MG_HELMHOLTZ;
+            SvItem it{};
+            it.k = level_coef(p, s.req, h.n, h.n, h.sx[0], 0);
+            it.alpha = s.alpha_lv[0];
+            it.beta = (float)s.req.beta;
+            it.alpha64 = s.req.alpha;
+            it.beta64 = s.req.beta;
+            it.slot = s.slot;
+            it.sxd = h.sxd;
+            it.u64 = h.u64;
+            it.f64 = h.f64;
+            it.in = h.phi1[0];
+            it.out = h.rhs[0];
+            const double hs = level_hsqinv(h.n, 0);
+            it.c64 = lap7_coefs<double>(helm ? hs : -hs);
+            it.units = h.n * h.n * h.n;
+            add_item(items, total, it);
+        }
+        std::copy(items.begin(), items.end(), sv->h_items.begin() + (size_t)ph * cap);
+        sv->h_hdr[ph] = SvPhaseHeader{(long long)items.size(), total};
+    }
+    // coarse-cycle arguments (entry level = depth s.depth)
+    sv->h_cargs.assign(cap, CoarseArgs<float>{});
+    sv->h_coffs.assign(cap, CoarseOffsets{});
+    int nc = 0;
+    size_t smem_max = 0;
+    for (size_t a = 0; a < act.size(); a++) {
+        SvSolve& s = *act[a];
+        SvHier& h = *s.h;
+        CoarseArgs<float> ca;
+        memset(&ca, 0, sizeof(ca));
+        const int d0 = s.depth, top = h.nlev - 1 - d0;   // coarse levels: index 0 = coarsest
+        const bool helm = s.req.form == PB_MG_HELMHOLTZ;
+        for (int l = 0; l <= top; l++) {
+            const int d = h.nlev - 1 - l;
+            CoarseLevel<float>& c = ca.lv[l];
+            c.phi[0] = h.phi0[d];
+            c.phi[1] = h.phi1[d];
+            c.rhs = h.rhs[d];
+            c.alpha = h.alpha[d];
+            c.k = level_coef(p, s.req, h.n, h.edge[d], h.sx[d], d);
+            const double hs = level_hsqinv(h.n, d);
+            c.crelax = lap7_coefs<float>(helm ? hs : p.omega / 6.0);
+            c.cres = lap7_coefs<float>(helm ? hs : -hs);
+        }
+        ca.top = top;
+        ca.nu1 = p.nu1;
+        ca.nu2 = p.nu2;
+        ca.nu_bottom = p.nu_bottom;
+        ca.direct = 0;
+        ca.ainv = nullptr;
+        ca.beta = (float)s.req.beta;
+        CoarseOffsets off;
+        memset(&off, 0, sizeof(off));
+        const size_t smem = coarse_smem_layout(ca, helm, off.o);
+        ca.in_smem = smem <= sv->coarse_smem ? 1 : 0;
+        smem_max = std::max(smem_max, smem);
+        sv->h_cargs[nc] = ca;
+        sv->h_coffs[nc] = off;
+        nc++;
+    }
+    (void)smem_max;
+    PB_CUDA(cudaMemcpyAsync(sv->d_items, sv->h_items.data(), sizeof(SvItem) * sv->h_items.size(), cudaMemcpyHostToDevice, sv->st));
+    PB_CUDA(cudaMemcpyAsync(sv->d_hdr, sv->h_hdr.data(), sizeof(SvPhaseHeader) * sv->h_hdr.size(), cudaMemcpyHostToDevice, sv->st));
+    PB_CUDA(cudaMemcpyAsync(sv->d_cargs, sv->h_cargs.data(), sizeof(CoarseArgs<float>) * cap, cudaMemcpyHostToDevice, sv->st));
+    PB_CUDA(cudaMemcpyAsync(sv->d_coffs, sv->h_coffs.data(), sizeof(CoarseOffsets) * cap, cudaMemcpyHostToDevice, sv->st));
+    PB_CUDA(cudaMemcpyAsync(sv->d_ccount, &nc, sizeof(int), cudaMemcpyHostToDevice, sv->st));
+    PB_CUDA(cudaStreamSynchronize(sv->st));   // host mirrors may change after return
+    sv->lists_dirty = false;
+    return PB_OK;
+}
+
+static int launch_phase(pb_serve* sv, int slot, int op, double* norms, cudaStream_t st)
+{
+    const SvItem* items = sv->d_items + (size_t)slot * sv->p.max_active;
+    const SvPhaseHeader* hdr = sv->d_hdr + slot;
+    switch (op) {
+    case SV_RELAX: k_sv_phase<SV_RELAX><<<sv->grid, kSvUnit, 0, st>>>(items, hdr, norms); break;
+    case SV_RELAX_FIRST: k_sv_phase<SV_RELAX_FIRST><<<sv->grid, kSvUnit, 0, st>>>(items, hdr, norms); break;
+    case SV_RESTRICT: k_sv_phase<SV_RESTRICT><<<sv->grid, kSvUnit, 0, st>>>(items, hdr, norms); break;
+    case SV_PROLONG: k_sv_phase<SV_PROLONG><<<sv->grid, kSvUnit, 0, st>>>(items, hdr, norms); break;
+    case SV_K1: k_sv_phase<SV_K1><<<sv->grid, kSvUnit, 0, st>>>(items, hdr, norms); break;
+    case SV_UPDATE: k_sv_phase<SV_UPDATE><<<sv->grid, kSvUnit, 0, st>>>(items, hdr, norms); break;
+    default: return PB_ERR_ARG;
+    }
+    PB_LAUNCH_CHECK();
+    return PB_OK;
+}
+
+// One step's work for depth D, in stream order (captured into a graph).
+static int enqueue_step(pb_serve* sv, int D, cudaStream_t st)
+{
+    const std::vector<PhaseSlot> plan = phase_plan(sv->p, D);
+    int e;
+    for (size_t ph = 0; ph < plan.size(); ph++) {
+        const PhaseSlot& ps = plan[ph];
+        if (ps.op < 0) {
+            k_coarse_cycle_batch<float><<<sv->p.max_active, kCoarseThreads, sv->coarse_smem, st>>>(sv->d_cargs, sv->d_coffs,
+                                                                                                   sv->d_ccount);
+            PB_LAUNCH_CHECK();
+            continue;
+        }
+        if (ps.op == SV_K1) PB_CUDA(cudaMemsetAsync(sv->d_norms, 0, sizeof(double) * sv->p.max_active, st));
+        if ((e = launch_phase(sv, (int)ph, ps.op, sv->d_norms, st)) != PB_OK) return e;
+    }
+    PB_CUDA(cudaMemcpyAsync(sv->h_norms, sv->d_norms, sizeof(double) * sv->p.max_active, cudaMemcpyDeviceToHost, st));
+    return PB_OK;
+}
+
+static int admit(pb_serve* sv)
+{
+    while (!sv->waiting.empty()) {
+        int slot = -1;
+        for (int i = 0; i < (int)sv->slots.size(); i++)
+            if (!sv->slots[i]) {
+                slot = i;
+                break;
+            }
+        if (slot < 0) return PB_OK;
+        SvSolve& s = sv->solves[sv->waiting.front()];
+        const int n = s.req.n;
+        SvHier* h = nullptr;
+        auto it = sv->cache.find(n);
+        if (it != sv->cache.end()) {
+            h = it->second;
+            sv->cache.erase(it);
+        } else {
+            const size_t need = hier_bytes(n);
+            // make room by dropping idle hierarchies of other edges
+            while (sv->held + need > (size_t)sv->p.hbm_budget && !sv->cache.empty()) {
+                auto v = sv->cache.begin();
+                sv->held -= v->second->bytes;
+                hier_free(v->second);
+                sv->cache.erase(v);
+            }
+            if (sv->held + need > (size_t)sv->p.hbm_budget) return PB_OK;   // wait for memory
+            h = hier_alloc(n);
+            if (!h) return PB_OK;
+            sv->held += h->bytes;
+        }
+        sv->waiting.pop_front();
+        s.h = h;
+        s.slot = slot;
+        s.state = PB_SERVE_ACTIVE;
+        s.depth = batched_depth(h);
+        s.alpha_lv = level_alphas(s.req.alpha, h->nlev);
+        s.fresh = true;
+        sv->slots[slot] = s.ticket;
+        // initial guess zero, right-hand side in; constant alpha on the coarse levels
+        const size_t n3 = (size_t)n * n * n;
+        PB_CUDA(cudaMemsetAsync(h->u64, 0, sizeof(double) * (size_t)h->sxd * (n + 2) * (n + 2), sv->st));
+        PB_CUDA(cudaMemcpyAsync(h->f64, s.req.rhs, sizeof(double) * n3, cudaMemcpyHostToDevice, sv->st));
+        if (s.req.form == PB_MG_HELMHOLTZ)
+            for (int d = 0; d < h->nlev; d++)
+                if (h->alpha[d]) {
+                    const long long c = (long long)h->edge[d] * h->edge[d] * h->edge[d];
+                    k_sv_fill<<<grid_for(c, 256), 256, 0, sv->st>>>(h->alpha[d], c, s.alpha_lv[d]);
+                    PB_LAUNCH_CHECK();
+                }
+        sv->lists_dirty = true;
+    }
+    return PB_OK;
+}
+
+static void retire(pb_serve* sv, SvSolve& s, int state)
+{
+    SvHier* h = s.h;
+    const int n = h->n;
+    const size_t n3 = (size_t)n * n * n;
+    k_sv_pack_out<<<grid_for((long long)n3, 256), 256, 0, sv->st>>>(h->u64, h->f64, n, h->sxd);
+    cudaMemcpyAsync(s.req.out, h->f64, sizeof(double) * n3, cudaMemcpyDeviceToHost, sv->st);
+    s.state = state;
+    sv->slots[s.slot] = 0;
+    s.slot = -1;
+    s.h = nullptr;
+    sv->cache.insert({n, h});
+    sv->completed.push_back(s.ticket);
+    sv->lists_dirty = true;
+}
+
+extern "C" {
+
+int pb_serve_create(const pb_serve_params* p, pb_serve** out)
+{
+    if (!p || !out) return PB_ERR_ARG;
+    if (p->max_active < 1 || p->max_active > kSvMaxSolves || p->nu1 < 1 || p->nu2 < 1 || p->nu_bottom < 0 ||
+        p->hbm_budget <= 0 || !(p->tol > 0) || p->max_cycles < 1)
+        return PB_ERR_ARG;
+    pb_serve* sv = new (std::nothrow) pb_serve;
+    if (!sv) return PB_ERR_NOMEM;
+    sv->p = *p;
+    cudaGetDevice(&sv->device);
+    sv->slots.assign(p->max_active, 0);
+    sv->max_phases = phases_for(*p);
+    const size_t cap = (size_t)p->max_active;
+    bool ok = cudaStreamCreateWithFlags(&sv->st, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaMalloc(&sv->d_items, sizeof(SvItem) * cap * sv->max_phases) == cudaSuccess &&
+              cudaMalloc(&sv->d_hdr, sizeof(SvPhaseHeader) * sv->max_phases) == cudaSuccess &&
+              cudaMalloc(&sv->d_cargs, sizeof(CoarseArgs<float>) * cap) == cudaSuccess &&
+              cudaMalloc(&sv->d_coffs, sizeof(CoarseOffsets) * cap) == cudaSuccess &&
+              cudaMalloc(&sv->d_ccount, sizeof(int)) == cudaSuccess &&
+              cudaMalloc(&sv->d_norms, sizeof(double) * cap) == cudaSuccess &&
+              cudaMalloc(&sv->d_r0, sizeof(double) * cap) == cudaSuccess &&
+              cudaMallocHost(&sv->h_norms, sizeof(double) * cap) == cudaSuccess &&
+              cudaMallocHost(&sv->h_r0, sizeof(double) * cap) == cudaSuccess;
+    if (ok) {
+        sv->grid = cached_sm_count() * 8;
+        // coarse part: the largest arena (edge 16, Helmholtz) fits in shared memory
+        CoarseArgs<float> ca;
+        memset(&ca, 0, sizeof(ca));
+        int l = 0;
+        for (int e = kCoarseEdge; e >= 1; e /= 2, l++) {}
+        ca.top = l - 1;
+        for (int i = 0, e = 1; i < l; i++, e *= 2) {
+            ca.lv[i].k.n = e;
+            ca.lv[i].k.sx = grown_pitch<float>(e);
+        }
+        sv->coarse_smem = coarse_smem_layout(ca, 1, nullptr);
+        ok = cudaFuncSetAttribute(k_coarse_cycle_batch<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)sv->coarse_smem) == cudaSuccess;
+    }
+    if (!ok) {
+        cudaGetLastError();
+        pb_serve_destroy(sv);
+        return PB_ERR_NOMEM;
+    }
+    *out = sv;
+    return PB_OK;
+}
+
+int pb_serve_destroy(pb_serve* sv)
+{
+    if (!sv) return PB_OK;
+    if (sv->st) cudaStreamSynchronize(sv->st);
+    for (auto& g : sv->graphs) cudaGraphExecDestroy(g.second);
+    for (auto& s : sv->solves)
+        if (s.second.h) hier_free(s.second.h);
+    for (auto& c : sv->cache) hier_free(c.second);
+    cudaFree(sv->d_items);
+    cudaFree(sv->d_hdr);
+    cudaFree(sv->d_cargs);
+    cudaFree(sv->d_coffs);
+    cudaFree(sv->d_ccount);
+    cudaFree(sv->d_norms);
+    cudaFree(sv->d_r0);
+    cudaFreeHost(sv->h_norms);
+    cudaFreeHost(sv->h_r0);
+    if (sv->st) cudaStreamDestroy(sv->st);
+    delete sv;
+    return PB_OK;
+}
+
+int pb_serve_submit(pb_serve* sv, const pb_serve_request* q, long long* ticket)
+{
+    if (!sv || !q || !q->rhs || !q->out) return PB_ERR_ARG;
+    if (!edge_ok(q->n) || (q->form != PB_MG_POISSON && q->form != PB_MG_HELMHOLTZ)) return PB_ERR_ARG;
+    if (hier_bytes(q->n) > (size_t)sv->p.hbm_budget) return PB_ERR_BUDGET;
+    SvSolve s;
+    s.ticket = sv->next_ticket++;
+    s.req = *q;
+    if (s.req.form == PB_MG_POISSON) {
+        s.req.alpha = 0.0;
+        s.req.beta = 1.0;
+    }
+    sv->solves[s.ticket] = s;
+    sv->waiting.push_back(s.ticket);
+    if (ticket) *ticket = s.ticket;
+    return PB_OK;
+}
+
+int pb_serve_step(pb_serve* sv, int* active, int* waiting)
+{
+    if (!sv) return PB_ERR_ARG;
+    int e;
+    if ((e = admit(sv)) != PB_OK) return e;
+    bool any = false;
+    for (long long t : sv->slots) any = any || t;
+    if (any) {
+        if (sv->lists_dirty && (e = build_lists(sv)) != PB_OK) return e;
+        // first residual pass of the solves admitted since the last step
+        bool fresh = false;
+        for (long long t : sv->slots)
+            if (t && sv->solves[t].fresh) fresh = true;
+        if (fresh) {
+            PB_CUDA(cudaMemsetAsync(sv->d_r0, 0, sizeof(double) * sv->p.max_active, sv->st));
+            if ((e = launch_phase(sv, sv->max_phases - 1, SV_K1, sv->d_r0, sv->st)) != PB_OK) return e;
+            PB_CUDA(cudaMemcpyAsync(sv->h_r0, sv->d_r0, sizeof(double) * sv->p.max_active, cudaMemcpyDeviceToHost, sv->st));
+        }
+        const int D = std::max(sv->depth_now, 1);
+        auto g = sv->graphs.find(D);
+        if (g == sv->graphs.end()) {
+            cudaGraph_t graph;
+            PB_CUDA(cudaStreamBeginCapture(sv->st, cudaStreamCaptureModeThreadLocal));
+            e = enqueue_step(sv, D, sv->st);
+            cudaError_t ce = cudaStreamEndCapture(sv->st, &graph);
+            if (e != PB_OK) {
+                if (ce == cudaSuccess) cudaGraphDestroy(graph);
+                return e;
+            }
+            if (ce != cudaSuccess) { set_cuda_error(ce); return PB_ERR_CUDA; }
+            cudaGraphExec_t ex;
+            ce = cudaGraphInstantiate(&ex, graph, 0);
+            cudaGraphDestroy(graph);
+            if (ce != cudaSuccess) { set_cuda_error(ce); return PB_ERR_CUDA; }
+            g = sv->graphs.insert({D, ex}).first;
+        }
+        PB_CUDA(cudaGraphLaunch(g->second, sv->st));
+        PB_CUDA(cudaStreamSynchronize(sv->st));
+        if (read_error_serve() > 0) return PB_ERR_DEVICE;
+        // bookkeeping: converged or out of cycles -> copy out and free the slot
+        for (int i = 0; i < (int)sv->slots.size(); i++) {
+            const long long t = sv->slots[i];
+            if (!t) continue;
+            SvSolve& s = sv->solves[t];
+            if (s.fresh) {
+                s.r0 = sv->h_r0[i];
+                s.fresh = false;
+                sv->lists_dirty = true;
+            }
+            s.cycles++;
+            s.r = sv->h_norms[i];
+            if (s.r < sv->p.tol * s.r0) retire(sv, s, PB_SERVE_DONE);
+            else if (s.cycles >= sv->p.max_cycles) retire(sv, s, PB_SERVE_FAILED);
+        }
+        PB_CUDA(cudaStreamSynchronize(sv->st));   // results are on the host when step returns
+    }
+    int na = 0;
+    for (long long t : sv->slots) na += t ? 1 : 0;
+    if (active) *active = na;
+    if (waiting) *waiting = (int)sv->waiting.size();
+    return PB_OK;
+}
+
+int pb_serve_poll(pb_serve* sv, long long* tickets, int cap, int* n)
+{
+    if (!sv || !n || (cap > 0 && !tickets)) return PB_ERR_ARG;
+    const int k = std::min(cap, (int)sv->completed.size());
+    for (int i = 0; i < k; i++) tickets[i] = sv->completed[i];
+    sv->completed.erase(sv->completed.begin(), sv->completed.begin() + k);
+    *n = k;
+    return PB_OK;
+}
+
+int pb_serve_status(const pb_serve* sv, long long ticket, int* state, int* cycles, double* rel_res)
+{
+    if (!sv) return PB_ERR_ARG;
+    auto it = sv->solves.find(ticket);
+    if (it == sv->solves.end()) return PB_ERR_ARG;
+    const SvSolve& s = it->second;
+    if (state) *state = s.state;
+    if (cycles) *cycles = s.cycles;
+    if (rel_res) *rel_res = s.r0 > 0 ? s.r / s.r0 : 0.0;
+    return PB_OK;
+}
+
+long long pb_serve_device_bytes(const pb_serve* sv)
+{
+    return sv ? (long long)sv->held : -1;
+}
+
+long long pb_serve_request_bytes(int n)
+{
+    return edge_ok(n) ? (long long)hier_bytes(n) : -1;
+}
+
+} // extern "C"

@@ -107,3 +107,19 @@ def test_multigrid_parameter_rules():
         assert L.pb_mg_coarse_edge(-1) == -1
     finally:
         L.pb_mg_coarse_edge(16)
+
+
+def test_serve_host_rules():
+    L = pb.lib()
+    assert pb.Serve.request_bytes(33) == -1          # 33 does not halve down to <= 16
+    assert pb.Serve.request_bytes(15) == -1          # the top level must coarsen once
+    assert pb.Serve.request_bytes(16) > 0
+    assert pb.Serve.request_bytes(16 * 12) > 8 * 192 ** 3 * 2
+    assert pb.Serve.request_bytes(64) < pb.Serve.request_bytes(128)
+    h = ctypes.c_void_p()
+    bad = pb.pb_serve_params(1 << 30, 0, 4, 4, 10, 2.0 / 3.0, 1e-8, 100)   # no slots
+    assert L.pb_serve_create(ctypes.byref(bad), ctypes.byref(h)) == -1
+    bad = pb.pb_serve_params(1 << 30, 4, 0, 4, 10, 2.0 / 3.0, 1e-8, 100)   # nu1 = 0
+    assert L.pb_serve_create(ctypes.byref(bad), ctypes.byref(h)) == -1
+    bad = pb.pb_serve_params(0, 4, 4, 4, 10, 2.0 / 3.0, 1e-8, 100)         # no budget
+    assert L.pb_serve_create(ctypes.byref(bad), ctypes.byref(h)) == -1

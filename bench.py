@@ -11,6 +11,9 @@ restriction/prolongation pair stalls at depth (reference CPU path: 0.48, 0.72, 0
   e2e   : the same through the public API with host buffers: H2D of f, solve, D2H of u per step
   stencil: Stencil::apply 7-point FP64 on a 256^3 box (src 258^3), GB/s and fraction of HBM
   roofline: the dominant kernel, the finest-level Jacobi sweep (k_star_tma<Lap7, EpiRelax>)
+  mixed : the same problem with FP32 V-cycles inside FP64 residual/correction/norm
+  serving: a stream of Poisson/Helmholtz requests (edges 32..192) served by the batching engine vs
+          plain FP64 multigrid one request at a time (saturated and at the 200/s arrival rate)
 
 Multi-GPU (torchrun): every rank solves its own grid (replicas; no data-path collective), value is
 the whole-job rate. --impl reference times the reference's own CPU code (oracle/_ref) on host cores.
@@ -144,6 +147,34 @@ def _ref_cycle_time(reps):
     return R.mg_cs_time_cycles(N, 64, LEVELS, NU1, NU2, NU_BOTTOM, OMEGA, rho, reps)
 
 
+def run_serving(pb, count):
+    """Request stream of periodic Poisson/Helmholtz solves (Poisson arrivals at 200/s, seed 4; edge
+    log-uniform in [32, 192] rounded to 16; alpha ~ U[0, 1]; 4-mode right-hand sides; tolerance
+    1e-8). Served by the batching engine (mixed precision, in-flight solves advanced together) and
+    by plain FP64 multigrid one request at a time, both open loop at the arrival rate and saturated
+    (every request available at once). Host buffers are pinned for both."""
+    import numpy as np
+    from proto_b200 import serving as S
+    trace = S.make_trace(count=count)
+    pool = S.rhs_pool([r["n"] for r in trace])
+    eng = pb.Serve(150 << 30, max_active=64, tol=1e-8)
+    ring = S._Ring([r["n"] for r in trace], 12)
+    warm = trace[:min(len(trace), 400)]
+    S.serve_trace(pb, warm, pool, realtime=False, engine=eng, ring=ring)
+    S.fp64_trace(pb, warm[:100], pool, realtime=False)
+    out = {"workload": "%d requests, Poisson arrivals 200/s (seed 4), edge log-uniform [32,192] step 16, "
+                       "Poisson/Helmholtz 50/50, alpha~U[0,1], 4 sine modes, tol 1e-8" % count,
+           "hbm_budget_gb": 150, "max_active": 64}
+    for mode, rt in (("saturated", False), ("arrival_rate", True)):
+        a, ka = S.serve_trace(pb, trace, pool, realtime=rt, keep=20, engine=eng, ring=ring)
+        b, kb = S.fp64_trace(pb, trace, pool, realtime=rt, keep=20)
+        err = max(float(np.max(np.abs(ka[i] - kb[i])) / np.max(np.abs(kb[i]))) for i in ka)
+        out[mode] = {"served_mixed": a, "fp64_one_at_a_time": b,
+                     "solves_per_s_ratio": a["solves_per_s"] / b["solves_per_s"],
+                     "max_rel_diff_vs_fp64_first20": err}
+    return out
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -167,6 +198,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=2000)
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -318,6 +351,8 @@ def main():
     t_rx32 = a.elapsed_time(b) / 1000.0 / reps
     pb.device_check()
     value_m = world * args.steps / t_mx
+    # the serving replay is a one-GPU measurement (replicas add nothing to it)
+    serving = None if (args.no_serving or world > 1) else run_serving(pb, args.serve_requests)
     peak, peak_kind = measured_peaks()
     st_gbs = STENCIL_BYTES / t_st / 1e9
     rx_gbs = RELAX_BYTES / t_rx / 1e9
@@ -357,6 +392,8 @@ def main():
                       "relax_fp32_us": t_rx32 * 1e6, "relax_fp32_gbs": 12 * 256 ** 3 / t_rx32 / 1e9,
                       "gpu_launches": (2 + itm * mgm.launches_per_cycle() + 1) * args.steps},
         }
+        if serving is not None:
+            line["serving"] = serving
         if iters != CYCLES_PER_SOLVE:
             line["note"] = "cycles per solve %d differ from the %d the reference arm scales by" % (iters, CYCLES_PER_SOLVE)
         if world == 1 and not args.no_cpu_baseline:

@@ -72,8 +72,10 @@ struct pb_serve {
     // phase lists (device + host mirror)
     int max_phases = 0;
     SvItem* d_items = nullptr;
+    long long* d_unit0 = nullptr;       // per phase: first rows of its items (compact, for the search)
     SvPhaseHeader* d_hdr = nullptr;
     std::vector<SvItem> h_items;
+    std::vector<long long> h_unit0;
     std::vector<SvPhaseHeader> h_hdr;
     CoarseArgs<float>* d_cargs = nullptr;
     CoarseOffsets* d_coffs = nullptr;
@@ -132,7 +134,7 @@ size_t hier_bytes(int n)
     return b;
 }
 
-SvHier* hier_alloc(int n)
+SvHier* hier_alloc(int n, cudaStream_t st)
 {
     SvHier* h = new SvHier;
     h->n = n;
@@ -144,7 +146,7 @@ SvHier* hier_alloc(int n)
         float *a = nullptr, *b = nullptr, *r = nullptr, *al = nullptr;
         ok = ok && cudaMalloc(&a, g) == cudaSuccess && cudaMalloc(&b, g) == cudaSuccess && cudaMalloc(&r, c) == cudaSuccess;
         if (ok && e <= kCoarseEdge) ok = cudaMalloc(&al, c) == cudaSuccess;
-        if (ok) ok = cudaMemset(a, 0, g) == cudaSuccess && cudaMemset(b, 0, g) == cudaSuccess;
+        if (ok) ok = cudaMemsetAsync(a, 0, g, st) == cudaSuccess && cudaMemsetAsync(b, 0, g, st) == cudaSuccess;
         h->phi0.push_back(a);
         h->phi1.push_back(b);
         h->rhs.push_back(r);
@@ -253,7 +255,7 @@ std::vector<PhaseSlot> phase_plan(const pb_serve_params& p, int D)
 void add_item(std::vector<SvItem>& items, long long& total, SvItem it)
 {
     it.unit0 = total;
-    total += ((long long)it.units + kSvUnit - 1) / kSvUnit * kSvUnit;
+    total += ((long long)it.units + kSvRows - 1) / kSvRows * kSvRows;
     items.push_back(it);
 }
 
@@ -274,6 +276,7 @@ static int build_lists(pb_serve* sv)
     const std::vector<PhaseSlot> plan = phase_plan(p, std::max(D, 1));
     const int cap = (int)p.max_active;
     sv->h_items.assign((size_t)sv->max_phases * cap, SvItem{});
+    sv->h_unit0.assign((size_t)sv->max_phases * cap, 0);
     sv->h_hdr.assign(sv->max_phases, SvPhaseHeader{0, 0});
     // per solve: the buffer index of each level's current solution as the plan advances
     std::vector<std::vector<int>> cur(act.size());
@@ -312,14 +315,14 @@ static int build_lists(pb_serve* sv)
                 it.out = ph_[1 - c];
                 it.rhs = h.rhs[d];
                 it.c = lap7_coefs<float>(helm ? level_hsqinv(n, d) : p.omega / 6.0);
-                it.units = e * e * e;
+                it.units = e * e;
                 if (ps.op == SV_RELAX) c = 1 - c;
                 break;
             case SV_RELAX_FIRST:
                 c = 0;
                 it.out = ph_[1];
                 it.rhs = h.rhs[d];
-                it.units = e * e * e;
+                it.units = e * e;
                 c = 1;
                 break;
             case SV_RESTRICT: {
@@ -328,7 +331,7 @@ static int build_lists(pb_serve* sv)
                 it.rhs = h.rhs[d];
                 const double hs = level_hsqinv(n, d);
                 it.c = lap7_coefs<float>(helm ? hs : -hs);
-                it.units = (e / 2) * (e / 2) * (e / 2);
+                it.units = (e / 2) * (e / 2);
                 break;
             }
             case SV_PROLONG: {
@@ -338,7 +341,7 @@ static int build_lists(pb_serve* sv)
                 const int cc = dc >= s.depth ? 0 : cur[a][dc];
                 it.delta = cc ? h.phi1[dc] : h.phi0[dc];
                 it.sxc = h.sx[dc];
-                it.units = e * e * e;
+                it.units = e * e;
                 break;
             }
             case SV_K1: {
@@ -346,7 +349,7 @@ static int build_lists(pb_serve* sv)
                 it.out = h.rhs[0];
                 const double hs = level_hsqinv(n, 0);
                 it.c64 = lap7_coefs<double>(helm ? hs : -hs);
-                it.units = e * e * e;
+                it.units = e * e;
                 c = 1;
                 break;
             }
@@ -354,6 +357,7 @@ static int build_lists(pb_serve* sv)
             add_item(items, total, it);
         }
         std::copy(items.begin(), items.end(), sv->h_items.begin() + ph * cap);
+        for (size_t k = 0; k < items.size(); k++) sv->h_unit0[ph * cap + k] = items[k].unit0;
         sv->h_hdr[ph] = SvPhaseHeader{(long long)items.size(), total};
     }
     // the residual pass for freshly admitted solves (slot max_phases-1)
@@ -380,10 +384,11 @@ static int build_lists(pb_serve* sv)
             it.out = h.rhs[0];
             const double hs = level_hsqinv(h.n, 0);
             it.c64 = lap7_coefs<double>(helm ? hs : -hs);
-            it.units = h.n * h.n * h.n;
+            it.units = h.n * h.n;
             add_item(items, total, it);
         }
         std::copy(items.begin(), items.end(), sv->h_items.begin() + (size_t)ph * cap);
+        for (size_t k = 0; k < items.size(); k++) sv->h_unit0[(size_t)ph * cap + k] = items[k].unit0;
         sv->h_hdr[ph] = SvPhaseHeader{(long long)items.size(), total};
     }
     // coarse-cycle arguments (entry level = depth s.depth)
@@ -427,7 +432,13 @@ static int build_lists(pb_serve* sv)
         nc++;
     }
     (void)smem_max;
-    PB_CUDA(cudaMemcpyAsync(sv->d_items, sv->h_items.data(), sizeof(SvItem) * sv->h_items.size(), cudaMemcpyHostToDevice, sv->st));
+    // the phases of this depth's plan and the residual-pass slot (the last one)
+    const size_t used = plan.size() * cap;
+    PB_CUDA(cudaMemcpyAsync(sv->d_items, sv->h_items.data(), sizeof(SvItem) * used, cudaMemcpyHostToDevice, sv->st));
+    PB_CUDA(cudaMemcpyAsync(sv->d_unit0, sv->h_unit0.data(), sizeof(long long) * used, cudaMemcpyHostToDevice, sv->st));
+    const size_t last = (size_t)(sv->max_phases - 1) * cap;
+    PB_CUDA(cudaMemcpyAsync(sv->d_items + last, sv->h_items.data() + last, sizeof(SvItem) * cap, cudaMemcpyHostToDevice, sv->st));
+    PB_CUDA(cudaMemcpyAsync(sv->d_unit0 + last, sv->h_unit0.data() + last, sizeof(long long) * cap, cudaMemcpyHostToDevice, sv->st));
     PB_CUDA(cudaMemcpyAsync(sv->d_hdr, sv->h_hdr.data(), sizeof(SvPhaseHeader) * sv->h_hdr.size(), cudaMemcpyHostToDevice, sv->st));
     PB_CUDA(cudaMemcpyAsync(sv->d_cargs, sv->h_cargs.data(), sizeof(CoarseArgs<float>) * cap, cudaMemcpyHostToDevice, sv->st));
     PB_CUDA(cudaMemcpyAsync(sv->d_coffs, sv->h_coffs.data(), sizeof(CoarseOffsets) * cap, cudaMemcpyHostToDevice, sv->st));
@@ -440,14 +451,15 @@ static int build_lists(pb_serve* sv)
 static int launch_phase(pb_serve* sv, int slot, int op, double* norms, cudaStream_t st)
 {
     const SvItem* items = sv->d_items + (size_t)slot * sv->p.max_active;
+    const long long* u0 = sv->d_unit0 + (size_t)slot * sv->p.max_active;
     const SvPhaseHeader* hdr = sv->d_hdr + slot;
     switch (op) {
-    case SV_RELAX: k_sv_phase<SV_RELAX><<<sv->grid, kSvUnit, 0, st>>>(items, hdr, norms); break;
-    case SV_RELAX_FIRST: k_sv_phase<SV_RELAX_FIRST><<<sv->grid, kSvUnit, 0, st>>>(items, hdr, norms); break;
-    case SV_RESTRICT: k_sv_phase<SV_RESTRICT><<<sv->grid, kSvUnit, 0, st>>>(items, hdr, norms); break;
-    case SV_PROLONG: k_sv_phase<SV_PROLONG><<<sv->grid, kSvUnit, 0, st>>>(items, hdr, norms); break;
-    case SV_K1: k_sv_phase<SV_K1><<<sv->grid, kSvUnit, 0, st>>>(items, hdr, norms); break;
-    case SV_UPDATE: k_sv_phase<SV_UPDATE><<<sv->grid, kSvUnit, 0, st>>>(items, hdr, norms); break;
+    case SV_RELAX: k_sv_phase<SV_RELAX><<<sv->grid, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
+    case SV_RELAX_FIRST: k_sv_phase<SV_RELAX_FIRST><<<sv->grid, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
+    case SV_RESTRICT: k_sv_phase<SV_RESTRICT><<<sv->grid, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
+    case SV_PROLONG: k_sv_phase<SV_PROLONG><<<sv->grid, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
+    case SV_K1: k_sv_phase<SV_K1><<<sv->grid, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
+    case SV_UPDATE: k_sv_phase<SV_UPDATE><<<sv->grid, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
     default: return PB_ERR_ARG;
     }
     PB_LAUNCH_CHECK();
@@ -501,7 +513,7 @@ static int admit(pb_serve* sv)
                 sv->cache.erase(v);
             }
             if (sv->held + need > (size_t)sv->p.hbm_budget) return PB_OK;   // wait for memory
-            h = hier_alloc(n);
+            h = hier_alloc(n, sv->st);
             if (!h) return PB_OK;
             sv->held += h->bytes;
         }
@@ -562,6 +574,7 @@ int pb_serve_create(const pb_serve_params* p, pb_serve** out)
     const size_t cap = (size_t)p->max_active;
     bool ok = cudaStreamCreateWithFlags(&sv->st, cudaStreamNonBlocking) == cudaSuccess &&
               cudaMalloc(&sv->d_items, sizeof(SvItem) * cap * sv->max_phases) == cudaSuccess &&
+              cudaMalloc(&sv->d_unit0, sizeof(long long) * cap * sv->max_phases) == cudaSuccess &&
               cudaMalloc(&sv->d_hdr, sizeof(SvPhaseHeader) * sv->max_phases) == cudaSuccess &&
               cudaMalloc(&sv->d_cargs, sizeof(CoarseArgs<float>) * cap) == cudaSuccess &&
               cudaMalloc(&sv->d_coffs, sizeof(CoarseOffsets) * cap) == cudaSuccess &&
@@ -604,6 +617,7 @@ int pb_serve_destroy(pb_serve* sv)
         if (s.second.h) hier_free(s.second.h);
     for (auto& c : sv->cache) hier_free(c.second);
     cudaFree(sv->d_items);
+    cudaFree(sv->d_unit0);
     cudaFree(sv->d_hdr);
     cudaFree(sv->d_cargs);
     cudaFree(sv->d_coffs);

@@ -4,8 +4,10 @@
 // memory; the kernels are persistent (grid fixed, work read from the list), so a captured CUDA
 // graph of a whole cycle stays valid while solves come and go.
 //
-// Each item's work units (cells) start at a multiple of kSvUnit in the phase's index space, so a
-// block-wide chunk of kSvUnit units lies in one item: the block finds it with one binary search.
+// Work units are grid rows (one (y, z) pair; a restriction's rows are coarse rows). A block takes
+// kSvRows consecutive rows, one warp per row, lanes striding along x (coalesced). Each item's rows
+// start at a multiple of kSvRows, so a chunk lies in one item: the block finds it with one binary
+// search over the phase's compact array of first rows.
 // The per-cell arithmetic is the single-solve solver's (same helpers, same order), so a solve's
 // result does not depend on what else is in the batch.
 #pragma once
@@ -13,7 +15,8 @@
 
 namespace pb {
 
-constexpr int kSvUnit = 256;       // threads per block = units per chunk
+constexpr int kSvUnit = 256;       // threads per block
+constexpr int kSvRows = kSvUnit / 32;   // rows per chunk (one warp each)
 constexpr int kSvMaxSolves = 256;  // solves in flight at most
 
 struct SvItem {
@@ -32,22 +35,22 @@ struct SvItem {
     int sxc;               // prolong: coarse pitch
     int sxd;               // K1 / update: pitch of u64
     int slot;              // solve slot (norms)
-    int units;             // work units of this item
-    long long unit0;       // first unit (multiple of kSvUnit)
+    int units;             // rows of this item
+    long long unit0;       // first row (multiple of kSvRows)
 };
 
 struct SvPhaseHeader {
     long long count;       // items
-    long long total;       // units spanned (multiple of kSvUnit)
+    long long total;       // rows spanned (multiple of kSvRows)
 };
 
-// item holding the chunk that starts at unit w (items sorted by unit0)
-__device__ __forceinline__ int sv_find(const SvItem* items, int count, long long w)
+// item holding the chunk that starts at row w (first rows ascending, in a compact array)
+__device__ __forceinline__ int sv_find(const long long* __restrict__ unit0, int count, long long w)
 {
     int lo = 0, hi = count - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
-        if (items[mid].unit0 <= w) lo = mid;
+        if (__ldg(unit0 + mid) <= w) lo = mid;
         else hi = mid - 1;
     }
     return lo;
@@ -64,92 +67,111 @@ __device__ __forceinline__ void sv_cell(int i, int n, int& x, int& y, int& z)
 
 template <int OP>
 __global__ void __launch_bounds__(kSvUnit) k_sv_phase(const SvItem* __restrict__ items,
+                                                      const long long* __restrict__ unit0,
                                                       const SvPhaseHeader* __restrict__ hdr, double* norms)
 {
     const int count = (int)hdr->count;
     const long long total = hdr->total;
-    for (long long w0 = (long long)blockIdx.x * kSvUnit; w0 < total; w0 += (long long)gridDim.x * kSvUnit) {
-        const SvItem& it = items[sv_find(items, count, w0)];
-        const int i = (int)(w0 - it.unit0) + threadIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (long long w0 = (long long)blockIdx.x * kSvRows; w0 < total; w0 += (long long)gridDim.x * kSvRows) {
+        const SvItem& it = items[sv_find(unit0, count, w0)];
+        const int row = (int)(w0 - it.unit0) + warp;
         double m = 0.0;
-        if (i < it.units) {
+        if (row < it.units) {
             const int n = it.k.n, sx = it.k.sx;
-            int x, y, z;
-            sv_cell(i, n, x, y, z);
-            if constexpr (OP == SV_RELAX || OP == SV_UPDATE) {
-                const long long Sy = sx, Sz = (long long)sx * (n + 2);
-                const long long g = grown_index<float>(n, sx, x, y, z);
-                float acc = 0.f;
-#pragma unroll
-                for (int j = 0; j < ShapeLap7::NT; j++) {
-                    const long long o = ShapeLap7::off(j, 0) + Sy * ShapeLap7::off(j, 1) + Sz * ShapeLap7::off(j, 2);
-                    acc = dadd(acc, dmul(it.c.c[j], it.in[g + o]));
-                }
-                const float v = relax_value(it.k, acc, it.in[g], it.rhs[i], it.alpha);
-                if constexpr (OP == SV_RELAX) {
-                    store_periodic(it.out, n, sx, x, y, z, v);
-                } else {
-                    const long long gd = grown_index<double>(n, it.sxd, x, y, z);
-                    store_periodic(it.u64, n, it.sxd, x, y, z, dadd(it.u64[gd], (double)v));
-                }
-            } else if constexpr (OP == SV_RELAX_FIRST) {
-                store_periodic(it.out, n, sx, x, y, z, relax_value(it.k, 0.f, 0.f, it.rhs[i], it.alpha));
-            } else if constexpr (OP == SV_RESTRICT) {
-                // unit = coarse cell of the (n/2)^3 level below; 8 fine residuals in Box([0,1]^3) order
+            if constexpr (OP == SV_RESTRICT) {
+                // a row of coarse cells of the (n/2)^3 level below; 8 fine residuals each, Box([0,1]^3) order
                 const int nc = n / 2;
-                sv_cell(i, nc, x, y, z);
+                const int y = row % nc, z = row / nc;
                 const long long Sy = sx, Sz = (long long)sx * (n + 2);
-                float acc = 0.f;
+                float* out = it.out + (long long)row * nc;
+                for (int x = lane; x < nc; x += 32) {
+                    float acc = 0.f;
 #pragma unroll
-                for (int k = 0; k < 8; k++) {
-                    const int fx = 2 * x + (k & 1), fy = 2 * y + ((k >> 1) & 1), fz = 2 * z + (k >> 2);
-                    const int fi = fx + n * (fy + n * fz);
-                    const float r = fine_residual(it.in, grown_index<float>(n, sx, fx, fy, fz), Sy, Sz, it.rhs[fi],
-                                                  it.alpha, it.k.helm, it.c, it.beta);
-                    acc = dadd(acc, dmul(0.125f, r));
-                }
-                it.out[i] = acc;
-            } else if constexpr (OP == SV_PROLONG) {
-                const float d = it.delta[grown_index<float>(n / 2, it.sxc, x / 2, y / 2, z / 2)];
-                const long long g = grown_index<float>(n, sx, x, y, z);
-                store_periodic(it.in, n, sx, x, y, z, dadd(it.in[g], dmul(1.f, d)));
-            } else if constexpr (OP == SV_K1) {
-                // FP64 residual of u64, its max-norm, the FP32 right-hand side and the first FP32 sweep
-                const int sxd = it.sxd;
-                const long long Sy = sxd, Sz = (long long)sxd * (n + 2);
-                const long long g = grown_index<double>(n, sxd, x, y, z);
-                double res;
-                float al = 0.f;
-                if (!it.k.helm) {
-                    res = dadd(0.0, it.f64[i]);
-#pragma unroll
-                    for (int j = 0; j < ShapeLap7::NT; j++) {
-                        const long long o = ShapeLap7::off(j, 0) + Sy * ShapeLap7::off(j, 1) + Sz * ShapeLap7::off(j, 2);
-                        res = dadd(res, dmul(it.c64.c[j], it.u64[g + o]));
+                    for (int k = 0; k < 8; k++) {
+                        const int fx = 2 * x + (k & 1), fy = 2 * y + ((k >> 1) & 1), fz = 2 * z + (k >> 2);
+                        const int fi = fx + n * (fy + n * fz);
+                        const float r = fine_residual(it.in, grown_index<float>(n, sx, fx, fy, fz), Sy, Sz, it.rhs[fi],
+                                                      it.alpha, it.k.helm, it.c, it.beta);
+                        acc = dadd(acc, dmul(0.125f, r));
                     }
-                } else {
-                    double lp = 0.0;
-#pragma unroll
-                    for (int j = 0; j < ShapeLap7::NT; j++) {
-                        const long long o = ShapeLap7::off(j, 0) + Sy * ShapeLap7::off(j, 1) + Sz * ShapeLap7::off(j, 2);
-                        lp = dadd(lp, dmul(it.c64.c[j], it.u64[g + o]));
-                    }
-                    res = dsub(it.f64[i], dsub(dmul(it.alpha64, it.u64[g]), dmul(it.beta64, lp)));
-                    al = __double2float_rn(it.alpha64);
+                    out[x] = acc;
                 }
-                m = upd_abs(0.0, res);
-                const float r32 = __double2float_rn(res);
-                it.out[i] = r32;   // the level's rho
-                store_periodic(it.in, n, sx, x, y, z, relax_value(it.k, 0.f, 0.f, r32, al));
+            } else {
+                const int y = row % n, z = row / n;
+                const int ey = edge_code(y, n), ez = edge_code(z, n);
+                const long long g0 = grown_index<float>(n, sx, 0, y, z);   // valid cell x = 0 of the row
+                const long long i0 = (long long)row * n;                    // its n^3 index
+                if constexpr (OP == SV_RELAX || OP == SV_UPDATE) {
+                    const long long Sy = sx, Sz = (long long)sx * (n + 2);
+                    const long long gd0 = OP == SV_UPDATE ? grown_index<double>(n, it.sxd, 0, y, z) : 0;
+                    for (int x = lane; x < n; x += 32) {
+                        const long long g = g0 + x;
+                        float acc = 0.f;
+#pragma unroll
+                        for (int j = 0; j < ShapeLap7::NT; j++) {
+                            const long long o = ShapeLap7::off(j, 0) + Sy * ShapeLap7::off(j, 1) + Sz * ShapeLap7::off(j, 2);
+                            acc = dadd(acc, dmul(it.c.c[j], it.in[g + o]));
+                        }
+                        const float v = relax_value(it.k, acc, it.in[g], it.rhs[i0 + x], it.alpha);
+                        if constexpr (OP == SV_RELAX) {
+                            store_with_images(it.out, n, sx, it.out + g, edge_code(x, n), ey, ez, v);
+                        } else {
+                            double* q = it.u64 + gd0 + x;
+                            store_with_images(it.u64, n, it.sxd, q, edge_code(x, n), ey, ez, dadd(*q, (double)v));
+                        }
+                    }
+                } else if constexpr (OP == SV_RELAX_FIRST) {
+                    for (int x = lane; x < n; x += 32)
+                        store_with_images(it.out, n, sx, it.out + g0 + x, edge_code(x, n), ey, ez,
+                                          relax_value(it.k, 0.f, 0.f, it.rhs[i0 + x], it.alpha));
+                } else if constexpr (OP == SV_PROLONG) {
+                    const float* d = it.delta + grown_index<float>(n / 2, it.sxc, 0, y / 2, z / 2);
+                    for (int x = lane; x < n; x += 32) {
+                        float* q = it.in + g0 + x;
+                        store_with_images(it.in, n, sx, q, edge_code(x, n), ey, ez, dadd(*q, dmul(1.f, d[x / 2])));
+                    }
+                } else if constexpr (OP == SV_K1) {
+                    // FP64 residual of u64, its max-norm, the FP32 right-hand side and the first FP32 sweep
+                    const int sxd = it.sxd;
+                    const long long Sy = sxd, Sz = (long long)sxd * (n + 2);
+                    const long long gd0 = grown_index<double>(n, sxd, 0, y, z);
+                    const float al = it.k.helm ? __double2float_rn(it.alpha64) : 0.f;
+                    for (int x = lane; x < n; x += 32) {
+                        const long long g = gd0 + x;
+                        double res;
+                        if (!it.k.helm) {
+                            res = dadd(0.0, it.f64[i0 + x]);
+#pragma unroll
+                            for (int j = 0; j < ShapeLap7::NT; j++) {
+                                const long long o = ShapeLap7::off(j, 0) + Sy * ShapeLap7::off(j, 1) + Sz * ShapeLap7::off(j, 2);
+                                res = dadd(res, dmul(it.c64.c[j], it.u64[g + o]));
+                            }
+                        } else {
+                            double lp = 0.0;
+#pragma unroll
+                            for (int j = 0; j < ShapeLap7::NT; j++) {
+                                const long long o = ShapeLap7::off(j, 0) + Sy * ShapeLap7::off(j, 1) + Sz * ShapeLap7::off(j, 2);
+                                lp = dadd(lp, dmul(it.c64.c[j], it.u64[g + o]));
+                            }
+                            res = dsub(it.f64[i0 + x], dsub(dmul(it.alpha64, it.u64[g]), dmul(it.beta64, lp)));
+                        }
+                        m = upd_abs(m, res);
+                        const float r32 = __double2float_rn(res);
+                        it.out[i0 + x] = r32;   // the level's rho
+                        store_with_images(it.in, n, sx, it.in + g0 + x, edge_code(x, n), ey, ez,
+                                          relax_value(it.k, 0.f, 0.f, r32, al));
+                    }
+                }
             }
         }
         if constexpr (OP == SV_K1) {
-            // the chunk lies in one item: one max per warp, one atomic per warp
+            // a warp's row lies in one item: one max per warp, one atomic per warp
             for (int o = 16; o > 0; o >>= 1) {
                 const double w = __shfl_down_sync(0xffffffffu, m, o);
                 m = (m < w) ? w : m;
             }
-            if ((threadIdx.x & 31) == 0 && m > 0.0) atomic_max_nonneg(norms + it.slot, m);
+            if (lane == 0 && m > 0.0 && row < it.units) atomic_max_nonneg(norms + it.slot, m);
         }
     }
 }

@@ -253,6 +253,10 @@ int pb_serve_step(pb_serve* sv, int* active, int* waiting);
 int pb_serve_poll(pb_serve* sv, long long* tickets, int cap, int* n);
 /* state PB_SERVE_*, cycles run, last relative residual. */
 int pb_serve_status(const pb_serve* sv, long long ticket, int* state, int* cycles, double* rel_res);
+/* Host wall time spent so far per stage of pb_serve_step (seconds: admission, work-list build,
+ * first residual pass of new solves, the cycle graph including its wait, retirement) and the number
+ * of steps that ran a cycle. */
+int pb_serve_timing(const pb_serve* sv, double* seconds5, long long* steps);
 /* Bytes of hierarchies held (in use and cached for reuse). */
 long long pb_serve_device_bytes(const pb_serve* sv);
 /* Bytes one solve of edge n holds (-1 if n is not servable). */

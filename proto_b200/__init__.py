@@ -383,6 +383,13 @@ class Serve:
     def device_bytes(self):
         return lib().pb_serve_device_bytes(self._h)
 
+    def timing(self):
+        """Host seconds per step stage (admit, lists, first residual, cycle, retire) and steps."""
+        t = (_c_dbl * 5)()
+        n = _c_ll()
+        _check(lib().pb_serve_timing(self._h, t, ctypes.byref(n)), "pb_serve_timing")
+        return dict(zip(("admit", "lists", "first_residual", "cycle", "retire"), list(t)), steps=n.value)
+
     def run_until_idle(self, max_steps=100000):
         for _ in range(max_steps):
             a, w = self.step()

@@ -15,6 +15,7 @@
 // Reference counterpart: none (the reference runs one solve at a time, LevelMultigridSolver::solve,
 // include/utils/implem/Proto_LevelMultigridSolverImplem.H:85-123).
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <deque>
@@ -81,6 +82,7 @@ struct pb_serve {
     CoarseOffsets* d_coffs = nullptr;
     int* d_ccount = nullptr;
     std::vector<CoarseArgs<float>> h_cargs;
+    int h_ccount = 0;
     std::vector<CoarseOffsets> h_coffs;
     double* d_norms = nullptr;          // per slot: residual norm of the step
     double* d_r0 = nullptr;             // per slot: first residual norm
@@ -92,6 +94,8 @@ struct pb_serve {
     int depth_now = 0;
     int grid = 0;                       // persistent grid of the phase kernels
     size_t coarse_smem = 0;
+    double t_stage[5] = {0, 0, 0, 0, 0};   // host seconds: admit, lists, residual pass, cycle, retire
+    long long steps = 0;
 };
 
 namespace {
@@ -275,8 +279,10 @@ static int build_lists(pb_serve* sv)
     sv->depth_now = D;
     const std::vector<PhaseSlot> plan = phase_plan(p, std::max(D, 1));
     const int cap = (int)p.max_active;
-    sv->h_items.assign((size_t)sv->max_phases * cap, SvItem{});
-    sv->h_unit0.assign((size_t)sv->max_phases * cap, 0);
+    if (sv->h_items.size() != (size_t)sv->max_phases * cap) {
+        sv->h_items.assign((size_t)sv->max_phases * cap, SvItem{});
+        sv->h_unit0.assign((size_t)sv->max_phases * cap, 0);
+    }
     sv->h_hdr.assign(sv->max_phases, SvPhaseHeader{0, 0});
     // per solve: the buffer index of each level's current solution as the plan advances
     std::vector<std::vector<int>> cur(act.size());
@@ -442,8 +448,10 @@ static int build_lists(pb_serve* sv)
     PB_CUDA(cudaMemcpyAsync(sv->d_hdr, sv->h_hdr.data(), sizeof(SvPhaseHeader) * sv->h_hdr.size(), cudaMemcpyHostToDevice, sv->st));
     PB_CUDA(cudaMemcpyAsync(sv->d_cargs, sv->h_cargs.data(), sizeof(CoarseArgs<float>) * cap, cudaMemcpyHostToDevice, sv->st));
     PB_CUDA(cudaMemcpyAsync(sv->d_coffs, sv->h_coffs.data(), sizeof(CoarseOffsets) * cap, cudaMemcpyHostToDevice, sv->st));
-    PB_CUDA(cudaMemcpyAsync(sv->d_ccount, &nc, sizeof(int), cudaMemcpyHostToDevice, sv->st));
-    PB_CUDA(cudaStreamSynchronize(sv->st));   // host mirrors may change after return
+    sv->h_ccount = nc;
+    PB_CUDA(cudaMemcpyAsync(sv->d_ccount, &sv->h_ccount, sizeof(int), cudaMemcpyHostToDevice, sv->st));
+    // (copies from pageable host memory return once the source is staged, so the mirrors may be
+    // rebuilt right away)
     sv->lists_dirty = false;
     return PB_OK;
 }
@@ -652,12 +660,23 @@ int pb_serve_submit(pb_serve* sv, const pb_serve_request* q, long long* ticket)
 int pb_serve_step(pb_serve* sv, int* active, int* waiting)
 {
     if (!sv) return PB_ERR_ARG;
+    using clk = std::chrono::steady_clock;
+    auto lap = [](clk::time_point& t0) {
+        const clk::time_point t1 = clk::now();
+        const double s = std::chrono::duration<double>(t1 - t0).count();
+        t0 = t1;
+        return s;
+    };
+    clk::time_point t0 = clk::now();
     int e;
     if ((e = admit(sv)) != PB_OK) return e;
+    sv->t_stage[0] += lap(t0);
     bool any = false;
     for (long long t : sv->slots) any = any || t;
     if (any) {
+        sv->steps++;
         if (sv->lists_dirty && (e = build_lists(sv)) != PB_OK) return e;
+        sv->t_stage[1] += lap(t0);
         // first residual pass of the solves admitted since the last step
         bool fresh = false;
         for (long long t : sv->slots)
@@ -667,6 +686,7 @@ int pb_serve_step(pb_serve* sv, int* active, int* waiting)
             if ((e = launch_phase(sv, sv->max_phases - 1, SV_K1, sv->d_r0, sv->st)) != PB_OK) return e;
             PB_CUDA(cudaMemcpyAsync(sv->h_r0, sv->d_r0, sizeof(double) * sv->p.max_active, cudaMemcpyDeviceToHost, sv->st));
         }
+        sv->t_stage[2] += lap(t0);
         const int D = std::max(sv->depth_now, 1);
         auto g = sv->graphs.find(D);
         if (g == sv->graphs.end()) {
@@ -687,6 +707,7 @@ int pb_serve_step(pb_serve* sv, int* active, int* waiting)
         }
         PB_CUDA(cudaGraphLaunch(g->second, sv->st));
         PB_CUDA(cudaStreamSynchronize(sv->st));
+        sv->t_stage[3] += lap(t0);
         if (read_error_serve() > 0) return PB_ERR_DEVICE;
         // bookkeeping: converged or out of cycles -> copy out and free the slot
         for (int i = 0; i < (int)sv->slots.size(); i++) {
@@ -704,6 +725,7 @@ int pb_serve_step(pb_serve* sv, int* active, int* waiting)
             else if (s.cycles >= sv->p.max_cycles) retire(sv, s, PB_SERVE_FAILED);
         }
         PB_CUDA(cudaStreamSynchronize(sv->st));   // results are on the host when step returns
+        sv->t_stage[4] += lap(t0);
     }
     int na = 0;
     for (long long t : sv->slots) na += t ? 1 : 0;
@@ -731,6 +753,14 @@ int pb_serve_status(const pb_serve* sv, long long ticket, int* state, int* cycle
     if (state) *state = s.state;
     if (cycles) *cycles = s.cycles;
     if (rel_res) *rel_res = s.r0 > 0 ? s.r / s.r0 : 0.0;
+    return PB_OK;
+}
+
+int pb_serve_timing(const pb_serve* sv, double* seconds5, long long* steps)
+{
+    if (!sv || !seconds5) return PB_ERR_ARG;
+    for (int k = 0; k < 5; k++) seconds5[k] = sv->t_stage[k];
+    if (steps) *steps = sv->steps;
     return PB_OK;
 }
 

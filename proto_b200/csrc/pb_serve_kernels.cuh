@@ -91,8 +91,8 @@ __global__ void __launch_bounds__(kSvUnit) k_sv_phase(const SvItem* __restrict__
                     for (int k = 0; k < 8; k++) {
                         const int fx = 2 * x + (k & 1), fy = 2 * y + ((k >> 1) & 1), fz = 2 * z + (k >> 2);
                         const int fi = fx + n * (fy + n * fz);
-                        const float r = fine_residual(it.in, grown_index<float>(n, sx, fx, fy, fz), Sy, Sz, it.rhs[fi],
-                                                      it.alpha, it.k.helm, it.c, it.beta);
+                        const float r = fine_residual<float>(it.in, grown_index<float>(n, sx, fx, fy, fz), Sy, Sz,
+                                                             it.rhs[fi], it.alpha, it.k.helm, it.c, it.beta);
                         acc = dadd(acc, dmul(0.125f, r));
                     }
                     out[x] = acc;

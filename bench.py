@@ -12,6 +12,7 @@ restriction/prolongation pair stalls at depth (reference CPU path: 0.48, 0.72, 0
   stencil: Stencil::apply 7-point FP64 on a 256^3 box (src 258^3), GB/s and fraction of HBM
   roofline: the dominant kernel, the finest-level Jacobi sweep (k_star_tma<Lap7, EpiRelax>)
   mixed : the same problem with FP32 V-cycles inside FP64 residual/correction/norm
+  amr_level: 100 steps of exchange + 13-point Euler update over a 512-patch uneven level
   serving: a stream of Poisson/Helmholtz requests (edges 32..192) served by the batching engine vs
           plain FP64 multigrid one request at a time (saturated and at the 200/s arrival rate)
 
@@ -147,6 +148,82 @@ def _ref_cycle_time(reps):
     return R.mg_cs_time_cycles(N, 64, LEVELS, NU1, NU2, NU_BOTTOM, OMEGA, rho, reps)
 
 
+def profile_kernels(pb, torch):
+    """One launch each of the bench's roofline kernels on 256^3 data: the FP64 Jacobi sweep, the
+    FP32 sweep of the mixed-precision solver and the 7-point Stencil::apply."""
+    offs = [(0, 0, 0), (1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1)]
+    S = pb.Stencil([-6.0, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0], offs)
+    src = torch.rand(258 ** 3, dtype=torch.float64, device="cuda")
+    dst = torch.empty(256 ** 3, dtype=torch.float64, device="cuda")
+    mg64 = pb.Multigrid(pb.MGParams(n=N, levels=LEVELS, nu1=NU1, nu2=NU2))
+    mg32 = pb.Multigrid(pb.MGParams(n=N, levels=LEVELS, nu1=NU1, nu2=NU2, precision=pb.MG_MIXED))
+    mg64.relax(1)
+    mg32.relax(1)
+    S.apply(src, pb.Box.cube(256).grow(1), dst, pb.Box.cube(256), scale=65536.0)
+    torch.cuda.synchronize()
+    pb.device_check()
+
+
+LAP13_OFFS = [(1, 0, 0), (0, 0, 0), (-1, 0, 0), (2, 0, 0), (-2, 0, 0), (0, 1, 0), (0, -1, 0), (0, 2, 0), (0, -2, 0),
+              (0, 0, 1), (0, 0, -1), (0, 0, 2), (0, 0, -2)]
+LAP13_COEFS = [4.0 / 3, -7.5, 4.0 / 3, -1.0 / 12, -1.0 / 12] + [4.0 / 3, 4.0 / 3, -1.0 / 12, -1.0 / 12] * 2
+
+
+def run_amr_level(pb, torch, steps=100, reps=5):
+    """Uneven AMR level: 512 patches (per-axis widths from {16,24,32,48,64}, seed 2) tiling a
+    periodic domain, 2 ghost cells, u ~ U[-1,1]; a step = ghost exchange + u += dt*L13(u) (4th-order
+    13-point Laplacian, dt = 0.1 h^2) over every patch; 100 steps as one captured graph, tiles
+    autotuned per patch-size class. Algorithmic bytes: 16 B per interior cell per step."""
+    from proto_b200 import workloads as W
+    widths = W.amr_widths(seed=2)
+    boxes, L = W.amr_patches(widths)
+    lv = pb.Level([pb.Box(*b) for b in boxes], 2, pb.Box((0, 0, 0), [v - 1 for v in L]), (1, 1, 1))
+    S = pb.Stencil(LAP13_COEFS, LAP13_OFFS)
+    interior = sum((b[1][0] - b[0][0] + 1) * (b[1][1] - b[0][1] + 1) * (b[1][2] - b[0][2] + 1) for b in boxes)
+    a = torch.rand(lv.slab_elems, dtype=torch.float64, device="cuda") * 2 - 1
+    b = torch.zeros_like(a)
+    h = 1.0 / L[0]
+    scale, dt = 1.0 / (h * h), 0.1 * h * h
+    lv.autotune(S, a, b, scale=scale)
+    lv.steps(S, pb.EPI_EULER, a, b, steps, scale=scale, a=dt)     # capture + warm
+    torch.cuda.synchronize()
+    st = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(reps):
+        lv.steps(S, pb.EPI_EULER, a, b, steps, scale=scale, a=dt)
+    e1.record(st)
+    torch.cuda.synchronize()
+    pb.device_check()
+    t = e0.elapsed_time(e1) / 1000.0 / (reps * steps)
+    peak, _ = measured_peaks()
+    out = {"workload": "512 patches, domain %dx%dx%d, 2 ghosts, 13-point 4th-order, u += dt*L(u), %d steps per "
+                       "graph launch" % (L[0], L[1], L[2], steps),
+           "interior_cells": interior, "us_per_step": t * 1e6, "steps_per_s": 1.0 / t,
+           "gpts_per_s": interior / t / 1e9, "gbs_algorithmic": 16.0 * interior / t / 1e9,
+           "frac_of_hbm": 16.0 * interior / t / 1e9 / peak, "tiles": lv.tiles(),
+           "gpu_launches_per_step": 2}
+    try:   # the reference's own per-patch stepping on one host core, one step
+        from oracle.oracle import Ref
+        if Ref.available():
+            import numpy as np
+            data = np.zeros(lv.slab_elems)
+            parts, off = [], 0
+            for p, o in zip(lv.patches, lv.offsets):
+                n = int(np.prod([p.size(d) + 4 for d in range(3)]))
+                parts.append(data[o:o + n])
+            cat = np.concatenate(parts)
+            t0 = time.perf_counter()
+            Ref().level13_steps(widths, 2, h, dt, 1, cat)
+            tc = time.perf_counter() - t0
+            out["cpu_baseline"] = {"value": 1.0 / tc, "unit": "steps/s", "cores": 1, "kind": "reference",
+                                   "sample": "1 step of the same level with the reference's BoxData/copyTo/Stencil "
+                                             "code (oracle/_ref), single-threaded"}
+    except Exception as e:   # the baseline never hides the GPU result
+        out["cpu_baseline"] = {"error": str(e)}
+    return out
+
+
 def run_serving(pb, count):
     """Request stream of periodic Poisson/Helmholtz solves (Poisson arrivals at 200/s, seed 4; edge
     log-uniform in [32, 192] rounded to 16; alpha ~ U[0, 1]; 4-mode right-hand sides; tolerance
@@ -199,6 +276,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--profile-kernels", action="store_true",
+                    help="run one 256^3 FP64 sweep, one FP32 sweep and one Stencil::apply, then exit (for ncu)")
     ap.add_argument("--serve-requests", type=int, default=2000)
     args = ap.parse_args()
 
@@ -212,6 +291,8 @@ def main():
     import proto_b200 as pb
     from proto_b200 import workloads as W
     torch.cuda.set_device(local)
+    if args.profile_kernels:
+        return profile_kernels(pb, torch)
     dist = None
     if world > 1:
         import torch.distributed as dist
@@ -351,6 +432,7 @@ def main():
     t_rx32 = a.elapsed_time(b) / 1000.0 / reps
     pb.device_check()
     value_m = world * args.steps / t_mx
+    amr = None if world > 1 else run_amr_level(pb, torch)
     # the serving replay is a one-GPU measurement (replicas add nothing to it)
     serving = None if (args.no_serving or world > 1) else run_serving(pb, args.serve_requests)
     peak, peak_kind = measured_peaks()
@@ -392,6 +474,8 @@ def main():
                       "relax_fp32_us": t_rx32 * 1e6, "relax_fp32_gbs": 12 * 256 ** 3 / t_rx32 / 1e9,
                       "gpu_launches": (2 + itm * mgm.launches_per_cycle() + 1) * args.steps},
         }
+        if amr is not None:
+            line["amr_level"] = amr
         if serving is not None:
             line["serving"] = serving
         if iters != CYCLES_PER_SOLVE:

@@ -160,6 +160,19 @@ int pb_level_exchange_f64(const pb_level* lv, double* slab, void* stream);
  * same level. */
 int pb_level_stencil_f64(const pb_level* lv, const pb_stencil* s, int epilogue, const double* u_slab,
                          double* out_slab, double scale, double a, void* stream);
+/* 'steps' steps of exchange(u_slab), out = u + a*S(u) (PB_EPI_EULER) or S(u) (0), swap, over
+ * every patch; the result ends in u_slab (tmp_slab is scratch of the same size). The launches are
+ * captured into one CUDA graph on the first call and replayed while the arguments stay the same.
+ * Each step is bitwise the pair pb_level_exchange_f64 + pb_level_stencil_f64. No counterpart in
+ * the reference, whose callers loop over exchange and per-patch stencils on the host. */
+int pb_level_steps_f64(pb_level* lv, const pb_stencil* s, int epilogue, double* u_slab, double* tmp_slab,
+                       double scale, double a, int steps, void* stream);
+/* Times the batched stencil per patch-size class (valid x extent) over a few tile shapes (columns
+ * along x, planes per thread) and keeps the fastest per class (blocks until done; out_slab is
+ * overwritten). pb_level_tiles reports the choice as (x extent, columns, planes) triples. */
+int pb_level_autotune_f64(pb_level* lv, const pb_stencil* s, const double* u_slab, double* out_slab,
+                          double scale, void* stream);
+int pb_level_tiles(const pb_level* lv, int* triples, int cap, int* n);
 
 /* ---- Point-Jacobi multigrid (reference: LevelMultigridSolver, include/utils/implem/
  * Proto_LevelMultigridSolverImplem.H:85-433, and the archived LevelMultigrid,

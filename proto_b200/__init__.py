@@ -286,6 +286,22 @@ class Level:
         _check(lib().pb_level_stencil_f64(self._h, stencil._h, _c_int(epilogue), _ptr(u_slab), _ptr(out_slab),
                                           _c_dbl(scale), _c_dbl(a), _stream(stream)), "pb_level_stencil_f64")
 
+    def steps(self, stencil, epilogue, u_slab, tmp_slab, nsteps, scale=1.0, a=0.0, stream=None):
+        """nsteps of exchange + stencil step as one captured graph; the result ends in u_slab."""
+        _check(lib().pb_level_steps_f64(self._h, stencil._h, _c_int(epilogue), _ptr(u_slab), _ptr(tmp_slab),
+                                        _c_dbl(scale), _c_dbl(a), _c_int(nsteps), _stream(stream)),
+               "pb_level_steps_f64")
+
+    def autotune(self, stencil, u_slab, out_slab, scale=1.0, stream=None):
+        _check(lib().pb_level_autotune_f64(self._h, stencil._h, _ptr(u_slab), _ptr(out_slab), _c_dbl(scale),
+                                           _stream(stream)), "pb_level_autotune_f64")
+
+    def tiles(self):
+        buf = (_c_int * 96)()
+        n = _c_int()
+        _check(lib().pb_level_tiles(self._h, buf, _c_int(32), ctypes.byref(n)), "pb_level_tiles")
+        return [(buf[3 * k], buf[3 * k + 1], buf[3 * k + 2]) for k in range(n.value)]
+
     def __del__(self):
         if getattr(self, "_h", None) and _LIB is not None:
             _LIB.pb_level_destroy(self._h)

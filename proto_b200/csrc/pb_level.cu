@@ -9,6 +9,7 @@
 // allowed, periodic images included) and one kernel launch executes every item of the level.
 #include <algorithm>
 #include <cstring>
+#include <map>
 #include <vector>
 
 #include "pb_internal.cuh"
@@ -41,36 +42,53 @@ __global__ void __launch_bounds__(256) k_exchange(double* slab, const MotionItem
     }
 }
 
-// One tile = a run of whole z-planes of one patch's valid box.
+// One tile = a (tx x ty) block of (x, y) columns of one patch's valid box, each column walked over
+// zd planes by one thread. The tile shape is chosen per patch-size class (the x extent of the
+// valid box) by pb_level_autotune; the default is 16 x 16 columns, 8 planes deep.
 struct PatchTile {
     long long off;             // slab offset of the patch
-    int glo[3], gS[3];         // grown box low corner and extents
-    int vlo[3], vn[3];         // valid box low corner and extents
-    int z0, nz;                // planes of the valid box this tile covers
+    int gS[3];                 // grown box extents
+    int gh[3];                 // ghost widths (valid cell (0,0,0) sits at grown (gh0, gh1, gh2))
+    int vn[3];                 // valid box extents
+    int x0, y0, z0;            // tile origin in valid coordinates
+    int tx, zd;                // columns along x (ty = 256 / tx) and planes per thread
 };
 
+constexpr int kLevelThreads = 256;
+
+// out = u + a*S(u) (euler) or S(u) on the tile's points. z neighbours come from a (2R+1)-deep
+// register window per column; x/y neighbours from global memory (L1). Terms are summed in the
+// stencil's insertion order, so results are bitwise the one-point-per-thread kernel's.
 template <class S>
-__global__ void __launch_bounds__(256) k_level_star(const double* __restrict__ u, double* out,
-                                                    const PatchTile* __restrict__ tiles, Coefs<double> cf, double a,
-                                                    int euler)
+__global__ void __launch_bounds__(kLevelThreads) k_level_star(const double* __restrict__ u, double* out,
+                                                              const PatchTile* __restrict__ tiles, Coefs<double> cf,
+                                                              double a, int euler)
 {
+    constexpr int R = S::R, W = 2 * R + 1;
     const PatchTile t = tiles[blockIdx.x];
+    const int lx = threadIdx.x % t.tx, ly = threadIdx.x / t.tx;
+    const int x = t.x0 + lx, y = t.y0 + ly;
+    if (x >= t.vn[0] || y >= t.vn[1]) return;
     const long long Sx = t.gS[0], Sxy = (long long)t.gS[0] * t.gS[1];
-    const long long total = (long long)t.vn[0] * t.vn[1] * t.nz;
-    for (long long i = threadIdx.x; i < total; i += blockDim.x) {
-        int x = (int)(i % t.vn[0]);
-        long long q = i / t.vn[0];
-        int y = (int)(q % t.vn[1]);
-        int z = t.z0 + (int)(q / t.vn[1]);
-        long long gi = t.off + (x + t.vlo[0] - t.glo[0]) + Sx * (y + t.vlo[1] - t.glo[1]) + Sxy * (z + t.vlo[2] - t.glo[2]);
+    const int z1 = min(t.z0 + t.zd, t.vn[2]);
+    const double* col = u + t.off + (x + t.gh[0]) + Sx * (y + t.gh[1]) + Sxy * t.gh[2];   // (x, y, z = 0)
+    double* ocol = out + t.off + (x + t.gh[0]) + Sx * (y + t.gh[1]) + Sxy * t.gh[2];
+    double win[W];
+#pragma unroll
+    for (int k = 0; k < 2 * R; k++) win[k] = __ldg(col + Sxy * (t.z0 - R + k));
+    for (int z = t.z0; z < z1; z++) {
+        win[2 * R] = __ldg(col + Sxy * (z + R));
+        const double* c = col + Sxy * z;
         double acc = 0.0;
 #pragma unroll
         for (int j = 0; j < S::NT; j++) {
-            const long long o = S::off(j, 0) + Sx * S::off(j, 1) + Sxy * S::off(j, 2);
-            acc = dadd(acc, dmul(cf.c[j], __ldg(u + gi + o)));
+            const int ox = S::off(j, 0), oy = S::off(j, 1), oz = S::off(j, 2);
+            const double v = (oz != 0 || (ox == 0 && oy == 0)) ? win[R + oz] : __ldg(c + ox + Sx * oy);
+            acc = dadd(acc, dmul(cf.c[j], v));
         }
-        double c = __ldg(u + gi);
-        out[gi] = euler ? dadd(c, dmul(a, acc)) : acc;
+        ocol[Sxy * z] = euler ? dadd(win[R], dmul(a, acc)) : acc;
+#pragma unroll
+        for (int k = 0; k < 2 * R; k++) win[k] = win[k + 1];
     }
 }
 
@@ -89,6 +107,10 @@ struct pb_level {
     std::vector<pb::PatchTile> tiles;
     pb::PatchTile* d_tiles = nullptr;
     int device = 0;
+    std::map<int, std::pair<int, int>> tune;   // valid x extent -> (tx, zd)
+    // captured multi-step graph and what it was captured for
+    cudaGraphExec_t graph = nullptr;
+    std::vector<double> graph_key;
 };
 
 using namespace pb;
@@ -143,28 +165,88 @@ static void build_items(pb_level* lv)
     }
 }
 
-static void build_tiles(pb_level* lv)
+static std::pair<int, int> tile_shape(const pb_level* lv, int nx)
 {
+    auto it = lv->tune.find(nx);
+    return it != lv->tune.end() ? it->second : std::make_pair(16, 8);
+}
+
+static void build_tiles(pb_level* lv, int only_nx = -1)
+{
+    lv->tiles.clear();
     const int np = (int)lv->patches.size();
     for (int i = 0; i < np; i++) {
         const Box3& v = lv->patches[i];
         PatchTile t;
         t.off = lv->offsets[i];
         for (int d = 0; d < 3; d++) {
-            t.glo[d] = v.lo[d] - lv->ghost[d];
+            t.gh[d] = lv->ghost[d];
             t.gS[d] = (int)bsize(v, d) + 2 * lv->ghost[d];
-            t.vlo[d] = v.lo[d];
             t.vn[d] = (int)bsize(v, d);
         }
-        // about 4K points per tile
-        int plane = t.vn[0] * t.vn[1];
-        int nzt = std::max(1, 4096 / std::max(1, plane));
-        for (int z0 = 0; z0 < t.vn[2]; z0 += nzt) {
-            t.z0 = z0;
-            t.nz = std::min(nzt, t.vn[2] - z0);
-            lv->tiles.push_back(t);
-        }
+        if (only_nx >= 0 && t.vn[0] != only_nx) continue;
+        const std::pair<int, int> sh = tile_shape(lv, t.vn[0]);
+        t.tx = sh.first;
+        t.zd = sh.second;
+        const int ty = kLevelThreads / t.tx;
+        for (int z0 = 0; z0 < t.vn[2]; z0 += t.zd)
+            for (int y0 = 0; y0 < t.vn[1]; y0 += ty)
+                for (int x0 = 0; x0 < t.vn[0]; x0 += t.tx) {
+                    t.x0 = x0;
+                    t.y0 = y0;
+                    t.z0 = z0;
+                    lv->tiles.push_back(t);
+                }
     }
+}
+
+static int upload_tiles(pb_level* lv)
+{
+    cudaFree(lv->d_tiles);
+    lv->d_tiles = nullptr;
+    if (lv->tiles.empty()) return PB_OK;
+    if (cudaMalloc(&lv->d_tiles, lv->tiles.size() * sizeof(PatchTile)) != cudaSuccess ||
+        cudaMemcpy(lv->d_tiles, lv->tiles.data(), lv->tiles.size() * sizeof(PatchTile), cudaMemcpyHostToDevice) !=
+            cudaSuccess) {
+        cudaGetLastError();
+        return PB_ERR_CUDA;
+    }
+    return PB_OK;
+}
+
+static void drop_graph(pb_level* lv)
+{
+    if (lv->graph) cudaGraphExecDestroy(lv->graph);
+    lv->graph = nullptr;
+    lv->graph_key.clear();
+}
+
+// stencil coefficients (scale folded in) and its shape; PB_OK or an error status
+static int level_coefs(const pb_level* lv, const pb_stencil* s, double scale, Coefs<double>& cf, int& shape)
+{
+    int nterms = 0;
+    pb_box span;
+    shape = 0;
+    pb_stencil_info(s, &nterms, &span, &shape);
+    if (shape != 1 && shape != 2) return PB_ERR_UNSUPPORTED;
+    for (int d = 0; d < 3; d++)
+        if (-span.lo[d] > lv->ghost[d] || span.hi[d] > lv->ghost[d]) return PB_ERR_GHOST;
+    double c[13];
+    stencil_coefs(s, c, 13);
+    for (int j = 0; j < 13; j++) cf.c[j] = 0.0;
+    for (int j = 0; j < nterms; j++) cf.c[j] = (scale != 1.0) ? c[j] * scale : c[j];
+    return PB_OK;
+}
+
+static int launch_level_star(const pb_level* lv, int shape, const double* u, double* out, const Coefs<double>& cf,
+                             double a, int euler, cudaStream_t st)
+{
+    const unsigned nb = (unsigned)lv->tiles.size();
+    if (nb == 0) return PB_OK;
+    if (shape == 1) k_level_star<ShapeLap7><<<nb, kLevelThreads, 0, st>>>(u, out, lv->d_tiles, cf, a, euler);
+    else k_level_star<ShapeLap13><<<nb, kLevelThreads, 0, st>>>(u, out, lv->d_tiles, cf, a, euler);
+    PB_LAUNCH_CHECK();
+    return PB_OK;
 }
 
 extern "C" {
@@ -206,11 +288,8 @@ int pb_level_create(const pb_box* patches, int npatch, const int ghost[3], pb_bo
             return PB_ERR_CUDA;
         }
     }
-    if (cudaMalloc(&lv->d_tiles, lv->tiles.size() * sizeof(PatchTile)) != cudaSuccess ||
-        cudaMemcpy(lv->d_tiles, lv->tiles.data(), lv->tiles.size() * sizeof(PatchTile), cudaMemcpyHostToDevice) !=
-            cudaSuccess) {
+    if (upload_tiles(lv) != PB_OK) {
         cudaFree(lv->d_items);
-        cudaFree(lv->d_tiles);
         delete lv;
         return PB_ERR_CUDA;
     }
@@ -221,6 +300,7 @@ int pb_level_create(const pb_box* patches, int npatch, const int ghost[3], pb_bo
 int pb_level_destroy(pb_level* lv)
 {
     if (!lv) return PB_OK;
+    drop_graph(lv);
     cudaFree(lv->d_items);
     cudaFree(lv->d_tiles);
     delete lv;
@@ -251,21 +331,138 @@ int pb_level_stencil_f64(const pb_level* lv, const pb_stencil* s, int epilogue, 
     if (!lv || !s || !u_slab || !out_slab) return PB_ERR_ARG;
     if (epilogue != 0 && epilogue != PB_EPI_EULER) return PB_ERR_ARG;
     if (lv->ncomp != 1) return PB_ERR_UNSUPPORTED;
-    int nterms = 0, shape = 0;
-    pb_box span;
-    pb_stencil_info(s, &nterms, &span, &shape);
-    if (shape != 1 && shape != 2) return PB_ERR_UNSUPPORTED;
-    for (int d = 0; d < 3; d++)
-        if (-span.lo[d] > lv->ghost[d] || span.hi[d] > lv->ghost[d]) return PB_ERR_GHOST;
-    double c[13];
-    stencil_coefs(s, c, 13);
     Coefs<double> cf;
-    for (int j = 0; j < nterms; j++) cf.c[j] = (scale != 1.0) ? c[j] * scale : c[j];
+    int shape, e;
+    if ((e = level_coefs(lv, s, scale, cf, shape)) != PB_OK) return e;
+    return launch_level_star(lv, shape, u_slab, out_slab, cf, a, epilogue == PB_EPI_EULER, (cudaStream_t)stream);
+}
+
+// 'steps' steps of: exchange(u), out = u + a*S(u) (or S(u)), swap; the result ends in u_slab. The
+// launches are captured into one CUDA graph on the first call and replayed while the arguments
+// stay the same (the graph holds the slab pointers).
+int pb_level_steps_f64(pb_level* lv, const pb_stencil* s, int epilogue, double* u_slab, double* tmp_slab, double scale,
+                       double a, int steps, void* stream)
+{
+    if (!lv || !s || !u_slab || !tmp_slab || steps < 0 || u_slab == tmp_slab) return PB_ERR_ARG;
+    if (epilogue != 0 && epilogue != PB_EPI_EULER) return PB_ERR_ARG;
+    if (lv->ncomp != 1) return PB_ERR_UNSUPPORTED;
+    if (steps == 0) return PB_OK;
+    Coefs<double> cf;
+    int shape, e;
+    if ((e = level_coefs(lv, s, scale, cf, shape)) != PB_OK) return e;
     cudaStream_t st = (cudaStream_t)stream;
-    unsigned nb = (unsigned)lv->tiles.size();
-    if (shape == 1) k_level_star<ShapeLap7><<<nb, 256, 0, st>>>(u_slab, out_slab, lv->d_tiles, cf, a, epilogue == PB_EPI_EULER);
-    else k_level_star<ShapeLap13><<<nb, 256, 0, st>>>(u_slab, out_slab, lv->d_tiles, cf, a, epilogue == PB_EPI_EULER);
-    PB_LAUNCH_CHECK();
+    std::vector<double> key = {(double)(uintptr_t)u_slab, (double)(uintptr_t)tmp_slab, scale, a, (double)epilogue,
+                               (double)steps, (double)shape, (double)(uintptr_t)lv->d_tiles};
+    for (int j = 0; j < 13; j++) key.push_back(cf.c[j]);
+    if (!lv->graph || key != lv->graph_key) {
+        drop_graph(lv);
+        cudaStream_t cs;
+        PB_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        cudaGraph_t g;
+        cudaError_t ce = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+        if (ce != cudaSuccess) { cudaStreamDestroy(cs); set_cuda_error(ce); return PB_ERR_CUDA; }
+        double* a_ = u_slab;
+        double* b_ = tmp_slab;
+        for (int k = 0; k < steps && e == PB_OK; k++) {
+            if (!lv->items.empty()) {
+                k_exchange<<<(unsigned)lv->items.size(), 256, 0, cs>>>(a_, lv->d_items, lv->ncomp);
+                if (cudaGetLastError() != cudaSuccess) e = PB_ERR_CUDA;
+            }
+            if (e == PB_OK) e = launch_level_star(lv, shape, a_, b_, cf, a, epilogue == PB_EPI_EULER, cs);
+            std::swap(a_, b_);
+        }
+        if (e == PB_OK && (steps & 1))
+            if (cudaMemcpyAsync(u_slab, tmp_slab, sizeof(double) * lv->slab_elems, cudaMemcpyDeviceToDevice, cs) != cudaSuccess)
+                e = PB_ERR_CUDA;
+        ce = cudaStreamEndCapture(cs, &g);
+        cudaStreamDestroy(cs);
+        if (e != PB_OK) {
+            if (ce == cudaSuccess) cudaGraphDestroy(g);
+            return e;
+        }
+        if (ce != cudaSuccess) { set_cuda_error(ce); return PB_ERR_CUDA; }
+        ce = cudaGraphInstantiate(&lv->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (ce != cudaSuccess) { lv->graph = nullptr; set_cuda_error(ce); return PB_ERR_CUDA; }
+        lv->graph_key = key;
+    }
+    PB_CUDA(cudaGraphLaunch(lv->graph, st));
+    return PB_OK;
+}
+
+// Picks the tile shape (columns along x, planes per thread) for each patch-size class (valid x
+// extent) by timing the stencil over that class's patches alone; the level keeps the choice.
+int pb_level_autotune_f64(pb_level* lv, const pb_stencil* s, const double* u_slab, double* out_slab, double scale,
+                          void* stream)
+{
+    if (!lv || !s || !u_slab || !out_slab) return PB_ERR_ARG;
+    if (lv->ncomp != 1) return PB_ERR_UNSUPPORTED;
+    Coefs<double> cf;
+    int shape, e;
+    if ((e = level_coefs(lv, s, scale, cf, shape)) != PB_OK) return e;
+    cudaStream_t st = (cudaStream_t)stream;
+    std::vector<int> classes;
+    for (const Box3& b : lv->patches) classes.push_back((int)bsize(b, 0));
+    std::sort(classes.begin(), classes.end());
+    classes.erase(std::unique(classes.begin(), classes.end()), classes.end());
+    static const int cand_tx[] = {8, 16, 32, 64};
+    static const int cand_zd[] = {4, 8, 16, 32};
+    cudaEvent_t e0, e1;
+    PB_CUDA(cudaEventCreate(&e0));
+    PB_CUDA(cudaEventCreate(&e1));
+    for (int nx : classes) {
+        float best = 1e30f;
+        std::pair<int, int> pick = tile_shape(lv, nx);
+        for (int tx : cand_tx) {
+            if (tx > 2 * nx && tx != cand_tx[0]) continue;   // mostly idle columns
+            for (int zd : cand_zd) {
+                lv->tune[nx] = {tx, zd};
+                build_tiles(lv, nx);
+                if ((e = upload_tiles(lv)) != PB_OK) break;
+                for (int w = 0; w < 2; w++) launch_level_star(lv, shape, u_slab, out_slab, cf, 0.0, 0, st);
+                cudaEventRecord(e0, st);
+                for (int r = 0; r < 5; r++) launch_level_star(lv, shape, u_slab, out_slab, cf, 0.0, 0, st);
+                cudaEventRecord(e1, st);
+                cudaEventSynchronize(e1);
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (ms < best) {
+                    best = ms;
+                    pick = {tx, zd};
+                }
+            }
+            if (e != PB_OK) break;
+        }
+        lv->tune[nx] = pick;
+        if (e != PB_OK) break;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    build_tiles(lv);
+    const int e2 = upload_tiles(lv);
+    drop_graph(lv);
+    return e != PB_OK ? e : e2;
+}
+
+// The chosen tile shape of each patch-size class: up to cap entries of (x extent, tx, zd).
+int pb_level_tiles(const pb_level* lv, int* triples, int cap, int* n)
+{
+    if (!lv || !n || (cap > 0 && !triples)) return PB_ERR_ARG;
+    std::vector<int> classes;
+    for (const Box3& b : lv->patches) classes.push_back((int)bsize(b, 0));
+    std::sort(classes.begin(), classes.end());
+    classes.erase(std::unique(classes.begin(), classes.end()), classes.end());
+    int k = 0;
+    for (int nx : classes) {
+        if (k < cap) {
+            const std::pair<int, int> sh = tile_shape(lv, nx);
+            triples[3 * k] = nx;
+            triples[3 * k + 1] = sh.first;
+            triples[3 * k + 2] = sh.second;
+        }
+        k++;
+    }
+    *n = std::min(k, cap);
     return PB_OK;
 }
 

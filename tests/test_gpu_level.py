@@ -88,3 +88,69 @@ def test_level13_steps_golden(golden, pb):
         shp = tuple(p.size(d) + 2 * gh for d in (2, 1, 0))
         parts.append(host[off:off + int(np.prod(shp))].reshape(shp)[gh:-gh, gh:-gh, gh:-gh].reshape(-1))
     assert digest(np.concatenate(parts)) == g["sha256"]
+
+
+def _level13(golden, pb, widths, seed):
+    import torch
+    boxes, L = W.amr_patches(widths)
+    gh = 2
+    lv = pb.Level([pb.Box(*b) for b in boxes], gh, pb.Box((0, 0, 0), [v - 1 for v in L]), (1, 1, 1))
+    c, o, m = table(golden[1], "laplacian13")
+    u = W.uniform_box((L[2], L[1], L[0]), seed)
+    a = torch.from_numpy(_slab_from_valid(lv, u, 0.0)).cuda()
+    return lv, pb.Stencil(c, o), (c, o), u, a, L
+
+
+def _valid(lv, slab):
+    gh = lv.ghost[0]
+    parts = []
+    for p, off in zip(lv.patches, lv.offsets):
+        shp = tuple(p.size(d) + 2 * gh for d in (2, 1, 0))
+        parts.append(slab[off:off + int(np.prod(shp))].reshape(shp)[gh:-gh, gh:-gh, gh:-gh].reshape(-1))
+    return np.concatenate(parts)
+
+
+@pytest.mark.parametrize("tune", [False, True])
+def test_level13_graph_steps_golden(golden, pb, tune):
+    """The captured multi-step graph (with default or autotuned tiles) gives the golden digest."""
+    import torch
+    g = golden[0]["level13"]
+    lv, S, _, _, a, _ = _level13(golden, pb, g["widths"], g["seed"])
+    b = torch.zeros_like(a)
+    if tune:
+        lv.autotune(S, a, b, scale=1.0 / (g["h"] * g["h"]))
+        assert all(tx in (8, 16, 32, 64) and zd in (4, 8, 16, 32) for _, tx, zd in lv.tiles())
+    lv.steps(S, pb.EPI_EULER, a, b, g["steps"], scale=1.0 / (g["h"] * g["h"]), a=g["dt"])
+    torch.cuda.synchronize()
+    assert digest(_valid(lv, a.cpu().numpy())) == g["sha256"]
+    lv.steps(S, pb.EPI_EULER, a, b, 2, scale=1.0 / (g["h"] * g["h"]), a=g["dt"])   # a new graph (step count)
+    lv.steps(S, pb.EPI_EULER, a, b, 2, scale=1.0 / (g["h"] * g["h"]), a=g["dt"])   # replayed
+    torch.cuda.synchronize()
+    pb.device_check()
+
+
+def test_amr_level_full_size_against_port(golden, pb, port):
+    """The 512-patch uneven level (widths from seed 2), autotuned tiles, 4 graph steps: bitwise the
+    C port's periodic stepping on the whole domain."""
+    import torch
+    widths = W.amr_widths(seed=2)
+    lv, S, (c, o), u, a, L = _level13(golden, pb, widths, 7)
+    assert len(lv.patches) == 512
+    h = 1.0 / L[0]
+    b = torch.zeros_like(a)
+    lv.autotune(S, a, b, scale=1.0 / (h * h))
+    lv.steps(S, pb.EPI_EULER, a, b, 4, scale=1.0 / (h * h), a=0.1 * h * h)
+    torch.cuda.synchronize()
+    got = a.cpu().numpy()
+    gh = 2
+    G = np.zeros((L[2] + 2 * gh, L[1] + 2 * gh, L[0] + 2 * gh))
+    G[gh:-gh, gh:-gh, gh:-gh] = u
+    G = G.reshape(-1).copy()
+    port.periodic_steps(L, gh, c, o.reshape(-1), h, 0.1 * h * h, 4, G)
+    ref = G.reshape(L[2] + 2 * gh, L[1] + 2 * gh, L[0] + 2 * gh)[gh:-gh, gh:-gh, gh:-gh]
+    out = np.zeros_like(u)
+    for p, off in zip(lv.patches, lv.offsets):
+        shp = tuple(p.size(d) + 2 * gh for d in (2, 1, 0))
+        blk = got[off:off + int(np.prod(shp))].reshape(shp)[gh:-gh, gh:-gh, gh:-gh]
+        out[p.lo[2]:p.hi[2] + 1, p.lo[1]:p.hi[1] + 1, p.lo[0]:p.hi[0] + 1] = blk
+    assert np.array_equal(out, ref)

@@ -228,6 +228,21 @@ int pb_mg_launches_per_cycle(const pb_mg_params* p);
  * 0 turns this off. Default 16. Applies to solvers created and cycles captured afterwards. */
 int pb_mg_coarse_edge(int edge);
 
+/* ---- FAS multigrid with the 4th-order flux-form Laplacian (reference: LevelMultigridSolver<
+ * BoxOp_Laplace>, include/utils/implem/Proto_LevelMultigridSolverImplem.H:85-433, operator
+ * examples/_common/BoxOp_Laplace.H:22-27 through BoxOp::operator(), Proto_BoxOpImplem.H:125-172) ---
+ * Periodic cell-centred n^3 grid, num_levels grids (n >> (num_levels-1) the coarsest), h = 1/n.
+ * Drives op(phi) + force to zero, op = -sum_d DIV_d(DiffCellToFace_d(phi)/h)/h; V(6,6) with
+ * lambda = 0.5/(6/h^2) Jacobi, 10 bottom sweeps, FAS coarse force and correction; stops when
+ * res < tol*res0 (max norm). Residual history and solution are bitwise the reference's. */
+typedef struct pb_fas pb_fas;
+int pb_fas_create(int n, int num_levels, pb_fas** out);
+int pb_fas_destroy(pb_fas* m);
+/* force, phi: device n^3 (x fastest); phi is the initial guess and receives the solution; hist
+ * (host, max_iter+1, may be NULL) the residual norms; *iters the cycles run. Blocks. */
+int pb_fas_solve(pb_fas* m, const double* force, double* phi, int max_iter, double tol, int* iters,
+                 double* hist, void* stream);
+
 /* ---- Serving engine (no counterpart in the reference, which solves one grid at a time) ----------
  * Periodic Poisson/Helmholtz solves of different edges, solved together: each admitted solve keeps
  * its hierarchy on the device; one pb_serve_step runs one mixed-precision V-cycle (FP32 cycle,

@@ -35,7 +35,7 @@ class Port:
         self.lib = L = ctypes.CDLL(path)
         L.or_reduce.restype = _c_dbl
         L.or_reduce.argtypes = [_c_int, _vp, ctypes.c_long]
-        for name in ("or_stencil_apply", "or_interp_constant", "or_exchange", "or_mg_cs",
+        for name in ("or_stencil_apply", "or_interp_constant", "or_exchange", "or_mg_cs", "or_mg_fas",
                      "or_plain_apply", "or_periodic_steps", "or_num_threads"):
             getattr(L, name).restype = _c_int
 
@@ -88,6 +88,14 @@ class Port:
                               _p(rhs), _p(phi), _p(hist), _c_int(bottom))
         if n < 0:
             raise RuntimeError("or_mg_cs: singular coarsest operator")
+        return n, hist[: n + 1]
+
+    def mg_fas(self, N, num_levels, max_iter, tol, force, phi):
+        """FAS V(6,6) with the 4th-order flux-form Laplacian (LevelMultigridSolver<BoxOp_Laplace>)."""
+        hist = np.zeros(max_iter + 1)
+        force = _f64(force)
+        n = self.lib.or_mg_fas(_c_int(N), _c_int(num_levels), _c_int(max_iter), _c_dbl(tol), _p(force), _p(phi),
+                               _p(hist))
         return n, hist[: n + 1]
 
     def plain_apply(self, n, u, out, h, a, b):

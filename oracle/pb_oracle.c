@@ -560,6 +560,188 @@ int or_mg_cs(int N, int levels, int nu1, int nu2, int nuBottom, double omega, do
 }
 
 /* ---------------------------------------------------------------------------------------------
+ * FAS multigrid with the 4th-order flux-form Laplacian: LevelMultigridSolver<BoxOp_Laplace>
+ * (include/utils/implem/Proto_LevelMultigridSolverImplem.H:85-433; BoxOp::operator(),
+ * include/base/implem/Proto_BoxOpImplem.H:125-172; BoxOp_Laplace::flux,
+ * examples/_common/BoxOp_Laplace.H:22-27) on one periodic box per level, ghost width 2.
+ *   flux_d(q)  = sum_k g_k u[q + k e_d], k = -2,-1,0,1 (DiffCellToFace(d, Lo, 4) * 1/dx, |=)
+ *   div(p)     = 0; per d: div += c+ * flux_d(p + e_d); div += c0 * flux_d(p)   (DIV * 1/dx, +=)
+ *   op(p)      = (0 + div) * (-1)                                             (fluxScale = -1)
+ *   relax      : res = op(u) + f;  u += (-lambda) * res, lambda = 0.5 / (6/dx^2)
+ *   coarse force: AvgDown(op(u) + f) - op_c(AvgDown(u));  correction: u += 1.0 * (-(c0 - c))
+ * V(6,6), 10 bottom sweeps. Per-patch evaluation in the reference equals this per-cell evaluation
+ * (each cell's operations depend only on values, and ghosts hold the periodic images).
+ * ------------------------------------------------------------------------------------------- */
+static void fas_op(const double* u, int n, double dx, const double* dc, double* out)
+{
+    /* dc: 4 face-gradient coefficients then the 2 divergence coefficients (term order +e, 0) */
+    long S = n + 4;
+    double g[4], cp = dc[4], c0 = dc[5];
+    for (int k = 0; k < 4; k++) g[k] = dc[k];
+    (void)dx;
+    #pragma omp parallel for collapse(2) schedule(static)
+    for (int z = 0; z < n; z++) for (int y = 0; y < n; y++) for (int x = 0; x < n; x++) {
+        long i = IDX(x+2, y+2, z+2, S);
+        double div = 0.0;
+        for (int d = 0; d < 3; d++) {
+            long e = d == 0 ? 1 : (d == 1 ? S : S*S);
+            double fp = 0.0, fm = 0.0;
+            for (int k = 0; k < 4; k++) fp = fp + g[k] * u[i + e + (k - 2) * e];
+            for (int k = 0; k < 4; k++) fm = fm + g[k] * u[i + (k - 2) * e];
+            div = div + cp * fp;
+            div = div + c0 * fm;
+        }
+        out[IDX(x, y, z, n)] = (0.0 + div) * -1.0;
+    }
+}
+
+/* the operator's coefficients at spacing dx: DiffCellToFace(.,Lo,4) = {1,-15,15,-1} * (1/12),
+ * folded by 1/dx; divergence 1.0*Shift(+e) - 1.0*Shift(0), folded by 1/dx */
+static void fas_coefs(double dx, double* dc)
+{
+    const double base[4] = {1.0, -15.0, 15.0, -1.0};
+    double s = 1.0 / dx;
+    for (int k = 0; k < 4; k++) {
+        double c = base[k] * (1.0 / 12.0);
+        dc[k] = (s != 1.0) ? c * s : c;
+    }
+    dc[4] = (s != 1.0) ? 1.0 * s : 1.0;
+    dc[5] = (s != 1.0) ? -1.0 * s : -1.0;
+}
+
+typedef struct {
+    int N, levels;      /* finest edge; number of levels (finest index levels-1) */
+    double** u;         /* per level (n+4)^3 */
+    double** f;         /* per level n^3 */
+    double** c0;        /* per level n^3 (copy of the averaged-down state) */
+    double** t;         /* per level n^3 scratch */
+    double** r;         /* per level n^3 scratch */
+} or_fas;
+
+static int fas_n(const or_fas* m, int l) { return m->N >> (m->levels - 1 - l); }
+static double fas_dx(const or_fas* m, int l) { return (double)(1 << (m->levels - 1 - l)) / (double)m->N; }
+
+static void fas_relax(or_fas* m, int l, int sweeps)
+{
+    int n = fas_n(m, l); long S = n + 4;
+    double dx = fas_dx(m, l), dc[6];
+    fas_coefs(dx, dc);
+    double lambda = 0.5 / ((2.0 * 3) / pow(dx, 2));
+    for (int s = 0; s < sweeps; s++) {
+        fill_periodic(m->u[l], n, 2);
+        fas_op(m->u[l], n, dx, dc, m->t[l]);
+        #pragma omp parallel for collapse(2) schedule(static)
+        for (int z = 0; z < n; z++) for (int y = 0; y < n; y++) for (int x = 0; x < n; x++) {
+            long o = IDX(x, y, z, n), i = IDX(x+2, y+2, z+2, S);
+            double res = m->t[l][o] + m->f[l][o];
+            m->u[l][i] = m->u[l][i] + (-lambda) * res;
+        }
+    }
+}
+
+static void fas_vcycle(or_fas* m, int l)
+{
+    if (l == 0) { fas_relax(m, l, 10); return; }
+    int n = fas_n(m, l), nc = n / 2; long S = n + 4, Sc = nc + 4;
+    double dx = fas_dx(m, l), dcx = fas_dx(m, l - 1), dc[6], dcc[6];
+    fas_coefs(dx, dc);
+    fas_coefs(dcx, dcc);
+    fas_relax(m, l, 6);
+    /* averageDown(crseState, state): AvgDown(2), children in Box([0,1]^3) order */
+    double* uc = m->u[l-1];
+    #pragma omp parallel for collapse(2) schedule(static)
+    for (int z = 0; z < nc; z++) for (int y = 0; y < nc; y++) for (int x = 0; x < nc; x++) {
+        double acc = 0.0;
+        for (int kz = 0; kz < 2; kz++) for (int ky = 0; ky < 2; ky++) for (int kx = 0; kx < 2; kx++)
+            acc = acc + 0.125 * m->u[l][IDX(2*x+kx+2, 2*y+ky+2, 2*z+kz+2, S)];
+        uc[IDX(x+2, y+2, z+2, Sc)] = acc;
+        m->c0[l-1][IDX(x, y, z, nc)] = acc;
+    }
+    /* coarseForce */
+    fill_periodic(m->u[l], n, 2);
+    fill_periodic(uc, nc, 2);
+    fas_op(m->u[l], n, dx, dc, m->t[l]);
+    #pragma omp parallel for collapse(2) schedule(static)
+    for (int z = 0; z < nc; z++) for (int y = 0; y < nc; y++) for (int x = 0; x < nc; x++) {
+        double acc = 0.0;
+        for (int kz = 0; kz < 2; kz++) for (int ky = 0; ky < 2; ky++) for (int kx = 0; kx < 2; kx++) {
+            long o = IDX(2*x+kx, 2*y+ky, 2*z+kz, n);
+            double res = m->t[l][o] + m->f[l][o];
+            acc = acc + 0.125 * res;
+        }
+        m->f[l-1][IDX(x, y, z, nc)] = acc;
+    }
+    fas_op(uc, nc, dcx, dcc, m->t[l-1]);
+    for (long o = 0; o < (long)nc*nc*nc; o++) m->f[l-1][o] = m->f[l-1][o] - m->t[l-1][o];
+    fas_vcycle(m, l - 1);
+    /* fineCorrect: c0 = -(c0 - crse); fine += 1.0 * c0(p/2) */
+    #pragma omp parallel for collapse(2) schedule(static)
+    for (int z = 0; z < nc; z++) for (int y = 0; y < nc; y++) for (int x = 0; x < nc; x++) {
+        long o = IDX(x, y, z, nc);
+        m->c0[l-1][o] = (m->c0[l-1][o] - uc[IDX(x+2, y+2, z+2, Sc)]) * -1.0;
+    }
+    #pragma omp parallel for collapse(2) schedule(static)
+    for (int z = 0; z < n; z++) for (int y = 0; y < n; y++) for (int x = 0; x < n; x++) {
+        long i = IDX(x+2, y+2, z+2, S);
+        m->u[l][i] = m->u[l][i] + 1.0 * m->c0[l-1][IDX(x/2, y/2, z/2, nc)];
+    }
+    fas_relax(m, l, 6);
+}
+
+static double fas_resnorm(or_fas* m, int l)
+{
+    int n = fas_n(m, l);
+    double dx = fas_dx(m, l), dc[6];
+    fas_coefs(dx, dc);
+    fill_periodic(m->u[l], n, 2);
+    fas_op(m->u[l], n, dx, dc, m->t[l]);
+    double best = 0.0;
+    for (long o = 0; o < (long)n*n*n; o++) best = upd_abs(best, m->t[l][o] + m->f[l][o]);
+    return best;
+}
+
+/* force, phi: N^3 (x fastest); numLevels as LevelMultigridSolver's; hist: maxIter+1 entries.
+ * Returns the number of V-cycles run. */
+int or_mg_fas(int N, int numLevels, int maxIter, double tol, const double* force, double* phi, double* hist)
+{
+    or_fas m;
+    m.N = N; m.levels = numLevels;
+    m.u = (double**)calloc(numLevels, sizeof(double*));
+    m.f = (double**)calloc(numLevels, sizeof(double*));
+    m.c0 = (double**)calloc(numLevels, sizeof(double*));
+    m.t = (double**)calloc(numLevels, sizeof(double*));
+    m.r = (double**)calloc(numLevels, sizeof(double*));
+    for (int l = 0; l < numLevels; l++) {
+        long n = fas_n(&m, l);
+        m.u[l] = (double*)calloc((size_t)(n+4)*(n+4)*(n+4), sizeof(double));
+        m.f[l] = (double*)calloc((size_t)n*n*n, sizeof(double));
+        m.c0[l] = (double*)calloc((size_t)n*n*n, sizeof(double));
+        m.t[l] = (double*)calloc((size_t)n*n*n, sizeof(double));
+        m.r[l] = (double*)calloc((size_t)n*n*n, sizeof(double));
+    }
+    int top = numLevels - 1;
+    long S = N + 4;
+    for (int z = 0; z < N; z++) for (int y = 0; y < N; y++) for (int x = 0; x < N; x++) {
+        m.u[top][IDX(x+2, y+2, z+2, S)] = phi[IDX(x, y, z, N)];
+        m.f[top][IDX(x, y, z, N)] = force[IDX(x, y, z, N)];
+    }
+    double r0 = fas_resnorm(&m, top);
+    hist[0] = r0;
+    int it = 0;
+    while (it < maxIter) {
+        fas_vcycle(&m, top);
+        double r = fas_resnorm(&m, top);
+        hist[++it] = r;
+        if (r < tol * r0) break;
+    }
+    for (int z = 0; z < N; z++) for (int y = 0; y < N; y++) for (int x = 0; x < N; x++)
+        phi[IDX(x, y, z, N)] = m.u[top][IDX(x+2, y+2, z+2, S)];
+    for (int l = 0; l < numLevels; l++) { free(m.u[l]); free(m.f[l]); free(m.c0[l]); free(m.t[l]); free(m.r[l]); }
+    free(m.u); free(m.f); free(m.c0); free(m.t); free(m.r);
+    return it;
+}
+
+/* ---------------------------------------------------------------------------------------------
  * Plain method, small: out = a*L(u, 1/h^2) + b*u on [0,n-1]^3 with u on [-1,n]^3.
  * ------------------------------------------------------------------------------------------- */
 int or_plain_apply(int n, const double* u, double* out, double h, double a, double b)

@@ -16,7 +16,7 @@ __all__ = ["ProtoError", "lib", "Box", "Stencil", "Level", "Multigrid", "MGParam
            "interp_constant", "device_check", "OP_ADD", "OP_SUB", "OP_MUL", "OP_DIV", "OP_ASSIGN",
            "RED_MAX", "RED_MIN", "RED_ABS", "RED_SUM", "RED_SUMABS", "RED_SUMSQ", "EPI_AXPBY", "EPI_EULER",
            "MG_POISSON", "MG_HELMHOLTZ", "MG_FP64", "MG_MIXED", "MG_BOTTOM_RELAX", "MG_BOTTOM_DIRECT",
-           "Serve", "SERVE_WAITING", "SERVE_ACTIVE", "SERVE_DONE", "SERVE_FAILED",
+           "FAS", "Serve", "SERVE_WAITING", "SERVE_ACTIVE", "SERVE_DONE", "SERVE_FAILED",
            "header_functions"]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -345,6 +345,29 @@ class Multigrid:
     def __del__(self):
         if getattr(self, "_h", None) and _LIB is not None:
             _LIB.pb_mg_destroy(self._h)
+            self._h = None
+
+
+class FAS:
+    """FAS V(6,6) multigrid with the 4th-order flux-form Laplacian (pb_fas_*): the reference's
+    LevelMultigridSolver<BoxOp_Laplace>, one periodic box per level."""
+
+    def __init__(self, n, num_levels):
+        self.n = n
+        h = _vp()
+        _check(lib().pb_fas_create(_c_int(n), _c_int(num_levels), ctypes.byref(h)), "pb_fas_create")
+        self._h = h
+
+    def solve(self, force, phi, max_iter=20, tol=1e-10, stream=None):
+        it = _c_int()
+        hist = (ctypes.c_double * (max_iter + 1))()
+        _check(lib().pb_fas_solve(self._h, _ptr(force), _ptr(phi), _c_int(max_iter), _c_dbl(tol), ctypes.byref(it),
+                                  hist, _stream(stream)), "pb_fas_solve")
+        return it.value, [hist[k] for k in range(it.value + 1)]
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _LIB is not None:
+            _LIB.pb_fas_destroy(self._h)
             self._h = None
 
 

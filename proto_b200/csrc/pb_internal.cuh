@@ -94,6 +94,7 @@ __device__ inline void flag_error(int code) { atomicCAS(&g_dev_error, 0, code); 
 int read_error_stencil();
 int read_error_mg();
 int read_error_serve();
+int read_error_fas();
 
 // ---------------------------------------------------------------------------------------------
 // Exact arithmetic: one IEEE rounding per operation, never contracted into FMA

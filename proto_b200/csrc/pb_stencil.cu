@@ -332,9 +332,9 @@ int pb_device_check(void* stream)
 {
     cudaStream_t st = (cudaStream_t)stream;
     PB_CUDA(cudaStreamSynchronize(st));
-    int a = read_error_stencil(), b = read_error_mg(), c = read_error_serve();
-    if (a < 0 || b < 0 || c < 0) return PB_ERR_CUDA;
-    return (a || b || c) ? PB_ERR_DEVICE : PB_OK;
+    int a = read_error_stencil(), b = read_error_mg(), c = read_error_serve(), d = read_error_fas();
+    if (a < 0 || b < 0 || c < 0 || d < 0) return PB_ERR_CUDA;
+    return (a || b || c || d) ? PB_ERR_DEVICE : PB_OK;
 }
 
 int pb_stencil_create(const double* coefs, const int* offsets, int nterms, const int src_ratio[3],

@@ -159,3 +159,32 @@ def test_coarse_levels_as_one_kernel_bitwise(pb, port, edge, lev):
     n2, h2 = port.mg_cs(N, lev, 4, 4, 10, 2.0 / 3.0, 1.0, None, 8, 1e-10,
                         W.poisson_rho(N, seed=1).reshape(-1).copy(), p2)
     assert it2 == n2 and hist2 == list(h2) and np.array_equal(phi2, p2)
+
+
+def test_fas_history_bitwise(golden, pb):
+    """LevelMultigridSolver<BoxOp_Laplace> (FAS, 4th-order flux form): the reference's own
+    residual history and solution, bit for bit."""
+    import torch
+    cfg = golden[0]["mg"]["fas_32"]
+    N = cfg["N"]
+    rho = W.poisson_rho(N, seed=1).reshape(-1)
+    mg = pb.FAS(N, cfg["numLevels"])
+    phi = torch.zeros(N ** 3, dtype=torch.float64, device="cuda")
+    it, hist = mg.solve(torch.from_numpy(-rho).cuda(), phi, max_iter=cfg["maxIter"], tol=cfg["tol"])
+    pb.device_check()
+    assert it == cfg["iters"]
+    assert hist == cfg["hist"]
+    assert digest(phi.cpu().numpy()) == cfg["phi_sha256"]
+
+
+def test_fas_against_port_64(pb, port):
+    import torch
+    N, levels = 64, 5
+    rho = W.poisson_rho(N, seed=1).reshape(-1).copy()
+    mg = pb.FAS(N, levels)
+    phi = torch.zeros(N ** 3, dtype=torch.float64, device="cuda")
+    it, hist = mg.solve(torch.from_numpy(-rho).cuda(), phi, max_iter=6, tol=1e-10)
+    p2 = np.zeros(N ** 3)
+    n2, h2 = port.mg_fas(N, levels, 6, 1e-10, -rho, p2)
+    assert it == n2 and hist == list(h2)
+    assert np.array_equal(phi.cpu().numpy(), p2)

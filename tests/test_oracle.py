@@ -146,3 +146,16 @@ def test_port_matches_reference_live(ref, port):
     ib = port.infer_box(o.reshape(-1), m, sb, db)
     port.stencil_apply(c, o.reshape(-1), m, src, sb, d2, db, ib, False, 0.7)
     assert np.array_equal(d1, d2)
+
+
+def test_port_fas_bitwise(golden, port):
+    """The C restatement of LevelMultigridSolver<BoxOp_Laplace> (FAS, 4th-order flux form) against
+    the reference's own history and solution."""
+    cfg = golden[0]["mg"]["fas_32"]
+    N = cfg["N"]
+    rho = W.poisson_rho(N, seed=1).reshape(-1).copy()
+    phi = np.zeros(N ** 3)
+    n, h = port.mg_fas(N, cfg["numLevels"], cfg["maxIter"], cfg["tol"], -rho, phi)
+    assert n == cfg["iters"]
+    assert list(h) == cfg["hist"]
+    assert digest(phi) == cfg["phi_sha256"]

@@ -9,6 +9,7 @@ restriction/prolongation pair stalls at depth (reference CPU path: 0.48, 0.72, 0
 
   value : solves/s with inputs resident in HBM (device-timed, max over ranks)
   e2e   : the same through the public API with host buffers: H2D of f, solve, D2H of u per step
+          (copies on a second stream, overlapping the neighbouring steps' solves)
   stencil: Stencil::apply 7-point FP64 on a 256^3 box (src 258^3), GB/s and fraction of HBM
   roofline: the dominant kernel, the finest-level Jacobi sweep (k_star_tma<Lap7, EpiRelax>)
   mixed : the same problem with FP32 V-cycles inside FP64 residual/correction/norm
@@ -169,7 +170,7 @@ LAP13_OFFS = [(1, 0, 0), (0, 0, 0), (-1, 0, 0), (2, 0, 0), (-2, 0, 0), (0, 1, 0)
 LAP13_COEFS = [4.0 / 3, -7.5, 4.0 / 3, -1.0 / 12, -1.0 / 12] + [4.0 / 3, 4.0 / 3, -1.0 / 12, -1.0 / 12] * 2
 
 
-def run_amr_level(pb, torch, steps=100, reps=5):
+def run_amr_level(pb, torch, steps=100, reps=5, cpu=True):
     """Uneven AMR level: 512 patches (per-axis widths from {16,24,32,48,64}, seed 2) tiling a
     periodic domain, 2 ghost cells, u ~ U[-1,1]; a step = ghost exchange + u += dt*L13(u) (4th-order
     13-point Laplacian, dt = 0.1 h^2) over every patch; 100 steps as one captured graph, tiles
@@ -205,7 +206,7 @@ def run_amr_level(pb, torch, steps=100, reps=5):
            "gpu_launches_per_step": 2}
     try:   # the reference's own per-patch stepping on one host core, one step
         from oracle.oracle import Ref
-        if Ref.available():
+        if cpu and Ref.available():
             import numpy as np
             data = np.zeros(lv.slab_elems)
             parts, off = [], 0
@@ -278,6 +279,8 @@ def main():
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--profile-kernels", action="store_true",
                     help="run one 256^3 FP64 sweep, one FP32 sweep and one Stencil::apply, then exit (for ncu)")
+    ap.add_argument("--profile-level", action="store_true",
+                    help="run the AMR-level setup, autotune and 2 graph steps, then exit (for ncu)")
     ap.add_argument("--serve-requests", type=int, default=2000)
     args = ap.parse_args()
 
@@ -293,6 +296,8 @@ def main():
     torch.cuda.set_device(local)
     if args.profile_kernels:
         return profile_kernels(pb, torch)
+    if args.profile_level:
+        return run_amr_level(pb, torch, steps=2, reps=1, cpu=False)
     dist = None
     if world > 1:
         import torch.distributed as dist
@@ -347,18 +352,41 @@ def main():
     t_max = max_over_ranks(t_dev)
     value = world * args.steps / t_max
 
-    # end to end: host buffers, H2D of f and D2H of u inside the timed region
+    # end to end: host buffers, H2D of f and D2H of u of every step inside the timed region. The
+    # copies run on a second stream, double-buffered: step k+1's f goes up and step k-1's u comes
+    # down while step k solves.
     rho_pin = torch.from_numpy(rho_host).pin_memory()
-    out_pin = torch.empty(N ** 3, dtype=torch.float64).pin_memory()
-    rho_dev = torch.empty_like(rho)
+    out_pin = [torch.empty(N ** 3, dtype=torch.float64).pin_memory() for _ in range(2)]
+    rdev = [torch.empty_like(rho) for _ in range(2)]
+    pdev = [torch.empty_like(phi) for _ in range(2)]
+    cs = torch.cuda.Stream()
+    ev_in = [torch.cuda.Event() for _ in range(2)]
+    ev_out = [torch.cuda.Event() for _ in range(2)]
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for _ in range(args.steps):
-        rho_dev.copy_(rho_pin, non_blocking=True)
-        phi.zero_()
-        mg.solve(rho_dev, phi)
-        out_pin.copy_(phi, non_blocking=True)
+    cs.wait_event(e0)
+    with torch.cuda.stream(cs):
+        rdev[0].copy_(rho_pin, non_blocking=True)
+        ev_in[0].record(cs)
+    for k in range(args.steps):
+        b = k % 2
+        if k + 1 < args.steps:
+            with torch.cuda.stream(cs):
+                rdev[1 - b].copy_(rho_pin, non_blocking=True)
+                ev_in[1 - b].record(cs)
+        stream.wait_event(ev_in[b])
+        if k >= 2:
+            stream.wait_event(ev_out[b])          # step k-2's result has left pdev[b]
+        pdev[b].zero_()
+        mg.solve(rdev[b], pdev[b])
+        done = torch.cuda.Event()
+        done.record(stream)
+        cs.wait_event(done)
+        with torch.cuda.stream(cs):
+            out_pin[b].copy_(pdev[b], non_blocking=True)
+            ev_out[b].record(cs)
+    stream.wait_stream(cs)
     e1.record(stream)
     barrier()
     t_e2e = max_over_ranks(e0.elapsed_time(e1) / 1000.0)

@@ -163,8 +163,10 @@ int pb_level_stencil_f64(const pb_level* lv, const pb_stencil* s, int epilogue, 
 /* 'steps' steps of exchange(u_slab), out = u + a*S(u) (PB_EPI_EULER) or S(u) (0), swap, over
  * every patch; the result ends in u_slab (tmp_slab is scratch of the same size). The launches are
  * captured into one CUDA graph on the first call and replayed while the arguments stay the same.
- * Each step is bitwise the pair pb_level_exchange_f64 + pb_level_stencil_f64. No counterpart in
- * the reference, whose callers loop over exchange and per-patch stencils on the host. */
+ * Each step's valid cells are bitwise the pair pb_level_exchange_f64 + pb_level_stencil_f64. On a
+ * periodic tensor-product tiling the stencil reads face neighbours' valid cells directly (no
+ * exchange pass); ghost cells of the result are then not refreshed (call pb_level_exchange_f64).
+ * No counterpart in the reference, whose callers loop over exchange and per-patch stencils. */
 int pb_level_steps_f64(pb_level* lv, const pb_stencil* s, int epilogue, double* u_slab, double* tmp_slab,
                        double scale, double a, int steps, void* stream);
 /* Times the batched stencil per patch-size class (valid x extent) over a few tile shapes (columns

@@ -52,6 +52,11 @@ struct PatchTile {
     int vn[3];                 // valid box extents
     int x0, y0, z0;            // tile origin in valid coordinates
     int tx, zd;                // columns along x (ty = 256 / tx) and planes per thread
+    // face neighbours along each axis (tensor-product periodic tilings; read directly instead of
+    // ghost cells): slab offset, valid extent and grown extent along that axis, low / high side
+    long long nb_off[3][2];
+    int nb_n[3][2];
+    int nb_S[3][2];
 };
 
 constexpr int kLevelThreads = 256;
@@ -92,6 +97,85 @@ __global__ void __launch_bounds__(kLevelThreads) k_level_star(const double* __re
     }
 }
 
+// The same step on a periodic tensor-product tiling without ghost cells: a tap that leaves the
+// patch along one axis (a star stencil moves along one axis at a time) reads the face neighbour's
+// valid cell, which is what the exchange would have copied there. Bitwise the exchange + stencil.
+// Each thread resolves, once, a column pointer and a plane stride per x/y tap (its own patch or a
+// face neighbour); z taps that leave the patch read the z neighbour's plane (uniform per CTA).
+template <class S>
+__global__ void __launch_bounds__(kLevelThreads) k_level_star_fused(const double* __restrict__ u, double* out,
+                                                                    const PatchTile* __restrict__ tiles,
+                                                                    Coefs<double> cf, double a, int euler)
+{
+    constexpr int R = S::R, W = 2 * R + 1;
+    const PatchTile t = tiles[blockIdx.x];
+    const int lx = threadIdx.x % t.tx, ly = threadIdx.x / t.tx;
+    const int x = t.x0 + lx, y = t.y0 + ly;
+    const int nx = t.vn[0], ny = t.vn[1], nz = t.vn[2];
+    if (x >= nx || y >= ny) return;
+    const int g0 = t.gh[0], g1 = t.gh[1], g2 = t.gh[2];
+    const long long Sx = t.gS[0], Sy = t.gS[1], Sxy = Sx * Sy;
+    // (x, y, z = 0) of this patch and of the z neighbours (same x/y extents)
+    const long long cxy = (x + g0) + Sx * (y + g1) + Sxy * g2;
+    const double* col = u + t.off + cxy;
+    const double* colzl = u + t.nb_off[2][0] + cxy + Sxy * t.nb_n[2][0];   // z' < 0 -> z' + nz_low
+    const double* colzh = u + t.nb_off[2][1] + cxy;                          // z' >= nz -> z' - nz
+    double* ocol = out + t.off + cxy;
+    // x/y taps: column pointer and plane stride, resolved once
+    const double* tp[S::NT];
+    long long ts[S::NT];
+#pragma unroll
+    for (int j = 0; j < S::NT; j++) {
+        const int ox = S::off(j, 0), oy = S::off(j, 1);
+        tp[j] = col + ox + Sx * oy;
+        ts[j] = Sxy;
+        if (ox != 0 && x + ox < 0) {
+            const long long Sq = t.nb_S[0][0];
+            tp[j] = u + t.nb_off[0][0] + (x + ox + t.nb_n[0][0] + g0) + Sq * ((y + g1) + Sy * g2);
+            ts[j] = Sq * Sy;
+        } else if (ox != 0 && x + ox >= nx) {
+            const long long Sq = t.nb_S[0][1];
+            tp[j] = u + t.nb_off[0][1] + (x + ox - nx + g0) + Sq * ((y + g1) + Sy * g2);
+            ts[j] = Sq * Sy;
+        } else if (oy != 0 && y + oy < 0) {
+            const long long Sq = t.nb_S[1][0];
+            tp[j] = u + t.nb_off[1][0] + (x + g0) + Sx * ((y + oy + t.nb_n[1][0] + g1) + Sq * g2);
+            ts[j] = Sx * Sq;
+        } else if (oy != 0 && y + oy >= ny) {
+            const long long Sq = t.nb_S[1][1];
+            tp[j] = u + t.nb_off[1][1] + (x + g0) + Sx * ((y + oy - ny + g1) + Sq * g2);
+            ts[j] = Sx * Sq;
+        }
+    }
+    auto zcol = [&](int zz) -> double {
+        if (zz >= nz) return __ldg(colzh + Sxy * (zz - nz));
+        return __ldg((zz < 0 ? colzl : col) + Sxy * zz);
+    };
+    const int z1 = min(t.z0 + t.zd, nz);
+#pragma unroll
+    for (int j = 0; j < S::NT; j++) tp[j] += ts[j] * t.z0;   // advanced one plane per step below
+    double* op = ocol + Sxy * t.z0;
+    double win[W];
+#pragma unroll
+    for (int k = 0; k < 2 * R; k++) win[k] = zcol(t.z0 - R + k);
+    for (int z = t.z0; z < z1; z++) {
+        win[2 * R] = zcol(z + R);
+        double acc = 0.0;
+#pragma unroll
+        for (int j = 0; j < S::NT; j++) {
+            const int ox = S::off(j, 0), oy = S::off(j, 1), oz = S::off(j, 2);
+            const double v = (oz != 0 || (ox == 0 && oy == 0)) ? win[R + oz] : __ldg(tp[j]);
+            acc = dadd(acc, dmul(cf.c[j], v));
+        }
+        *op = euler ? dadd(win[R], dmul(a, acc)) : acc;
+        op += Sxy;
+#pragma unroll
+        for (int j = 0; j < S::NT; j++) tp[j] += ts[j];
+#pragma unroll
+        for (int k = 0; k < 2 * R; k++) win[k] = win[k + 1];
+    }
+}
+
 } // namespace pb
 
 struct pb_level {
@@ -108,6 +192,9 @@ struct pb_level {
     pb::PatchTile* d_tiles = nullptr;
     int device = 0;
     std::map<int, std::pair<int, int>> tune;   // valid x extent -> (tx, zd)
+    // periodic tensor-product tiling: face neighbour of patch i along axis d, side s
+    bool tensor = false;
+    std::vector<int> nbr;                      // [i*6 + d*2 + s]
     // captured multi-step graph and what it was captured for
     cudaGraphExec_t graph = nullptr;
     std::vector<double> graph_key;
@@ -171,6 +258,56 @@ static std::pair<int, int> tile_shape(const pb_level* lv, int nx)
     return it != lv->tune.end() ? it->second : std::make_pair(16, 8);
 }
 
+// Recognises a periodic tensor-product tiling (every patch = X_i x Y_j x Z_k of per-axis interval
+// lists that tile the domain) and records each patch's face neighbours; other layouts keep the
+// exchange + ghost-cell path.
+static void detect_tensor(pb_level* lv)
+{
+    lv->tensor = false;
+    lv->nbr.clear();
+    for (int d = 0; d < 3; d++)
+        if (!lv->periodic[d]) return;
+    const int np = (int)lv->patches.size();
+    std::vector<std::pair<int, int>> iv[3];
+    for (int d = 0; d < 3; d++) {
+        for (const Box3& b : lv->patches) iv[d].push_back({b.lo[d], b.hi[d]});
+        std::sort(iv[d].begin(), iv[d].end());
+        iv[d].erase(std::unique(iv[d].begin(), iv[d].end()), iv[d].end());
+        int next = lv->domain.lo[d];
+        for (auto& r : iv[d]) {
+            if (r.first != next || r.second - r.first + 1 < lv->ghost[d]) return;   // gap, overlap or too thin
+            next = r.second + 1;
+        }
+        if (next != lv->domain.hi[d] + 1) return;
+    }
+    const long long P0 = (long long)iv[0].size(), P1 = (long long)iv[1].size(), P2 = (long long)iv[2].size();
+    if (P0 * P1 * P2 != np) return;
+    std::vector<int> at(np, -1);
+    std::vector<int> idx(3 * np);
+    for (int i = 0; i < np; i++) {
+        int c[3];
+        for (int d = 0; d < 3; d++) {
+            const Box3& b = lv->patches[i];
+            c[d] = (int)(std::lower_bound(iv[d].begin(), iv[d].end(), std::make_pair(b.lo[d], b.hi[d])) - iv[d].begin());
+            if (c[d] >= (int)iv[d].size() || iv[d][c[d]] != std::make_pair(b.lo[d], b.hi[d])) return;
+            idx[3 * i + d] = c[d];
+        }
+        const long long k = c[0] + P0 * (c[1] + P1 * c[2]);
+        if (at[k] >= 0) return;
+        at[k] = i;
+    }
+    const long long P[3] = {P0, P1, P2};
+    lv->nbr.assign(6 * np, -1);
+    for (int i = 0; i < np; i++)
+        for (int d = 0; d < 3; d++)
+            for (int sd = 0; sd < 2; sd++) {
+                long long c[3] = {idx[3 * i], idx[3 * i + 1], idx[3 * i + 2]};
+                c[d] = (c[d] + (sd ? 1 : P[d] - 1)) % P[d];
+                lv->nbr[6 * i + 2 * d + sd] = at[c[0] + P0 * (c[1] + P1 * c[2])];
+            }
+    lv->tensor = true;
+}
+
 static void build_tiles(pb_level* lv, int only_nx = -1)
 {
     lv->tiles.clear();
@@ -185,6 +322,14 @@ static void build_tiles(pb_level* lv, int only_nx = -1)
             t.vn[d] = (int)bsize(v, d);
         }
         if (only_nx >= 0 && t.vn[0] != only_nx) continue;
+        for (int d = 0; d < 3; d++)
+            for (int sd = 0; sd < 2; sd++) {
+                const int q = lv->tensor ? lv->nbr[6 * i + 2 * d + sd] : i;
+                const Box3& vq = lv->patches[q];
+                t.nb_off[d][sd] = lv->offsets[q];
+                t.nb_n[d][sd] = (int)bsize(vq, d);
+                t.nb_S[d][sd] = (int)bsize(vq, d) + 2 * lv->ghost[d];
+            }
         const std::pair<int, int> sh = tile_shape(lv, t.vn[0]);
         t.tx = sh.first;
         t.zd = sh.second;
@@ -238,13 +383,20 @@ static int level_coefs(const pb_level* lv, const pb_stencil* s, double scale, Co
     return PB_OK;
 }
 
+// fused: read face neighbours instead of ghost cells (tensor-product periodic tilings only)
 static int launch_level_star(const pb_level* lv, int shape, const double* u, double* out, const Coefs<double>& cf,
-                             double a, int euler, cudaStream_t st)
+                             double a, int euler, cudaStream_t st, bool fused = false)
 {
     const unsigned nb = (unsigned)lv->tiles.size();
     if (nb == 0) return PB_OK;
-    if (shape == 1) k_level_star<ShapeLap7><<<nb, kLevelThreads, 0, st>>>(u, out, lv->d_tiles, cf, a, euler);
-    else k_level_star<ShapeLap13><<<nb, kLevelThreads, 0, st>>>(u, out, lv->d_tiles, cf, a, euler);
+    if (fused && !lv->tensor) return PB_ERR_ARG;
+    if (fused) {
+        if (shape == 1) k_level_star_fused<ShapeLap7><<<nb, kLevelThreads, 0, st>>>(u, out, lv->d_tiles, cf, a, euler);
+        else k_level_star_fused<ShapeLap13><<<nb, kLevelThreads, 0, st>>>(u, out, lv->d_tiles, cf, a, euler);
+    } else {
+        if (shape == 1) k_level_star<ShapeLap7><<<nb, kLevelThreads, 0, st>>>(u, out, lv->d_tiles, cf, a, euler);
+        else k_level_star<ShapeLap13><<<nb, kLevelThreads, 0, st>>>(u, out, lv->d_tiles, cf, a, euler);
+    }
     PB_LAUNCH_CHECK();
     return PB_OK;
 }
@@ -277,6 +429,7 @@ int pb_level_create(const pb_box* patches, int npatch, const int ghost[3], pb_bo
     }
     lv->slab_elems = off;
     build_items(lv);
+    detect_tensor(lv);
     build_tiles(lv);
     cudaGetDevice(&lv->device);
     if (!lv->items.empty()) {
@@ -364,11 +517,11 @@ int pb_level_steps_f64(pb_level* lv, const pb_stencil* s, int epilogue, double* 
         double* a_ = u_slab;
         double* b_ = tmp_slab;
         for (int k = 0; k < steps && e == PB_OK; k++) {
-            if (!lv->items.empty()) {
+            if (!lv->tensor && !lv->items.empty()) {
                 k_exchange<<<(unsigned)lv->items.size(), 256, 0, cs>>>(a_, lv->d_items, lv->ncomp);
                 if (cudaGetLastError() != cudaSuccess) e = PB_ERR_CUDA;
             }
-            if (e == PB_OK) e = launch_level_star(lv, shape, a_, b_, cf, a, epilogue == PB_EPI_EULER, cs);
+            if (e == PB_OK) e = launch_level_star(lv, shape, a_, b_, cf, a, epilogue == PB_EPI_EULER, cs, lv->tensor);
             std::swap(a_, b_);
         }
         if (e == PB_OK && (steps & 1))
@@ -419,9 +572,9 @@ int pb_level_autotune_f64(pb_level* lv, const pb_stencil* s, const double* u_sla
                 lv->tune[nx] = {tx, zd};
                 build_tiles(lv, nx);
                 if ((e = upload_tiles(lv)) != PB_OK) break;
-                for (int w = 0; w < 2; w++) launch_level_star(lv, shape, u_slab, out_slab, cf, 0.0, 0, st);
+                for (int w = 0; w < 2; w++) launch_level_star(lv, shape, u_slab, out_slab, cf, 0.0, 0, st, lv->tensor);
                 cudaEventRecord(e0, st);
-                for (int r = 0; r < 5; r++) launch_level_star(lv, shape, u_slab, out_slab, cf, 0.0, 0, st);
+                for (int r = 0; r < 5; r++) launch_level_star(lv, shape, u_slab, out_slab, cf, 0.0, 0, st, lv->tensor);
                 cudaEventRecord(e1, st);
                 cudaEventSynchronize(e1);
                 float ms = 0.f;

@@ -154,3 +154,25 @@ def test_amr_level_full_size_against_port(golden, pb, port):
         blk = got[off:off + int(np.prod(shp))].reshape(shp)[gh:-gh, gh:-gh, gh:-gh]
         out[p.lo[2]:p.hi[2] + 1, p.lo[1]:p.hi[1] + 1, p.lo[0]:p.hi[0] + 1] = blk
     assert np.array_equal(out, ref)
+
+
+def test_steps_on_a_non_tensor_layout_use_the_exchange(golden, pb):
+    """A tiling that is not a tensor product keeps exchange + ghost cells; graph steps equal the
+    explicit loop bitwise."""
+    import torch
+    boxes = [((0, 0, 0), (15, 31, 31)), ((16, 0, 0), (31, 15, 31)), ((16, 16, 0), (31, 31, 31))]
+    lv = pb.Level([pb.Box(*b) for b in boxes], 2, pb.Box((0, 0, 0), (31, 31, 31)), (1, 1, 1))
+    c, o, m = table(golden[1], "laplacian13")
+    S = pb.Stencil(c, o)
+    u = W.uniform_box((32, 32, 32), 5)
+    a = torch.from_numpy(_slab_from_valid(lv, u, 0.0)).cuda()
+    b = torch.zeros_like(a)
+    a2, b2 = a.clone(), b.clone()
+    h = 1.0 / 32
+    lv.steps(S, pb.EPI_EULER, a, b, 3, scale=1.0 / (h * h), a=0.1 * h * h)
+    for _ in range(3):
+        lv.exchange(a2)
+        lv.stencil(S, pb.EPI_EULER, a2, b2, scale=1.0 / (h * h), a=0.1 * h * h)
+        a2, b2 = b2, a2
+    torch.cuda.synchronize()
+    assert np.array_equal(_valid(lv, a.cpu().numpy()), _valid(lv, a2.cpu().numpy()))

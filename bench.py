@@ -170,7 +170,7 @@ LAP13_OFFS = [(1, 0, 0), (0, 0, 0), (-1, 0, 0), (2, 0, 0), (-2, 0, 0), (0, 1, 0)
 LAP13_COEFS = [4.0 / 3, -7.5, 4.0 / 3, -1.0 / 12, -1.0 / 12] + [4.0 / 3, 4.0 / 3, -1.0 / 12, -1.0 / 12] * 2
 
 
-def run_amr_level(pb, torch, steps=100, reps=5, cpu=True):
+def run_amr_level(pb, torch, steps=100, reps=5, cpu=True, tune=True):
     """Uneven AMR level: 512 patches (per-axis widths from {16,24,32,48,64}, seed 2) tiling a
     periodic domain, 2 ghost cells, u ~ U[-1,1]; a step = ghost exchange + u += dt*L13(u) (4th-order
     13-point Laplacian, dt = 0.1 h^2) over every patch; 100 steps as one captured graph, tiles
@@ -185,7 +185,8 @@ def run_amr_level(pb, torch, steps=100, reps=5, cpu=True):
     b = torch.zeros_like(a)
     h = 1.0 / L[0]
     scale, dt = 1.0 / (h * h), 0.1 * h * h
-    lv.autotune(S, a, b, scale=scale)
+    if tune:
+        lv.autotune(S, a, b, scale=scale)
     lv.steps(S, pb.EPI_EULER, a, b, steps, scale=scale, a=dt)     # capture + warm
     torch.cuda.synchronize()
     st = torch.cuda.current_stream()
@@ -280,7 +281,7 @@ def main():
     ap.add_argument("--profile-kernels", action="store_true",
                     help="run one 256^3 FP64 sweep, one FP32 sweep and one Stencil::apply, then exit (for ncu)")
     ap.add_argument("--profile-level", action="store_true",
-                    help="run the AMR-level setup, autotune and 2 graph steps, then exit (for ncu)")
+                    help="run the AMR-level setup and 2 graph steps with default tiles, then exit (for ncu)")
     ap.add_argument("--serve-requests", type=int, default=2000)
     args = ap.parse_args()
 
@@ -297,7 +298,7 @@ def main():
     if args.profile_kernels:
         return profile_kernels(pb, torch)
     if args.profile_level:
-        return run_amr_level(pb, torch, steps=2, reps=1, cpu=False)
+        return run_amr_level(pb, torch, steps=2, reps=1, cpu=False, tune=False)
     dist = None
     if world > 1:
         import torch.distributed as dist

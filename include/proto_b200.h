@@ -276,12 +276,15 @@ int pb_serve_destroy(pb_serve* sv);
 /* Queues a request; rhs and out must stay valid until its ticket completes. PB_ERR_BUDGET if one
  * solve of this edge alone exceeds the budget. */
 int pb_serve_submit(pb_serve* sv, const pb_serve_request* q, long long* ticket);
-/* Admits what fits, runs one cycle for every in-flight solve, retires the finished ones (their
- * results are in their out buffers when this returns). active / waiting may be NULL. */
+/* Admits what fits, runs one cycle for every in-flight solve and retires the finished ones; a
+ * retired solve's result is copied to its out buffer in the background. *active counts solves in
+ * flight plus results still on their way (keep stepping while it is non-zero); active / waiting
+ * may be NULL. */
 int pb_serve_step(pb_serve* sv, int* active, int* waiting);
-/* Tickets completed since the last poll (up to cap). */
+/* Tickets completed since the last poll (up to cap): their results are in their out buffers. */
 int pb_serve_poll(pb_serve* sv, long long* tickets, int cap, int* n);
-/* state PB_SERVE_*, cycles run, last relative residual. */
+/* state PB_SERVE_* (DONE / FAILED from the poll that reports the ticket on), cycles run, last
+ * relative residual. */
 int pb_serve_status(const pb_serve* sv, long long ticket, int* state, int* cycles, double* rel_res);
 /* Host wall time spent so far per stage of pb_serve_step (seconds: admission, work-list build,
  * first residual pass of new solves, the cycle graph including its wait, retirement) and the number

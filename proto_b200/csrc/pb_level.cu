@@ -176,6 +176,110 @@ __global__ void __launch_bounds__(kLevelThreads) k_level_star_fused(const double
     }
 }
 
+// Shared-memory variant of the fused step: per z plane the CTA stages its (tx+2R) x (ty+2R) tile
+// of the plane (halo cells from the face neighbours; the corner cells, which a star stencil never
+// reads, are skipped), then takes the x/y taps from shared memory and the z taps from a per-column
+// register window. Bitwise the other two paths (same values, same term order).
+constexpr int kLevelSmemMax = (64 + 4) * (16 + 4);   // widest tile (tx = 64, ty = 4 at R = 2; 16x16 fits too)
+
+template <class S>
+__global__ void __launch_bounds__(kLevelThreads) k_level_star_tiled(const double* __restrict__ u, double* out,
+                                                                    const PatchTile* __restrict__ tiles,
+                                                                    Coefs<double> cf, double a, int euler)
+{
+    constexpr int R = S::R, W = 2 * R + 1;
+    __shared__ double plane[kLevelSmemMax];
+    const PatchTile t = tiles[blockIdx.x];
+    const int tx = t.tx, ty = kLevelThreads / t.tx;
+    const int BX = tx + 2 * R, BY = ty + 2 * R;
+    const int nx = t.vn[0], ny = t.vn[1], nz = t.vn[2];
+    const int g0 = t.gh[0], g1 = t.gh[1], g2 = t.gh[2];
+    const long long Sx = t.gS[0], Sy = t.gS[1], Sxy = Sx * Sy;
+    const int lx = threadIdx.x % tx, ly = threadIdx.x / tx;
+    const int x = t.x0 + lx, y = t.y0 + ly;
+    const bool act = x < nx && y < ny;
+    // this thread's staging assignments are fixed across planes: base pointer and plane stride each
+    constexpr int kMaxLoads = 3;   // (tx+2R)(ty+2R) <= 544 cells for every tile shape, 256 threads
+    const double* lp[kMaxLoads];
+    long long ls[kMaxLoads];
+    bool lv_[kMaxLoads];
+#pragma unroll
+    for (int k = 0; k < kMaxLoads; k++) {
+        const int i = threadIdx.x + k * kLevelThreads;
+        const int hx = i % BX, hy = i / BX;
+        const int xx = t.x0 - R + hx, yy = t.y0 - R + hy;
+        const bool xo = xx < 0 || xx >= nx, yo = yy < 0 || yy >= ny;
+        lv_[k] = i < BX * BY && !(xo && yo) && xx < nx + R && yy < ny + R;   // corners never read
+        lp[k] = u;
+        ls[k] = 0;
+        if (!lv_[k]) continue;
+        const double* p;
+        long long st = Sxy;
+        if (xx < 0) {
+            const long long Sq = t.nb_S[0][0];
+            p = u + t.nb_off[0][0] + (xx + t.nb_n[0][0] + g0) + Sq * ((yy + g1) + Sy * g2);
+            st = Sq * Sy;
+        } else if (xx >= nx) {
+            const long long Sq = t.nb_S[0][1];
+            p = u + t.nb_off[0][1] + (xx - nx + g0) + Sq * ((yy + g1) + Sy * g2);
+            st = Sq * Sy;
+        } else if (yy < 0) {
+            const long long Sq = t.nb_S[1][0];
+            p = u + t.nb_off[1][0] + (xx + g0) + Sx * ((yy + t.nb_n[1][0] + g1) + Sq * g2);
+            st = Sx * Sq;
+        } else if (yy >= ny) {
+            const long long Sq = t.nb_S[1][1];
+            p = u + t.nb_off[1][1] + (xx + g0) + Sx * ((yy - ny + g1) + Sq * g2);
+            st = Sx * Sq;
+        } else {
+            p = u + t.off + (xx + g0) + Sx * (yy + g1) + Sxy * g2;
+        }
+        lp[k] = p + st * t.z0;
+        ls[k] = st;
+    }
+    // own column (z taps) with its z neighbours
+    const long long cxy = (x + g0) + Sx * (y + g1) + Sxy * g2;
+    const double* col = u + t.off + cxy;
+    const double* colzl = u + t.nb_off[2][0] + cxy + Sxy * t.nb_n[2][0];
+    const double* colzh = u + t.nb_off[2][1] + cxy;
+    auto zcol = [&](int zz) -> double {
+        if (zz >= nz) return __ldg(colzh + Sxy * (zz - nz));
+        return __ldg((zz < 0 ? colzl : col) + Sxy * zz);
+    };
+    const int z1 = min(t.z0 + t.zd, nz);
+    double win[W];
+    if (act) {
+#pragma unroll
+        for (int k = 0; k < 2 * R; k++) win[k] = zcol(t.z0 - R + k);
+    }
+    double* op = out + t.off + cxy + Sxy * t.z0;
+    const int sc = (ly + R) * BX + (lx + R);
+    for (int z = t.z0; z < z1; z++) {
+#pragma unroll
+        for (int k = 0; k < kMaxLoads; k++)
+            if (lv_[k]) {
+                plane[threadIdx.x + k * kLevelThreads] = __ldg(lp[k]);
+                lp[k] += ls[k];
+            }
+        if (act) win[2 * R] = zcol(z + R);
+        __syncthreads();
+        if (act) {
+            double acc = 0.0;
+#pragma unroll
+            for (int j = 0; j < S::NT; j++) {
+                const int ox = S::off(j, 0), oy = S::off(j, 1), oz = S::off(j, 2);
+                const double v = (oz != 0 || (ox == 0 && oy == 0)) ? win[R + oz] : plane[sc + oy * BX + ox];
+                acc = dadd(acc, dmul(cf.c[j], v));
+            }
+            *op = euler ? dadd(win[R], dmul(a, acc)) : acc;
+#pragma unroll
+            for (int k = 0; k < 2 * R; k++) win[k] = win[k + 1];
+        }
+        op += Sxy;
+        __syncthreads();
+    }
+}
+
 } // namespace pb
 
 struct pb_level {
@@ -194,6 +298,7 @@ struct pb_level {
     std::map<int, std::pair<int, int>> tune;   // valid x extent -> (tx, zd)
     // periodic tensor-product tiling: face neighbour of patch i along axis d, side s
     bool tensor = false;
+    bool tiled = true;                         // fused steps use the shared-memory tile kernel
     std::vector<int> nbr;                      // [i*6 + d*2 + s]
     // captured multi-step graph and what it was captured for
     cudaGraphExec_t graph = nullptr;
@@ -390,7 +495,10 @@ static int launch_level_star(const pb_level* lv, int shape, const double* u, dou
     const unsigned nb = (unsigned)lv->tiles.size();
     if (nb == 0) return PB_OK;
     if (fused && !lv->tensor) return PB_ERR_ARG;
-    if (fused) {
+    if (fused && lv->tiled) {
+        if (shape == 1) k_level_star_tiled<ShapeLap7><<<nb, kLevelThreads, 0, st>>>(u, out, lv->d_tiles, cf, a, euler);
+        else k_level_star_tiled<ShapeLap13><<<nb, kLevelThreads, 0, st>>>(u, out, lv->d_tiles, cf, a, euler);
+    } else if (fused) {
         if (shape == 1) k_level_star_fused<ShapeLap7><<<nb, kLevelThreads, 0, st>>>(u, out, lv->d_tiles, cf, a, euler);
         else k_level_star_fused<ShapeLap13><<<nb, kLevelThreads, 0, st>>>(u, out, lv->d_tiles, cf, a, euler);
     } else {

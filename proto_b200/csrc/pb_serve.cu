@@ -69,6 +69,16 @@ struct pb_serve {
     std::vector<long long> slots;       // slot -> ticket (0: free)
     std::vector<long long> completed;   // tickets done since the last poll
     std::multimap<int, SvHier*> cache;  // idle hierarchies by edge
+    // retired solves whose result is still on its way to the host (copy stream)
+    struct Pending {
+        long long ticket;
+        SvHier* h;
+        cudaEvent_t done;
+        int state;                      // PB_SERVE_DONE / FAILED once the copy has landed
+    };
+    std::vector<Pending> pending;
+    std::vector<cudaEvent_t> free_events;
+    cudaStream_t cst = nullptr;         // copy stream for results
     size_t held = 0;                    // bytes of all hierarchies (busy and idle)
     // phase lists (device + host mirror)
     int max_phases = 0;
@@ -207,6 +217,9 @@ RelaxCoef<float> level_coef(const pb_serve_params& p, const pb_serve_request& q,
     return k;
 }
 
+// units of the column-walk phases: rows x 32-wide x chunks x kSvZ-deep z chunks
+int walk_units(int e) { return e * ((e + 31) / 32) * ((e + kSvZ - 1) / kSvZ); }
+
 double level_hsqinv(int n, int d)
 {
     const double h = (double)(1 << d) / (double)n;
@@ -321,7 +334,7 @@ static int build_lists(pb_serve* sv)
                 it.out = ph_[1 - c];
                 it.rhs = h.rhs[d];
                 it.c = lap7_coefs<float>(helm ? level_hsqinv(n, d) : p.omega / 6.0);
-                it.units = e * e;
+                it.units = walk_units(e);
                 if (ps.op == SV_RELAX) c = 1 - c;
                 break;
             case SV_RELAX_FIRST:
@@ -355,7 +368,7 @@ static int build_lists(pb_serve* sv)
                 it.out = h.rhs[0];
                 const double hs = level_hsqinv(n, 0);
                 it.c64 = lap7_coefs<double>(helm ? hs : -hs);
-                it.units = e * e;
+                it.units = walk_units(e);
                 c = 1;
                 break;
             }
@@ -390,7 +403,7 @@ static int build_lists(pb_serve* sv)
             it.out = h.rhs[0];
             const double hs = level_hsqinv(h.n, 0);
             it.c64 = lap7_coefs<double>(helm ? hs : -hs);
-            it.units = h.n * h.n;
+            it.units = walk_units(h.n);
             add_item(items, total, it);
         }
         std::copy(items.begin(), items.end(), sv->h_items.begin() + (size_t)ph * cap);
@@ -462,12 +475,12 @@ static int launch_phase(pb_serve* sv, int slot, int op, double* norms, cudaStrea
     const long long* u0 = sv->d_unit0 + (size_t)slot * sv->p.max_active;
     const SvPhaseHeader* hdr = sv->d_hdr + slot;
     switch (op) {
-    case SV_RELAX: k_sv_phase<SV_RELAX><<<sv->grid, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
+    case SV_RELAX: k_sv_walk<SV_RELAX, float><<<sv->grid, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
     case SV_RELAX_FIRST: k_sv_phase<SV_RELAX_FIRST><<<sv->grid, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
     case SV_RESTRICT: k_sv_phase<SV_RESTRICT><<<sv->grid, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
     case SV_PROLONG: k_sv_phase<SV_PROLONG><<<sv->grid, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
-    case SV_K1: k_sv_phase<SV_K1><<<sv->grid, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
-    case SV_UPDATE: k_sv_phase<SV_UPDATE><<<sv->grid, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
+    case SV_K1: k_sv_walk<SV_K1, double><<<sv->grid, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
+    case SV_UPDATE: k_sv_walk<SV_UPDATE, float><<<sv->grid, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
     default: return PB_ERR_ARG;
     }
     PB_LAUNCH_CHECK();
@@ -549,20 +562,59 @@ static int admit(pb_serve* sv)
     return PB_OK;
 }
 
-static void retire(pb_serve* sv, SvSolve& s, int state)
+// A finished solve leaves the cycle at once; its result goes to the host on the copy stream, and the
+// ticket is reported (and the hierarchy reused) when that copy has landed.
+static int retire(pb_serve* sv, SvSolve& s, int state)
 {
     SvHier* h = s.h;
     const int n = h->n;
     const size_t n3 = (size_t)n * n * n;
+    cudaEvent_t packed, done;
+    if (sv->free_events.size() < 2) {
+        for (int k = 0; k < 8; k++) {
+            cudaEvent_t e;
+            PB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            sv->free_events.push_back(e);
+        }
+    }
+    packed = sv->free_events.back();
+    sv->free_events.pop_back();
+    done = sv->free_events.back();
+    sv->free_events.pop_back();
     k_sv_pack_out<<<grid_for((long long)n3, 256), 256, 0, sv->st>>>(h->u64, h->f64, n, h->sxd);
-    cudaMemcpyAsync(s.req.out, h->f64, sizeof(double) * n3, cudaMemcpyDeviceToHost, sv->st);
-    s.state = state;
+    PB_LAUNCH_CHECK();
+    PB_CUDA(cudaEventRecord(packed, sv->st));
+    PB_CUDA(cudaStreamWaitEvent(sv->cst, packed, 0));
+    PB_CUDA(cudaMemcpyAsync(s.req.out, h->f64, sizeof(double) * n3, cudaMemcpyDeviceToHost, sv->cst));
+    PB_CUDA(cudaEventRecord(done, sv->cst));
+    sv->free_events.push_back(packed);   // reusable once recorded again later (stream order keeps it valid)
     sv->slots[s.slot] = 0;
     s.slot = -1;
     s.h = nullptr;
-    sv->cache.insert({n, h});
-    sv->completed.push_back(s.ticket);
+    sv->pending.push_back({s.ticket, h, done, state});
     sv->lists_dirty = true;
+    return PB_OK;
+}
+
+// Moves landed results to the completed list and their hierarchies to the cache; wait = block.
+static int drain(pb_serve* sv, bool wait)
+{
+    if (wait && !sv->pending.empty()) PB_CUDA(cudaStreamSynchronize(sv->cst));
+    for (size_t k = 0; k < sv->pending.size();) {
+        auto& q = sv->pending[k];
+        const cudaError_t r = cudaEventQuery(q.done);
+        if (r == cudaErrorNotReady) {
+            k++;
+            continue;
+        }
+        if (r != cudaSuccess) { set_cuda_error(r); return PB_ERR_CUDA; }
+        sv->cache.insert({q.h->n, q.h});
+        sv->solves[q.ticket].state = q.state;
+        sv->completed.push_back(q.ticket);
+        sv->free_events.push_back(q.done);
+        sv->pending.erase(sv->pending.begin() + k);
+    }
+    return PB_OK;
 }
 
 extern "C" {
@@ -581,6 +633,7 @@ int pb_serve_create(const pb_serve_params* p, pb_serve** out)
     sv->max_phases = phases_for(*p);
     const size_t cap = (size_t)p->max_active;
     bool ok = cudaStreamCreateWithFlags(&sv->st, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&sv->cst, cudaStreamNonBlocking) == cudaSuccess &&
               cudaMalloc(&sv->d_items, sizeof(SvItem) * cap * sv->max_phases) == cudaSuccess &&
               cudaMalloc(&sv->d_unit0, sizeof(long long) * cap * sv->max_phases) == cudaSuccess &&
               cudaMalloc(&sv->d_hdr, sizeof(SvPhaseHeader) * sv->max_phases) == cudaSuccess &&
@@ -620,6 +673,12 @@ int pb_serve_destroy(pb_serve* sv)
 {
     if (!sv) return PB_OK;
     if (sv->st) cudaStreamSynchronize(sv->st);
+    if (sv->cst) cudaStreamSynchronize(sv->cst);
+    for (auto& q : sv->pending) {
+        hier_free(q.h);
+        cudaEventDestroy(q.done);
+    }
+    for (cudaEvent_t e : sv->free_events) cudaEventDestroy(e);
     for (auto& g : sv->graphs) cudaGraphExecDestroy(g.second);
     for (auto& s : sv->solves)
         if (s.second.h) hier_free(s.second.h);
@@ -635,6 +694,7 @@ int pb_serve_destroy(pb_serve* sv)
     cudaFreeHost(sv->h_norms);
     cudaFreeHost(sv->h_r0);
     if (sv->st) cudaStreamDestroy(sv->st);
+    if (sv->cst) cudaStreamDestroy(sv->cst);
     delete sv;
     return PB_OK;
 }
@@ -669,6 +729,7 @@ int pb_serve_step(pb_serve* sv, int* active, int* waiting)
     };
     clk::time_point t0 = clk::now();
     int e;
+    if ((e = drain(sv, false)) != PB_OK) return e;
     if ((e = admit(sv)) != PB_OK) return e;
     sv->t_stage[0] += lap(t0);
     bool any = false;
@@ -721,13 +782,15 @@ int pb_serve_step(pb_serve* sv, int* active, int* waiting)
             }
             s.cycles++;
             s.r = sv->h_norms[i];
-            if (s.r < sv->p.tol * s.r0) retire(sv, s, PB_SERVE_DONE);
-            else if (s.cycles >= sv->p.max_cycles) retire(sv, s, PB_SERVE_FAILED);
+            if (s.r < sv->p.tol * s.r0) e = retire(sv, s, PB_SERVE_DONE);
+            else if (s.cycles >= sv->p.max_cycles) e = retire(sv, s, PB_SERVE_FAILED);
+            if (e != PB_OK) return e;
         }
-        PB_CUDA(cudaStreamSynchronize(sv->st));   // results are on the host when step returns
         sv->t_stage[4] += lap(t0);
+    } else if ((e = drain(sv, true)) != PB_OK) {   // nothing in flight: deliver what is on its way
+        return e;
     }
-    int na = 0;
+    int na = (int)sv->pending.size();
     for (long long t : sv->slots) na += t ? 1 : 0;
     if (active) *active = na;
     if (waiting) *waiting = (int)sv->waiting.size();
@@ -737,6 +800,8 @@ int pb_serve_step(pb_serve* sv, int* active, int* waiting)
 int pb_serve_poll(pb_serve* sv, long long* tickets, int cap, int* n)
 {
     if (!sv || !n || (cap > 0 && !tickets)) return PB_ERR_ARG;
+    const int e = drain(sv, false);
+    if (e != PB_OK) return e;
     const int k = std::min(cap, (int)sv->completed.size());
     for (int i = 0; i < k; i++) tickets[i] = sv->completed[i];
     sv->completed.erase(sv->completed.begin(), sv->completed.begin() + k);

@@ -176,6 +176,132 @@ __global__ void __launch_bounds__(kSvUnit) k_sv_phase(const SvItem* __restrict__
     }
 }
 
+// The stencil phases (sweep, sweep + FP64 update, FP64 residual pass) as warp column walks: a unit
+// is (row y, 32-wide x chunk, z chunk of kSvZ planes); a warp's lanes take consecutive x and walk
+// z with a register window of the 7-point stencil's z taps; +-x come from neighbouring lanes
+// (shuffles; the chunk's end lanes load the cell beyond, a ghost image at the box faces), +-y are
+// direct loads. Terms are summed in the Laplacian's insertion order, so results are bitwise the
+// row kernel's.
+constexpr int kSvZ = 16;
+
+__device__ __forceinline__ void sv_walk_units(int n, int& xc_count, int& zc_count)
+{
+    xc_count = (n + 31) / 32;
+    zc_count = (n + kSvZ - 1) / kSvZ;
+}
+
+template <int OP, typename V>
+__global__ void __launch_bounds__(kSvUnit) k_sv_walk(const SvItem* __restrict__ items, const long long* __restrict__ unit0,
+                                                     const SvPhaseHeader* __restrict__ hdr, double* norms)
+{
+    const int count = (int)hdr->count;
+    const long long total = hdr->total;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (long long w0 = (long long)blockIdx.x * kSvRows; w0 < total; w0 += (long long)gridDim.x * kSvRows) {
+        const SvItem& it = items[sv_find(unit0, count, w0)];
+        const int unit = (int)(w0 - it.unit0) + warp;
+        double m = 0.0;
+        if (unit < it.units) {
+            const int n = it.k.n;
+            int XC, ZC;
+            sv_walk_units(n, XC, ZC);
+            const int y = unit % n, xc = (unit / n) % XC, zc = unit / (n * XC);
+            const int x = xc * 32 + lane;
+            const bool act = x < n;
+            const bool last = act && (lane == 31 || x == n - 1);
+            const int z0 = zc * kSvZ, z1 = min(z0 + kSvZ, n);
+            // source field (FP32 level for the sweeps, FP64 u for the residual pass)
+            const V* src;
+            int sx;
+            if constexpr (OP == SV_K1) {
+                src = reinterpret_cast<const V*>(it.u64);
+                sx = it.sxd;
+            } else {
+                src = reinterpret_cast<const V*>(it.in);
+                sx = it.k.sx;
+            }
+            const int Sy = sx, Sz = sx * (n + 2);
+            const V* c = src + (long long)grown_index<V>(n, sx, act ? x : 0, y, z0);   // (x, y, z0)
+            Coefs<V> cf;
+            if constexpr (OP == SV_K1) cf = it.c64;
+            else cf = it.c;
+            const int ey = edge_code(y, n), ex = act ? edge_code(x, n) : 0;
+            V zm = act ? c[-Sz] : V(0), z_ = act ? c[0] : V(0);
+            for (int z = z0; z < z1; z++) {
+                const V zp = act ? c[Sz] : V(0);
+                // neighbours along x from the lanes beside (the chunk's end lanes load them)
+                V xm = __shfl_up_sync(0xffffffffu, z_, 1);
+                V xp = __shfl_down_sync(0xffffffffu, z_, 1);
+                if (act && lane == 0) xm = c[-1];
+                if (last) xp = c[1];
+                if (act) {
+                    const V ym = c[-Sy], yp = c[Sy];
+                    const int i = x + n * (y + n * z);
+                    const int ez = edge_code(z, n);
+                    // Laplacian insertion order: 0, +x, -x, +y, -y, +z, -z
+                    if constexpr (OP == SV_K1) {
+                        double res;
+                        float al = 0.f;
+                        if (!it.k.helm) {
+                            res = dadd(0.0, it.f64[i]);
+                            res = dadd(res, dmul(cf.c[0], (double)z_));
+                            res = dadd(res, dmul(cf.c[1], (double)xp));
+                            res = dadd(res, dmul(cf.c[2], (double)xm));
+                            res = dadd(res, dmul(cf.c[3], (double)yp));
+                            res = dadd(res, dmul(cf.c[4], (double)ym));
+                            res = dadd(res, dmul(cf.c[5], (double)zp));
+                            res = dadd(res, dmul(cf.c[6], (double)zm));
+                        } else {
+                            double lp = 0.0;
+                            lp = dadd(lp, dmul(cf.c[0], (double)z_));
+                            lp = dadd(lp, dmul(cf.c[1], (double)xp));
+                            lp = dadd(lp, dmul(cf.c[2], (double)xm));
+                            lp = dadd(lp, dmul(cf.c[3], (double)yp));
+                            lp = dadd(lp, dmul(cf.c[4], (double)ym));
+                            lp = dadd(lp, dmul(cf.c[5], (double)zp));
+                            lp = dadd(lp, dmul(cf.c[6], (double)zm));
+                            res = dsub(it.f64[i], dsub(dmul(it.alpha64, (double)z_), dmul(it.beta64, lp)));
+                            al = __double2float_rn(it.alpha64);
+                        }
+                        m = upd_abs(m, res);
+                        const float r32 = __double2float_rn(res);
+                        it.out[i] = r32;
+                        float* q = it.in + grown_index<float>(n, it.k.sx, x, y, z);
+                        store_with_images(it.in, n, it.k.sx, q, ex, ey, ez, relax_value(it.k, 0.f, 0.f, r32, al));
+                    } else {
+                        float acc = 0.f;
+                        acc = dadd(acc, dmul(cf.c[0], (float)z_));
+                        acc = dadd(acc, dmul(cf.c[1], (float)xp));
+                        acc = dadd(acc, dmul(cf.c[2], (float)xm));
+                        acc = dadd(acc, dmul(cf.c[3], (float)yp));
+                        acc = dadd(acc, dmul(cf.c[4], (float)ym));
+                        acc = dadd(acc, dmul(cf.c[5], (float)zp));
+                        acc = dadd(acc, dmul(cf.c[6], (float)zm));
+                        const float v = relax_value(it.k, acc, (float)z_, it.rhs[i], it.alpha);
+                        if constexpr (OP == SV_RELAX) {
+                            const long long g = (c - src) + 0;
+                            store_with_images(it.out, n, sx, it.out + g, ex, ey, ez, v);
+                        } else {
+                            double* q = it.u64 + grown_index<double>(n, it.sxd, x, y, z);
+                            store_with_images(it.u64, n, it.sxd, q, ex, ey, ez, dadd(*q, (double)v));
+                        }
+                    }
+                }
+                zm = z_;
+                z_ = zp;
+                c += Sz;
+            }
+        }
+        if constexpr (OP == SV_K1) {
+            for (int o = 16; o > 0; o >>= 1) {
+                const double w = __shfl_down_sync(0xffffffffu, m, o);
+                m = (m < w) ? w : m;
+            }
+            if (lane == 0 && m > 0.0 && unit < it.units) atomic_max_nonneg(norms + it.slot, m);
+        }
+    }
+}
+
 // u64 (grown, periodic) -> dst (n^3), one launch per solve being retired
 static __global__ void __launch_bounds__(256) k_sv_pack_out(const double* __restrict__ u, double* dst, int n, int sxd)
 {

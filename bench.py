@@ -226,6 +226,23 @@ def run_amr_level(pb, torch, steps=100, reps=5, cpu=True, tune=True):
     return out
 
 
+def profile_serving(pb, torch, count=16, n=96, steps=2):
+    """A small in-flight batch for kernel captures: `count` Helmholtz solves of edge n submitted to
+    one serving engine (public API, pinned host buffers), `steps` V-cycles for all of them."""
+    from proto_b200 import serving as S
+    from proto_b200 import workloads as W
+    eng = pb.Serve(8 << 30, max_active=count, tol=1e-30, max_cycles=steps)
+    f = S.pinned(n ** 3)
+    f[:] = W.sine_modes_rhs(n, seed=5, modes=4).reshape(-1)
+    outs = [S.pinned(n ** 3) for _ in range(count)]
+    for k in range(count):
+        eng.submit(n, f, outs[k], form=pb.MG_HELMHOLTZ, alpha=0.25 + 0.5 * k / count)
+    eng.run_until_idle()
+    eng.poll()
+    torch.cuda.synchronize()
+    pb.device_check()
+
+
 def run_serving(pb, count):
     """Request stream of periodic Poisson/Helmholtz solves (Poisson arrivals at 200/s, seed 4; edge
     log-uniform in [32, 192] rounded to 16; alpha ~ U[0, 1]; 4-mode right-hand sides; tolerance
@@ -282,6 +299,8 @@ def main():
                     help="run one 256^3 FP64 sweep, one FP32 sweep and one Stencil::apply, then exit (for ncu)")
     ap.add_argument("--profile-level", action="store_true",
                     help="run the AMR-level setup and 2 graph steps with default tiles, then exit (for ncu)")
+    ap.add_argument("--profile-serving", action="store_true",
+                    help="16 in-flight 96^3 Helmholtz solves, 2 V-cycles (small case for kernel captures)")
     ap.add_argument("--serve-requests", type=int, default=2000)
     args = ap.parse_args()
 
@@ -299,6 +318,8 @@ def main():
         return profile_kernels(pb, torch)
     if args.profile_level:
         return run_amr_level(pb, torch, steps=2, reps=1, cpu=False, tune=False)
+    if args.profile_serving:
+        return profile_serving(pb, torch)
     dist = None
     if world > 1:
         import torch.distributed as dist

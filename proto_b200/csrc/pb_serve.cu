@@ -217,8 +217,8 @@ RelaxCoef<float> level_coef(const pb_serve_params& p, const pb_serve_request& q,
     return k;
 }
 
-// units of the column-walk phases: rows x 32-wide x chunks x kSvZ-deep z chunks
-int walk_units(int e) { return e * ((e + 31) / 32) * ((e + kSvZ - 1) / kSvZ); }
+// units of the column-walk phases: rows x 32-wide x chunks x zd-deep z chunks
+long long walk_units(int e, int zd) { return (long long)e * ((e + 31) / 32) * ((e + zd - 1) / zd); }
 
 double level_hsqinv(int n, int d)
 {
@@ -269,12 +269,32 @@ std::vector<PhaseSlot> phase_plan(const pb_serve_params& p, int D)
 // buffer index holding a level's current solution just before each phase, following the
 // single-solve solver's ping-pong: depth 0 starts at 1 (the residual pass wrote phi[1]), deeper
 // levels start from zero (their first sweep writes phi[1])
-void add_item(std::vector<SvItem>& items, long long& total, SvItem it)
+// Lays a phase's items out in unit order. Column-walk phases take the deepest z chunk (kSvZ, 8, 4
+// or 2 planes) that still gives every warp of the persistent grid a unit: deep chunks reuse more
+// z planes from registers, shallow ones keep a small batch from leaving most SMs idle.
+long long layout_items(std::vector<SvItem>& items, bool walk, long long warps)
 {
-    it.unit0 = total;
-    total += ((long long)it.units + kSvRows - 1) / kSvRows * kSvRows;
-    items.push_back(it);
+    if (walk) {
+        int zd = kSvZ;
+        for (;; zd /= 2) {
+            long long sum = 0;
+            for (const SvItem& it : items) sum += walk_units(it.k.n, zd);
+            if (sum >= warps || zd <= 2) break;
+        }
+        for (SvItem& it : items) {
+            it.zd = zd;
+            it.units = (int)walk_units(it.k.n, zd);
+        }
+    }
+    long long total = 0;
+    for (SvItem& it : items) {
+        it.unit0 = total;
+        total += ((long long)it.units + kSvRows - 1) / kSvRows * kSvRows;
+    }
+    return total;
 }
+
+bool is_walk(int op) { return op == SV_RELAX || op == SV_UPDATE || op == SV_K1; }
 
 } // namespace
 
@@ -297,6 +317,7 @@ static int build_lists(pb_serve* sv)
         sv->h_unit0.assign((size_t)sv->max_phases * cap, 0);
     }
     sv->h_hdr.assign(sv->max_phases, SvPhaseHeader{0, 0});
+    const long long warps = (long long)sv->grid * kSvRows;
     // per solve: the buffer index of each level's current solution as the plan advances
     std::vector<std::vector<int>> cur(act.size());
     for (size_t a = 0; a < act.size(); a++) {
@@ -307,7 +328,6 @@ static int build_lists(pb_serve* sv)
         const PhaseSlot& ps = plan[ph];
         if (ps.op < 0) continue;   // coarse: its own argument table
         std::vector<SvItem> items;
-        long long total = 0;
         for (size_t a = 0; a < act.size(); a++) {
             SvSolve& s = *act[a];
             SvHier& h = *s.h;
@@ -334,7 +354,6 @@ static int build_lists(pb_serve* sv)
                 it.out = ph_[1 - c];
                 it.rhs = h.rhs[d];
                 it.c = lap7_coefs<float>(helm ? level_hsqinv(n, d) : p.omega / 6.0);
-                it.units = walk_units(e);
                 if (ps.op == SV_RELAX) c = 1 - c;
                 break;
             case SV_RELAX_FIRST:
@@ -368,13 +387,13 @@ static int build_lists(pb_serve* sv)
                 it.out = h.rhs[0];
                 const double hs = level_hsqinv(n, 0);
                 it.c64 = lap7_coefs<double>(helm ? hs : -hs);
-                it.units = walk_units(e);
                 c = 1;
                 break;
             }
             }
-            add_item(items, total, it);
+            items.push_back(it);
         }
+        const long long total = layout_items(items, is_walk(ps.op), warps);
         std::copy(items.begin(), items.end(), sv->h_items.begin() + ph * cap);
         for (size_t k = 0; k < items.size(); k++) sv->h_unit0[ph * cap + k] = items[k].unit0;
         sv->h_hdr[ph] = SvPhaseHeader{(long long)items.size(), total};
@@ -383,7 +402,6 @@ static int build_lists(pb_serve* sv)
     {
         const int ph = sv->max_phases - 1;
         std::vector<SvItem> items;
-        long long total = 0;
         for (size_t a = 0; a < act.size(); a++) {
             SvSolve& s = *act[a];
             if (!s.fresh) continue;
@@ -403,9 +421,9 @@ static int build_lists(pb_serve* sv)
             it.out = h.rhs[0];
             const double hs = level_hsqinv(h.n, 0);
             it.c64 = lap7_coefs<double>(helm ? hs : -hs);
-            it.units = walk_units(h.n);
-            add_item(items, total, it);
+            items.push_back(it);
         }
+        const long long total = layout_items(items, true, warps);
         std::copy(items.begin(), items.end(), sv->h_items.begin() + (size_t)ph * cap);
         for (size_t k = 0; k < items.size(); k++) sv->h_unit0[(size_t)ph * cap + k] = items[k].unit0;
         sv->h_hdr[ph] = SvPhaseHeader{(long long)items.size(), total};

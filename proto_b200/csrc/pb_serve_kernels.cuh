@@ -35,6 +35,7 @@ struct SvItem {
     int sxc;               // prolong: coarse pitch
     int sxd;               // K1 / update: pitch of u64
     int slot;              // solve slot (norms)
+    int zd;                // column-walk phases: z planes per unit (chosen per phase)
     int units;             // rows of this item
     long long unit0;       // first row (multiple of kSvRows)
 };
@@ -182,12 +183,12 @@ __global__ void __launch_bounds__(kSvUnit) k_sv_phase(const SvItem* __restrict__
 // (shuffles; the chunk's end lanes load the cell beyond, a ghost image at the box faces), +-y are
 // direct loads. Terms are summed in the Laplacian's insertion order, so results are bitwise the
 // row kernel's.
-constexpr int kSvZ = 16;
+constexpr int kSvZ = 16;   // deepest z chunk (a phase with few units takes shallower ones)
 
-__device__ __forceinline__ void sv_walk_units(int n, int& xc_count, int& zc_count)
+__device__ __forceinline__ void sv_walk_units(int n, int zd, int& xc_count, int& zc_count)
 {
     xc_count = (n + 31) / 32;
-    zc_count = (n + kSvZ - 1) / kSvZ;
+    zc_count = (n + zd - 1) / zd;
 }
 
 template <int OP, typename V>
@@ -203,13 +204,14 @@ __global__ void __launch_bounds__(kSvUnit) k_sv_walk(const SvItem* __restrict__ 
         double m = 0.0;
         if (unit < it.units) {
             const int n = it.k.n;
+            const int zd = it.zd;
             int XC, ZC;
-            sv_walk_units(n, XC, ZC);
+            sv_walk_units(n, zd, XC, ZC);
             const int y = unit % n, xc = (unit / n) % XC, zc = unit / (n * XC);
             const int x = xc * 32 + lane;
             const bool act = x < n;
             const bool last = act && (lane == 31 || x == n - 1);
-            const int z0 = zc * kSvZ, z1 = min(z0 + kSvZ, n);
+            const int z0 = zc * zd, z1 = min(z0 + zd, n);
             // source field (FP32 level for the sweeps, FP64 u for the residual pass)
             const V* src;
             int sx;

@@ -176,19 +176,34 @@ __global__ void __launch_bounds__(kLevelThreads) k_level_star_fused(const double
     }
 }
 
-// Shared-memory variant of the fused step: per z plane the CTA stages its (tx+2R) x (ty+2R) tile
-// of the plane (halo cells from the face neighbours; the corner cells, which a star stencil never
-// reads, are skipped), then takes the x/y taps from shared memory and the z taps from a per-column
-// register window. Bitwise the other two paths (same values, same term order).
-constexpr int kLevelSmemMax = (64 + 4) * (16 + 4);   // widest tile (tx = 64, ty = 4 at R = 2; 16x16 fits too)
+// Shared-memory variant of the fused step. Per z plane the CTA stages its (tx+2R) x (ty+2R) tile of
+// the plane (halo cells from the face neighbours; the corner cells, which a star stencil never
+// reads, are skipped) with per-thread asynchronous copies (cp.async) into a ring of kLevelRing(R)
+// planes, kLevelLead planes ahead of the one being computed; x/y taps come from the ring, z taps
+// from a per-column register window that is filled from the ring's centre column (from global
+// memory for the R planes past the tile's z chunk). One barrier per plane. Bitwise the other two
+// paths (same values, same term order).
+constexpr int kLevelPlaneMax = (64 + 4) * (4 + 4);   // (tx+2R)(ty+2R) <= 544 for every tile shape at R <= 2
+constexpr int kLevelPrefetch = 3;                    // planes in flight beyond the newest one waited for
+__host__ __device__ constexpr int level_lead(int R) { return R + kLevelPrefetch; }
+__host__ __device__ constexpr int level_ring(int R) { return level_lead(R) + 1; }
+
+__device__ __forceinline__ void cp_async8(uint32_t dst, const void* src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 template <class S>
 __global__ void __launch_bounds__(kLevelThreads) k_level_star_tiled(const double* __restrict__ u, double* out,
                                                                     const PatchTile* __restrict__ tiles,
                                                                     Coefs<double> cf, double a, int euler)
 {
-    constexpr int R = S::R, W = 2 * R + 1;
-    __shared__ double plane[kLevelSmemMax];
+    constexpr int R = S::R, W = 2 * R + 1, L = level_lead(R), Q = level_ring(R);
+    static_assert(R <= 2, "plane buffer sized for R <= 2");
+    __shared__ __align__(16) double ring[Q * kLevelPlaneMax];
     const PatchTile t = tiles[blockIdx.x];
     const int tx = t.tx, ty = kLevelThreads / t.tx;
     const int BX = tx + 2 * R, BY = ty + 2 * R;
@@ -198,8 +213,9 @@ __global__ void __launch_bounds__(kLevelThreads) k_level_star_tiled(const double
     const int lx = threadIdx.x % tx, ly = threadIdx.x / tx;
     const int x = t.x0 + lx, y = t.y0 + ly;
     const bool act = x < nx && y < ny;
+    const int z1 = min(t.z0 + t.zd, nz);
     // this thread's staging assignments are fixed across planes: base pointer and plane stride each
-    constexpr int kMaxLoads = 3;   // (tx+2R)(ty+2R) <= 544 cells for every tile shape, 256 threads
+    constexpr int kMaxLoads = (kLevelPlaneMax + kLevelThreads - 1) / kLevelThreads;
     const double* lp[kMaxLoads];
     long long ls[kMaxLoads];
     bool lv_[kMaxLoads];
@@ -237,6 +253,19 @@ __global__ void __launch_bounds__(kLevelThreads) k_level_star_tiled(const double
         lp[k] = p + st * t.z0;
         ls[k] = st;
     }
+    const uint32_t ring0 = smem_u32(ring) + 8u * threadIdx.x;
+    // stage plane zz (< z1) into ring slot q; every call commits one group (empty past z1)
+    auto stage = [&](int zz, int q) {
+        if (zz < z1) {
+#pragma unroll
+            for (int k = 0; k < kMaxLoads; k++)
+                if (lv_[k]) {
+                    cp_async8(ring0 + 8u * (q * kLevelPlaneMax + k * kLevelThreads), lp[k]);
+                    lp[k] += ls[k];
+                }
+        }
+        cp_async_commit();
+    };
     // own column (z taps) with its z neighbours
     const long long cxy = (x + g0) + Sx * (y + g1) + Sxy * g2;
     const double* col = u + t.off + cxy;
@@ -246,7 +275,8 @@ __global__ void __launch_bounds__(kLevelThreads) k_level_star_tiled(const double
         if (zz >= nz) return __ldg(colzh + Sxy * (zz - nz));
         return __ldg((zz < 0 ? colzl : col) + Sxy * zz);
     };
-    const int z1 = min(t.z0 + t.zd, nz);
+#pragma unroll
+    for (int k = 0; k < L; k++) stage(t.z0 + k, k);
     double win[W];
     if (act) {
 #pragma unroll
@@ -254,21 +284,22 @@ __global__ void __launch_bounds__(kLevelThreads) k_level_star_tiled(const double
     }
     double* op = out + t.off + cxy + Sxy * t.z0;
     const int sc = (ly + R) * BX + (lx + R);
+    int qz = 0;                          // ring slot of plane z
     for (int z = t.z0; z < z1; z++) {
-#pragma unroll
-        for (int k = 0; k < kMaxLoads; k++)
-            if (lv_[k]) {
-                plane[threadIdx.x + k * kLevelThreads] = __ldg(lp[k]);
-                lp[k] += ls[k];
-            }
-        if (act) win[2 * R] = zcol(z + R);
-        __syncthreads();
+        cp_async_wait<L - R - 1>();      // this thread's copies of plane z + R have landed
+        __syncthreads();                 // everyone's have; everyone is done with plane z - 1
+        const int qn = qz == 0 ? Q - 1 : qz - 1;   // slot of plane z - 1 = slot of plane z + L
+        stage(z + L, qn);
+        const double* pl = ring + qz * kLevelPlaneMax;
         if (act) {
+            int qr = qz + R;
+            if (qr >= Q) qr -= Q;
+            win[2 * R] = z + R < z1 ? ring[qr * kLevelPlaneMax + sc] : zcol(z + R);
             double acc = 0.0;
 #pragma unroll
             for (int j = 0; j < S::NT; j++) {
                 const int ox = S::off(j, 0), oy = S::off(j, 1), oz = S::off(j, 2);
-                const double v = (oz != 0 || (ox == 0 && oy == 0)) ? win[R + oz] : plane[sc + oy * BX + ox];
+                const double v = (oz != 0 || (ox == 0 && oy == 0)) ? win[R + oz] : pl[sc + oy * BX + ox];
                 acc = dadd(acc, dmul(cf.c[j], v));
             }
             *op = euler ? dadd(win[R], dmul(a, acc)) : acc;
@@ -276,8 +307,9 @@ __global__ void __launch_bounds__(kLevelThreads) k_level_star_tiled(const double
             for (int k = 0; k < 2 * R; k++) win[k] = win[k + 1];
         }
         op += Sxy;
-        __syncthreads();
+        qz = qz == Q - 1 ? 0 : qz + 1;
     }
+    cp_async_wait<0>();                  // no copy outlives the block
 }
 
 } // namespace pb

@@ -169,9 +169,10 @@ int pb_level_stencil_f64(const pb_level* lv, const pb_stencil* s, int epilogue, 
  * No counterpart in the reference, whose callers loop over exchange and per-patch stencils. */
 int pb_level_steps_f64(pb_level* lv, const pb_stencil* s, int epilogue, double* u_slab, double* tmp_slab,
                        double scale, double a, int steps, void* stream);
-/* Times the batched stencil per patch-size class (valid x extent) over a few tile shapes (columns
- * along x, planes per thread) and keeps the fastest per class (blocks until done; out_slab is
- * overwritten). pb_level_tiles reports the choice as (x extent, columns, planes) triples. */
+/* Times the batched stencil per patch-size class (valid x extent) over a few tile shapes (tile
+ * width along x, planes per thread) and keeps the fastest per class (blocks until done; out_slab is
+ * overwritten). pb_level_tiles reports the shapes of the fused halo-2 step as (x extent, tile width
+ * in cells, planes) triples. */
 int pb_level_autotune_f64(pb_level* lv, const pb_stencil* s, const double* u_slab, double* out_slab,
                           double scale, void* stream);
 int pb_level_tiles(const pb_level* lv, int* triples, int cap, int* n);

@@ -51,7 +51,8 @@ struct PatchTile {
     int gh[3];                 // ghost widths (valid cell (0,0,0) sits at grown (gh0, gh1, gh2))
     int vn[3];                 // valid box extents
     int x0, y0, z0;            // tile origin in valid coordinates
-    int tx, zd;                // columns along x (ty = 256 / tx) and planes per thread
+    int tx, zd;                // threads along x (ty = 256 / tx) and planes per thread
+    int xv;                    // x cells per thread (the tile is xv*tx cells wide)
     // face neighbours along each axis (tensor-product periodic tilings; read directly instead of
     // ghost cells): slab offset, valid extent and grown extent along that axis, low / high side
     long long nb_off[3][2];
@@ -312,6 +313,162 @@ __global__ void __launch_bounds__(kLevelThreads) k_level_star_tiled(const double
     cp_async_wait<0>();                  // no copy outlives the block
 }
 
+// Two adjacent x cells per thread, for halo width 2 on layouts where every patch's x extent, the x
+// ghost width and the slab are even (pb_level checks this): every staged pair of cells and every
+// output pair then sits on a 16-byte boundary, so the ring is filled with 16-byte cp.async copies
+// and the x/y taps are read as double2. The tile is (2 tx) x ty cells. Same terms in the same order
+// per cell, so bitwise the one-cell paths.
+constexpr int kLevelPairPlaneMax = (64 + 4) * (8 + 4);   // (2tx+4)(ty+4) <= 816 for tx in {8, 16, 32}
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+
+template <class S>
+__global__ void __launch_bounds__(kLevelThreads) k_level_star_pair(const double* __restrict__ u, double* out,
+                                                                   const PatchTile* __restrict__ tiles,
+                                                                   Coefs<double> cf, double a, int euler)
+{
+    constexpr int R = S::R, W = 2 * R + 1, L = level_lead(R), Q = level_ring(R), PM = kLevelPairPlaneMax;
+    static_assert(R == 2, "cell pairs line up with 16-byte boundaries for a halo of 2");
+    __shared__ __align__(16) double ring[Q * PM];
+    const PatchTile t = tiles[blockIdx.x];
+    const int tx = t.tx, ty = kLevelThreads / t.tx;
+    const int BX = 2 * tx + 2 * R, BY = ty + 2 * R, PX = BX / 2;
+    const int nx = t.vn[0], ny = t.vn[1], nz = t.vn[2];
+    const int g0 = t.gh[0], g1 = t.gh[1], g2 = t.gh[2];
+    const long long Sx = t.gS[0], Sy = t.gS[1], Sxy = Sx * Sy;
+    const int lx = threadIdx.x % tx, ly = threadIdx.x / tx;
+    const int x = t.x0 + 2 * lx, y = t.y0 + ly;
+    const bool act = x < nx && y < ny;
+    const int z1 = min(t.z0 + t.zd, nz);
+    constexpr int kMaxLoads = (PM / 2 + kLevelThreads - 1) / kLevelThreads;
+    const double* lp[kMaxLoads];
+    long long ls[kMaxLoads];
+    bool lv_[kMaxLoads];
+#pragma unroll
+    for (int k = 0; k < kMaxLoads; k++) {
+        const int i = threadIdx.x + k * kLevelThreads;   // pair index in the staged tile
+        const int hx = i % PX, hy = i / PX;
+        const int xx = t.x0 - R + 2 * hx, yy = t.y0 - R + hy;
+        const bool xo = xx < 0 || xx >= nx, yo = yy < 0 || yy >= ny;
+        lv_[k] = i < PX * BY && !(xo && yo) && xx < nx + R && yy < ny + R;   // corners never read
+        lp[k] = u;
+        ls[k] = 0;
+        if (!lv_[k]) continue;
+        const double* p;
+        long long st = Sxy;
+        if (xx < 0) {
+            const long long Sq = t.nb_S[0][0];
+            p = u + t.nb_off[0][0] + (xx + t.nb_n[0][0] + g0) + Sq * ((yy + g1) + Sy * g2);
+            st = Sq * Sy;
+        } else if (xx >= nx) {
+            const long long Sq = t.nb_S[0][1];
+            p = u + t.nb_off[0][1] + (xx - nx + g0) + Sq * ((yy + g1) + Sy * g2);
+            st = Sq * Sy;
+        } else if (yy < 0) {
+            const long long Sq = t.nb_S[1][0];
+            p = u + t.nb_off[1][0] + (xx + g0) + Sx * ((yy + t.nb_n[1][0] + g1) + Sq * g2);
+            st = Sx * Sq;
+        } else if (yy >= ny) {
+            const long long Sq = t.nb_S[1][1];
+            p = u + t.nb_off[1][1] + (xx + g0) + Sx * ((yy - ny + g1) + Sq * g2);
+            st = Sx * Sq;
+        } else {
+            p = u + t.off + (xx + g0) + Sx * (yy + g1) + Sxy * g2;
+        }
+        lp[k] = p + st * t.z0;
+        ls[k] = st;
+    }
+    const uint32_t ring0 = smem_u32(ring) + 16u * threadIdx.x;
+    auto stage = [&](int zz, int q) {
+        if (zz < z1) {
+#pragma unroll
+            for (int k = 0; k < kMaxLoads; k++)
+                if (lv_[k]) {
+                    cp_async16(ring0 + 8u * (q * PM + 2 * k * kLevelThreads), lp[k]);
+                    lp[k] += ls[k];
+                }
+        }
+        cp_async_commit();
+    };
+    const long long cxy = (x + g0) + Sx * (y + g1) + Sxy * g2;
+    const double* col = u + t.off + cxy;
+    const double* colzl = u + t.nb_off[2][0] + cxy + Sxy * t.nb_n[2][0];
+    const double* colzh = u + t.nb_off[2][1] + cxy;
+    auto zcol = [&](int zz) -> double2 {
+        const double* q = zz >= nz ? colzh + Sxy * (zz - nz) : (zz < 0 ? colzl : col) + Sxy * zz;
+        return __ldg(reinterpret_cast<const double2*>(q));
+    };
+#pragma unroll
+    for (int k = 0; k < L; k++) stage(t.z0 + k, k);
+    double w0[W], w1[W];
+    if (act) {
+#pragma unroll
+        for (int k = 0; k < 2 * R; k++) {
+            const double2 v = zcol(t.z0 - R + k);
+            w0[k] = v.x;
+            w1[k] = v.y;
+        }
+    }
+    double* op = out + t.off + cxy + Sxy * t.z0;
+    const int sc = (ly + R) * BX + (2 * lx + R);   // even: pairs are 16-byte aligned in the ring
+    int qz = 0;
+    for (int z = t.z0; z < z1; z++) {
+        cp_async_wait<L - R - 1>();
+        __syncthreads();
+        const int qn = qz == 0 ? Q - 1 : qz - 1;
+        stage(z + L, qn);
+        const double* pl = ring + qz * PM + sc;
+        if (act) {
+            int qr = qz + R;
+            if (qr >= Q) qr -= Q;
+            const double2 cn = z + R < z1 ? *reinterpret_cast<const double2*>(ring + qr * PM + sc) : zcol(z + R);
+            w0[2 * R] = cn.x;
+            w1[2 * R] = cn.y;
+            const double2 xm = *reinterpret_cast<const double2*>(pl - 2);   // x-2, x-1
+            const double2 xc = *reinterpret_cast<const double2*>(pl);       // x, x+1
+            const double2 xp = *reinterpret_cast<const double2*>(pl + 2);   // x+2, x+3
+            const double2 ym1 = *reinterpret_cast<const double2*>(pl - BX);
+            const double2 yp1 = *reinterpret_cast<const double2*>(pl + BX);
+            const double2 ym2 = *reinterpret_cast<const double2*>(pl - 2 * BX);
+            const double2 yp2 = *reinterpret_cast<const double2*>(pl + 2 * BX);
+            double a0 = 0.0, a1 = 0.0;
+#pragma unroll
+            for (int j = 0; j < S::NT; j++) {
+                const int ox = S::off(j, 0), oy = S::off(j, 1), oz = S::off(j, 2);
+                double v0, v1;
+                if (oz != 0 || (ox == 0 && oy == 0)) {
+                    v0 = w0[R + oz];
+                    v1 = w1[R + oz];
+                } else if (oy != 0) {
+                    const double2 q = oy == 1 ? yp1 : oy == -1 ? ym1 : oy == 2 ? yp2 : ym2;
+                    v0 = q.x;
+                    v1 = q.y;
+                } else {
+                    v0 = ox == -2 ? xm.x : ox == -1 ? xm.y : ox == 1 ? xc.y : xp.x;
+                    v1 = ox == -2 ? xm.y : ox == -1 ? xc.x : ox == 1 ? xp.x : xp.y;
+                }
+                a0 = dadd(a0, dmul(cf.c[j], v0));
+                a1 = dadd(a1, dmul(cf.c[j], v1));
+            }
+            double2 r;
+            r.x = euler ? dadd(w0[R], dmul(a, a0)) : a0;
+            r.y = euler ? dadd(w1[R], dmul(a, a1)) : a1;
+            *reinterpret_cast<double2*>(op) = r;
+#pragma unroll
+            for (int k = 0; k < 2 * R; k++) {
+                w0[k] = w0[k + 1];
+                w1[k] = w1[k + 1];
+            }
+        }
+        op += Sxy;
+        qz = qz == Q - 1 ? 0 : qz + 1;
+    }
+    cp_async_wait<0>();
+}
+
 } // namespace pb
 
 struct pb_level {
@@ -324,10 +481,14 @@ struct pb_level {
     long long slab_elems;
     std::vector<pb::MotionItem> items;
     pb::MotionItem* d_items = nullptr;
-    std::vector<pb::PatchTile> tiles;
+    std::vector<pb::PatchTile> tiles;          // one cell per thread
     pb::PatchTile* d_tiles = nullptr;
+    std::vector<pb::PatchTile> tiles2;         // two x cells per thread (fused halo-2 steps, pair_ok)
+    pb::PatchTile* d_tiles2 = nullptr;
+    bool pair_ok = false;                      // tensor tiling, even x extents and x ghost
     int device = 0;
-    std::map<int, std::pair<int, int>> tune;   // valid x extent -> (tx, zd)
+    std::map<int, std::pair<int, int>> tune;   // valid x extent -> (tx, zd), one cell per thread
+    std::map<int, std::pair<int, int>> tune2;  // the same for two cells per thread
     // periodic tensor-product tiling: face neighbour of patch i along axis d, side s
     bool tensor = false;
     bool tiled = true;                         // fused steps use the shared-memory tile kernel
@@ -389,10 +550,12 @@ static void build_items(pb_level* lv)
     }
 }
 
-static std::pair<int, int> tile_shape(const pb_level* lv, int nx)
+static std::pair<int, int> tile_shape(const pb_level* lv, int nx, int xv = 1)
 {
-    auto it = lv->tune.find(nx);
-    return it != lv->tune.end() ? it->second : std::make_pair(16, 8);
+    const auto& m = xv == 2 ? lv->tune2 : lv->tune;
+    auto it = m.find(nx);
+    if (it != m.end()) return it->second;
+    return xv == 2 ? std::make_pair(16, 16) : std::make_pair(16, 8);
 }
 
 // Recognises a periodic tensor-product tiling (every patch = X_i x Y_j x Z_k of per-axis interval
@@ -445,9 +608,10 @@ static void detect_tensor(pb_level* lv)
     lv->tensor = true;
 }
 
-static void build_tiles(pb_level* lv, int only_nx = -1)
+static void build_tiles(pb_level* lv, int xv = 1, int only_nx = -1)
 {
-    lv->tiles.clear();
+    std::vector<PatchTile>& tiles = xv == 2 ? lv->tiles2 : lv->tiles;
+    tiles.clear();
     const int np = (int)lv->patches.size();
     for (int i = 0; i < np; i++) {
         const Box3& v = lv->patches[i];
@@ -467,33 +631,41 @@ static void build_tiles(pb_level* lv, int only_nx = -1)
                 t.nb_n[d][sd] = (int)bsize(vq, d);
                 t.nb_S[d][sd] = (int)bsize(vq, d) + 2 * lv->ghost[d];
             }
-        const std::pair<int, int> sh = tile_shape(lv, t.vn[0]);
+        const std::pair<int, int> sh = tile_shape(lv, t.vn[0], xv);
         t.tx = sh.first;
         t.zd = sh.second;
+        t.xv = xv;
         const int ty = kLevelThreads / t.tx;
         for (int z0 = 0; z0 < t.vn[2]; z0 += t.zd)
             for (int y0 = 0; y0 < t.vn[1]; y0 += ty)
-                for (int x0 = 0; x0 < t.vn[0]; x0 += t.tx) {
+                for (int x0 = 0; x0 < t.vn[0]; x0 += xv * t.tx) {
                     t.x0 = x0;
                     t.y0 = y0;
                     t.z0 = z0;
-                    lv->tiles.push_back(t);
+                    tiles.push_back(t);
                 }
     }
 }
 
-static int upload_tiles(pb_level* lv)
+static int upload_tiles(pb_level* lv, int xv = 1)
 {
-    cudaFree(lv->d_tiles);
-    lv->d_tiles = nullptr;
-    if (lv->tiles.empty()) return PB_OK;
-    if (cudaMalloc(&lv->d_tiles, lv->tiles.size() * sizeof(PatchTile)) != cudaSuccess ||
-        cudaMemcpy(lv->d_tiles, lv->tiles.data(), lv->tiles.size() * sizeof(PatchTile), cudaMemcpyHostToDevice) !=
-            cudaSuccess) {
+    std::vector<PatchTile>& tiles = xv == 2 ? lv->tiles2 : lv->tiles;
+    PatchTile*& d = xv == 2 ? lv->d_tiles2 : lv->d_tiles;
+    cudaFree(d);
+    d = nullptr;
+    if (tiles.empty()) return PB_OK;
+    if (cudaMalloc(&d, tiles.size() * sizeof(PatchTile)) != cudaSuccess ||
+        cudaMemcpy(d, tiles.data(), tiles.size() * sizeof(PatchTile), cudaMemcpyHostToDevice) != cudaSuccess) {
         cudaGetLastError();
         return PB_ERR_CUDA;
     }
     return PB_OK;
+}
+
+// The two-cells-per-thread kernel applies: fused step of a halo-2 stencil, 16-byte aligned slabs.
+static bool use_pairs(const pb_level* lv, int shape, bool fused, const void* u, const void* out)
+{
+    return fused && lv->tiled && lv->pair_ok && shape == 2 && ((uintptr_t)u % 16) == 0 && ((uintptr_t)out % 16) == 0;
 }
 
 static void drop_graph(pb_level* lv)
@@ -524,9 +696,15 @@ static int level_coefs(const pb_level* lv, const pb_stencil* s, double scale, Co
 static int launch_level_star(const pb_level* lv, int shape, const double* u, double* out, const Coefs<double>& cf,
                              double a, int euler, cudaStream_t st, bool fused = false)
 {
+    if (fused && !lv->tensor) return PB_ERR_ARG;
+    if (use_pairs(lv, shape, fused, u, out)) {
+        const unsigned np = (unsigned)lv->tiles2.size();
+        if (np) k_level_star_pair<ShapeLap13><<<np, kLevelThreads, 0, st>>>(u, out, lv->d_tiles2, cf, a, euler);
+        PB_LAUNCH_CHECK();
+        return PB_OK;
+    }
     const unsigned nb = (unsigned)lv->tiles.size();
     if (nb == 0) return PB_OK;
-    if (fused && !lv->tensor) return PB_ERR_ARG;
     if (fused && lv->tiled) {
         if (shape == 1) k_level_star_tiled<ShapeLap7><<<nb, kLevelThreads, 0, st>>>(u, out, lv->d_tiles, cf, a, euler);
         else k_level_star_tiled<ShapeLap13><<<nb, kLevelThreads, 0, st>>>(u, out, lv->d_tiles, cf, a, euler);
@@ -570,7 +748,10 @@ int pb_level_create(const pb_box* patches, int npatch, const int ghost[3], pb_bo
     lv->slab_elems = off;
     build_items(lv);
     detect_tensor(lv);
+    lv->pair_ok = lv->tensor && ncomp == 1 && ghost[0] % 2 == 0;
+    for (const Box3& b : lv->patches) lv->pair_ok = lv->pair_ok && bsize(b, 0) % 2 == 0;
     build_tiles(lv);
+    if (lv->pair_ok) build_tiles(lv, 2);
     cudaGetDevice(&lv->device);
     if (!lv->items.empty()) {
         if (cudaMalloc(&lv->d_items, lv->items.size() * sizeof(MotionItem)) != cudaSuccess ||
@@ -581,8 +762,9 @@ int pb_level_create(const pb_box* patches, int npatch, const int ghost[3], pb_bo
             return PB_ERR_CUDA;
         }
     }
-    if (upload_tiles(lv) != PB_OK) {
+    if (upload_tiles(lv) != PB_OK || upload_tiles(lv, 2) != PB_OK) {
         cudaFree(lv->d_items);
+        cudaFree(lv->d_tiles);
         delete lv;
         return PB_ERR_CUDA;
     }
@@ -596,6 +778,7 @@ int pb_level_destroy(pb_level* lv)
     drop_graph(lv);
     cudaFree(lv->d_items);
     cudaFree(lv->d_tiles);
+    cudaFree(lv->d_tiles2);
     delete lv;
     return PB_OK;
 }
@@ -645,7 +828,8 @@ int pb_level_steps_f64(pb_level* lv, const pb_stencil* s, int epilogue, double* 
     if ((e = level_coefs(lv, s, scale, cf, shape)) != PB_OK) return e;
     cudaStream_t st = (cudaStream_t)stream;
     std::vector<double> key = {(double)(uintptr_t)u_slab, (double)(uintptr_t)tmp_slab, scale, a, (double)epilogue,
-                               (double)steps, (double)shape, (double)(uintptr_t)lv->d_tiles};
+                               (double)steps, (double)shape, (double)(uintptr_t)lv->d_tiles,
+                               (double)(uintptr_t)lv->d_tiles2};
     for (int j = 0; j < 13; j++) key.push_back(cf.c[j]);
     if (!lv->graph || key != lv->graph_key) {
         drop_graph(lv);
@@ -698,20 +882,25 @@ int pb_level_autotune_f64(pb_level* lv, const pb_stencil* s, const double* u_sla
     for (const Box3& b : lv->patches) classes.push_back((int)bsize(b, 0));
     std::sort(classes.begin(), classes.end());
     classes.erase(std::unique(classes.begin(), classes.end()), classes.end());
+    // the kernel the steps use: two cells per thread (tx up to 32, 64 cells) or one (tx up to 64)
+    const int xv = use_pairs(lv, shape, lv->tensor, u_slab, out_slab) ? 2 : 1;
+    auto& tune = xv == 2 ? lv->tune2 : lv->tune;
     static const int cand_tx[] = {8, 16, 32, 64};
     static const int cand_zd[] = {4, 8, 16, 32};
+    const int ntx = xv == 2 ? 3 : 4;
     cudaEvent_t e0, e1;
     PB_CUDA(cudaEventCreate(&e0));
     PB_CUDA(cudaEventCreate(&e1));
     for (int nx : classes) {
         float best = 1e30f;
-        std::pair<int, int> pick = tile_shape(lv, nx);
-        for (int tx : cand_tx) {
-            if (tx > 2 * nx && tx != cand_tx[0]) continue;   // mostly idle columns
+        std::pair<int, int> pick = tile_shape(lv, nx, xv);
+        for (int ti = 0; ti < ntx; ti++) {
+            const int tx = cand_tx[ti];
+            if (xv * tx > 2 * nx && ti != 0) continue;   // mostly idle columns
             for (int zd : cand_zd) {
-                lv->tune[nx] = {tx, zd};
-                build_tiles(lv, nx);
-                if ((e = upload_tiles(lv)) != PB_OK) break;
+                tune[nx] = {tx, zd};
+                build_tiles(lv, xv, nx);
+                if ((e = upload_tiles(lv, xv)) != PB_OK) break;
                 for (int w = 0; w < 2; w++) launch_level_star(lv, shape, u_slab, out_slab, cf, 0.0, 0, st, lv->tensor);
                 cudaEventRecord(e0, st);
                 for (int r = 0; r < 5; r++) launch_level_star(lv, shape, u_slab, out_slab, cf, 0.0, 0, st, lv->tensor);
@@ -726,18 +915,19 @@ int pb_level_autotune_f64(pb_level* lv, const pb_stencil* s, const double* u_sla
             }
             if (e != PB_OK) break;
         }
-        lv->tune[nx] = pick;
+        tune[nx] = pick;
         if (e != PB_OK) break;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    build_tiles(lv);
-    const int e2 = upload_tiles(lv);
+    build_tiles(lv, xv);
+    const int e2 = upload_tiles(lv, xv);
     drop_graph(lv);
     return e != PB_OK ? e : e2;
 }
 
-// The chosen tile shape of each patch-size class: up to cap entries of (x extent, tx, zd).
+// The tile shape of each patch-size class used by the fused halo-2 step (the two-cells-per-thread
+// tiles where the layout allows them): up to cap entries of (x extent, tile width in cells, planes).
 int pb_level_tiles(const pb_level* lv, int* triples, int cap, int* n)
 {
     if (!lv || !n || (cap > 0 && !triples)) return PB_ERR_ARG;
@@ -748,9 +938,10 @@ int pb_level_tiles(const pb_level* lv, int* triples, int cap, int* n)
     int k = 0;
     for (int nx : classes) {
         if (k < cap) {
-            const std::pair<int, int> sh = tile_shape(lv, nx);
+            const int xv = lv->pair_ok && lv->tiled ? 2 : 1;
+            const std::pair<int, int> sh = tile_shape(lv, nx, xv);
             triples[3 * k] = nx;
-            triples[3 * k + 1] = sh.first;
+            triples[3 * k + 1] = xv * sh.first;
             triples[3 * k + 2] = sh.second;
         }
         k++;

@@ -176,3 +176,31 @@ def test_steps_on_a_non_tensor_layout_use_the_exchange(golden, pb):
         a2, b2 = b2, a2
     torch.cuda.synchronize()
     assert np.array_equal(_valid(lv, a.cpu().numpy()), _valid(lv, a2.cpu().numpy()))
+
+
+@pytest.mark.parametrize("case", ["odd_x_extents_13pt", "even_7pt"])
+def test_fused_steps_other_kernels_equal_the_exchange_loop(golden, pb, case):
+    """Fused steps on tensor tilings that the two-cells-per-thread kernel does not take (odd x
+    extents; a halo-1 stencil) run the one-cell ring kernel: bitwise the exchange + stencil loop."""
+    import torch
+    if case == "odd_x_extents_13pt":
+        widths, name = [[15, 17, 16], [16, 24], [20, 12, 16]], "laplacian13"
+    else:
+        widths, name = [[16, 24, 32], [24, 16], [48, 16, 32]], "laplacian"
+    boxes, L = W.amr_patches(widths)
+    lv = pb.Level([pb.Box(*b) for b in boxes], 2, pb.Box((0, 0, 0), [v - 1 for v in L]), (1, 1, 1))
+    c, o, m = table(golden[1], name)
+    S = pb.Stencil(c, o)
+    u = W.uniform_box((L[2], L[1], L[0]), 11)
+    a = torch.from_numpy(_slab_from_valid(lv, u, 0.0)).cuda()
+    b = torch.zeros_like(a)
+    a2, b2 = a.clone(), b.clone()
+    h = 1.0 / L[0]
+    lv.steps(S, pb.EPI_EULER, a, b, 3, scale=1.0 / (h * h), a=0.1 * h * h)
+    for _ in range(3):
+        lv.exchange(a2)
+        lv.stencil(S, pb.EPI_EULER, a2, b2, scale=1.0 / (h * h), a=0.1 * h * h)
+        a2, b2 = b2, a2
+    torch.cuda.synchronize()
+    pb.device_check()
+    assert np.array_equal(_valid(lv, a.cpu().numpy()), _valid(lv, a2.cpu().numpy()))

@@ -13,6 +13,7 @@ restriction/prolongation pair stalls at depth (reference CPU path: 0.48, 0.72, 0
   stencil: Stencil::apply 7-point FP64 on a 256^3 box (src 258^3), GB/s and fraction of HBM
   roofline: the dominant kernel, the finest-level Jacobi sweep (k_star_tma<Lap7, EpiRelax>)
   mixed : the same problem with FP32 V-cycles inside FP64 residual/correction/norm
+  mixed_384: FP64 vs mixed at 384^3, Poisson and Helmholtz with a per-cell alpha (exact coarsest solve)
   amr_level: 100 steps of exchange + 13-point Euler update over a 512-patch uneven level
   serving: a stream of Poisson/Helmholtz requests (edges 32..192) served by the batching engine vs
           plain FP64 multigrid one request at a time (saturated and at the 200/s arrival rate)
@@ -226,6 +227,53 @@ def run_amr_level(pb, torch, steps=100, reps=5, cpu=True, tune=True):
     return out
 
 
+def run_precision(pb, torch, n=384, levels=7, reps=3):
+    """Mixed precision at 384^3: the 8-mode Poisson problem (seed 1) and the Helmholtz variant
+    alpha u - beta L u = f with alpha ~ U[0.1, 1] per cell (seed 3), beta = 1; V(4,4), omega = 2/3,
+    coarsest 3^3 solved exactly, tol 1e-10. Each form: the FP64 solver and the mixed solver (FP32
+    cycles, FP64 residual/correction/norms), iterations, solves/s (device events), final relative
+    residual and the mixed solution's error against the FP64 one (the FP64 GPU solver performs the
+    CPU oracle's arithmetic bit for bit)."""
+    from proto_b200 import workloads as W
+    rho = torch.from_numpy(W.poisson_rho(n, seed=1).reshape(-1).copy()).cuda()
+    alpha = torch.from_numpy(W.helmholtz_alpha(n, seed=3).reshape(-1).copy()).cuda()
+    st = torch.cuda.current_stream()
+    out = {"workload": "%d^3 periodic, 7-point, V(%d,%d) omega=2/3, coarsest 3^3 exact, tol 1e-10; Poisson (8 sine "
+                       "modes, seed 1) and Helmholtz alpha~U[0.1,1] per cell (seed 3), beta=1" % (n, NU1, NU2)}
+    for form, name in ((pb.MG_POISSON, "poisson"), (pb.MG_HELMHOLTZ, "helmholtz")):
+        f = rho if form == pb.MG_POISSON else -rho   # Poisson solves L u = -f in the reference's sign
+        res = {}
+        sol = {}
+        for prec, pname in ((pb.MG_FP64, "fp64"), (pb.MG_MIXED, "mixed")):
+            mg = pb.Multigrid(pb.MGParams(n=n, levels=levels, nu1=NU1, nu2=NU2, nu_bottom=NU_BOTTOM, omega=OMEGA,
+                                          max_iter=MAX_ITER, tol=TOL, form=form, precision=prec,
+                                          bottom=pb.MG_BOTTOM_DIRECT))
+            if form == pb.MG_HELMHOLTZ:
+                mg.set_alpha(alpha)
+            phi = torch.zeros(n ** 3, dtype=torch.float64, device="cuda")
+            it, hist = mg.solve(f, phi)   # warm-up (graph capture)
+            ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+            for e0, e1 in ev:
+                phi.zero_()
+                e0.record(st)
+                it, hist = mg.solve(f, phi)
+                e1.record(st)
+            torch.cuda.synchronize()
+            ms = sorted(e0.elapsed_time(e1) for e0, e1 in ev)
+            res[pname] = {"iters": it, "solves_per_s": 1000.0 / ms[len(ms) // 2], "ms_per_solve": ms[len(ms) // 2],
+                          "final_rel_residual": hist[-1] / hist[0]}
+            sol[pname] = phi
+            del mg
+        d = (sol["mixed"] - sol["fp64"]).abs().max().item()
+        res["mixed"]["max_abs_err_vs_fp64"] = d
+        res["mixed"]["max_rel_err_vs_fp64"] = d / sol["fp64"].abs().max().item()
+        res["speedup_mixed_vs_fp64"] = res["mixed"]["solves_per_s"] / res["fp64"]["solves_per_s"]
+        out[name] = res
+        del sol
+    pb.device_check()
+    return out
+
+
 def profile_serving(pb, torch, count=16, n=96, steps=2):
     """A small in-flight batch for kernel captures: `count` Helmholtz solves of edge n submitted to
     one serving engine (public API, pinned host buffers), `steps` V-cycles for all of them."""
@@ -295,6 +343,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-precision", action="store_true", help="skip the 384^3 mixed-precision section")
     ap.add_argument("--profile-kernels", action="store_true",
                     help="run one 256^3 FP64 sweep, one FP32 sweep and one Stencil::apply, then exit (for ncu)")
     ap.add_argument("--profile-level", action="store_true",
@@ -483,6 +532,7 @@ def main():
     pb.device_check()
     value_m = world * args.steps / t_mx
     amr = None if world > 1 else run_amr_level(pb, torch)
+    precision = None if (world > 1 or args.no_precision) else run_precision(pb, torch)
     # the serving replay is a one-GPU measurement (replicas add nothing to it)
     serving = None if (args.no_serving or world > 1) else run_serving(pb, args.serve_requests)
     peak, peak_kind = measured_peaks()
@@ -524,6 +574,8 @@ def main():
                       "relax_fp32_us": t_rx32 * 1e6, "relax_fp32_gbs": 12 * 256 ** 3 / t_rx32 / 1e9,
                       "gpu_launches": (2 + itm * mgm.launches_per_cycle() + 1) * args.steps},
         }
+        if precision is not None:
+            line["mixed_384"] = precision
         if amr is not None:
             line["amr_level"] = amr
         if serving is not None:

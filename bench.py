@@ -14,6 +14,7 @@ restriction/prolongation pair stalls at depth (reference CPU path: 0.48, 0.72, 0
   roofline: the dominant kernel, the finest-level Jacobi sweep (k_star_tma<Lap7, EpiRelax>)
   mixed : the same problem with FP32 V-cycles inside FP64 residual/correction/norm
   mixed_384: FP64 vs mixed at 384^3, Poisson and Helmholtz with a per-cell alpha (exact coarsest solve)
+  fas   : the reference's FAS LevelMultigridSolver (4th-order flux-form Laplacian) at 64^3..256^3
   amr_level: 100 steps of exchange + 13-point Euler update over a 512-patch uneven level
   serving: a stream of Poisson/Helmholtz requests (edges 32..192) served by the batching engine vs
           plain FP64 multigrid one request at a time (saturated and at the 200/s arrival rate)
@@ -274,6 +275,57 @@ def run_precision(pb, torch, n=384, levels=7, reps=3):
     return out
 
 
+def run_fas(pb, torch, sizes=(64, 128, 256), reps=3, cpu=True):
+    """LevelMultigridSolver<BoxOp_Laplace> (FAS V(6,6), 4th-order flux-form Laplacian, 10 bottom
+    sweeps, lambda = 0.5/rho) on periodic n^3 boxes, coarsest 4^3, force = 8 sine modes (seed 1),
+    tol 1e-10: solves/s (device events) and iterations per size; beside it the reference's own
+    solver (oracle/_ref, one core) timed for one cycle at 64^3 (the reference example's size, boxes
+    of 16) and scaled by the GPU's iteration count there."""
+    import math
+    from proto_b200 import workloads as W
+    st = torch.cuda.current_stream()
+    out = {"workload": "FAS V(6,6) 4th-order flux-form Laplace, periodic, coarsest 4^3, 8 sine modes (seed 1), "
+                       "tol 1e-10"}
+    iters64 = None
+    for n in sizes:
+        levels = int(round(math.log2(n))) - 1
+        force = torch.from_numpy(-W.poisson_rho(n, seed=1).reshape(-1)).cuda()
+        mg = pb.FAS(n, levels)
+        phi = torch.zeros(n ** 3, dtype=torch.float64, device="cuda")
+        it, hist = mg.solve(force, phi, max_iter=20, tol=1e-10)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+        for e0, e1 in ev:
+            phi.zero_()
+            e0.record(st)
+            it, hist = mg.solve(force, phi, max_iter=20, tol=1e-10)
+            e1.record(st)
+        torch.cuda.synchronize()
+        ms = sorted(e0.elapsed_time(e1) for e0, e1 in ev)[reps // 2]
+        out["n%d" % n] = {"levels": levels, "iters": it, "ms_per_solve": ms, "solves_per_s": 1000.0 / ms,
+                          "final_rel_residual": hist[-1] / hist[0]}
+        if n == 64:
+            iters64 = it
+        del mg
+    pb.device_check()
+    if cpu and iters64:
+        try:
+            from oracle.oracle import Ref
+            if Ref.available():
+                R = Ref()
+                f = -W.poisson_rho(64, seed=1).reshape(-1).copy()
+                p = np.zeros(64 ** 3)
+                t0 = time.perf_counter()
+                R.mg_fas(64, 16, 5, 1, 0.0, f, p)
+                t = time.perf_counter() - t0
+                out["cpu_baseline_64"] = {"value": 1.0 / (t * iters64), "unit": "solves/s", "cores": 1,
+                                          "kind": "reference",
+                                          "sample": "1 FAS cycle + 2 residual norms at 64^3 (boxes of 16) with the "
+                                                    "reference's LevelMultigridSolver, scaled by %d cycles" % iters64}
+        except Exception as e:   # the baseline never hides the GPU result
+            out["cpu_baseline_64"] = {"error": str(e)}
+    return out
+
+
 def profile_serving(pb, torch, count=16, n=96, steps=2):
     """A small in-flight batch for kernel captures: `count` Helmholtz solves of edge n submitted to
     one serving engine (public API, pinned host buffers), `steps` V-cycles for all of them."""
@@ -344,12 +396,15 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-precision", action="store_true", help="skip the 384^3 mixed-precision section")
+    ap.add_argument("--no-fas", action="store_true", help="skip the FAS (LevelMultigridSolver) section")
     ap.add_argument("--profile-kernels", action="store_true",
                     help="run one 256^3 FP64 sweep, one FP32 sweep and one Stencil::apply, then exit (for ncu)")
     ap.add_argument("--profile-level", action="store_true",
                     help="run the AMR-level setup and 2 graph steps with default tiles, then exit (for ncu)")
     ap.add_argument("--profile-serving", action="store_true",
                     help="16 in-flight 96^3 Helmholtz solves, 2 V-cycles (small case for kernel captures)")
+    ap.add_argument("--profile-fas", action="store_true",
+                    help="FAS solves at 256^3 only (for kernel captures)")
     ap.add_argument("--serve-requests", type=int, default=2000)
     args = ap.parse_args()
 
@@ -369,6 +424,8 @@ def main():
         return run_amr_level(pb, torch, steps=2, reps=1, cpu=False, tune=False)
     if args.profile_serving:
         return profile_serving(pb, torch)
+    if args.profile_fas:
+        return run_fas(pb, torch, sizes=(256,), reps=1, cpu=False)
     dist = None
     if world > 1:
         import torch.distributed as dist
@@ -533,6 +590,7 @@ def main():
     value_m = world * args.steps / t_mx
     amr = None if world > 1 else run_amr_level(pb, torch)
     precision = None if (world > 1 or args.no_precision) else run_precision(pb, torch)
+    fas = None if (world > 1 or args.no_fas) else run_fas(pb, torch, cpu=not args.no_cpu_baseline)
     # the serving replay is a one-GPU measurement (replicas add nothing to it)
     serving = None if (args.no_serving or world > 1) else run_serving(pb, args.serve_requests)
     peak, peak_kind = measured_peaks()
@@ -576,6 +634,8 @@ def main():
         }
         if precision is not None:
             line["mixed_384"] = precision
+        if fas is not None:
+            line["fas"] = fas
         if amr is not None:
             line["amr_level"] = amr
         if serving is not None:

@@ -99,6 +99,187 @@ __global__ void __launch_bounds__(256) k_fas_relax(const double* __restrict__ u,
     }
 }
 
+// the ghost cells (width 2) that are periodic images of valid cell (x, y, z), the cell itself excluded
+__device__ __noinline__ void fas_images(double* u, int n, int x, int y, int z, double v)
+{
+    const int S = n + 2 * kFasGhost;
+    for (int kz = -2; kz <= 2; kz++) {
+        const int zz = z + kz * n;
+        if (zz < -kFasGhost || zz >= n + kFasGhost) continue;
+        for (int ky = -2; ky <= 2; ky++) {
+            const int yy = y + ky * n;
+            if (yy < -kFasGhost || yy >= n + kFasGhost) continue;
+            for (int kx = -2; kx <= 2; kx++) {
+                const int xx = x + kx * n;
+                if (xx < -kFasGhost || xx >= n + kFasGhost || (kx | ky | kz) == 0) continue;
+                u[fas_index(S, xx, yy, zz)] = v;
+            }
+        }
+    }
+}
+
+// the same for edges n >= 4, where a cell has at most one image per axis (7 in all, near a corner)
+__device__ __noinline__ void fas_images_n4(double* u, int n, int x, int y, int z, double v)
+{
+    const int S = n + 2 * kFasGhost;
+    const int ix = x < 2 ? n : (x >= n - 2 ? -n : 0);
+    const int iy = y < 2 ? n : (y >= n - 2 ? -n : 0);
+    const int iz = z < 2 ? n : (z >= n - 2 ? -n : 0);
+#pragma unroll
+    for (int c = 1; c < 8; c++) {
+        const int dx = (c & 1) ? ix : 0, dy = (c & 2) ? iy : 0, dz = (c & 4) ? iz : 0;
+        if (((c & 1) && !ix) || ((c & 2) && !iy) || ((c & 4) && !iz)) continue;
+        u[fas_index(S, x + dx, y + dy, z + dz)] = v;
+    }
+}
+
+// one face flux of DiffCellToFace(d, Lo, 4): the four cells below-below .. above of the face
+__device__ __forceinline__ double fas_flux(const FasCoef& k, double a, double b, double c, double d)
+{
+    double f = 0.0;
+    f = dadd(f, dmul(k.g[0], a));
+    f = dadd(f, dmul(k.g[1], b));
+    f = dadd(f, dmul(k.g[2], c));
+    return dadd(f, dmul(k.g[3], d));
+}
+
+// The Jacobi sweep of k_fas_relax on large levels, two adjacent x cells per thread: a CTA owns a
+// (2 kFasTX) x kFasTY column of cells and a chunk of zd planes; per plane it stages the column's
+// tile with its 2-cell x/y halo (ghost cells are valid: every writer stores the periodic images)
+// into a ring of shared-memory planes with 16-byte cp.async copies, kFasLead planes ahead; z
+// neighbours come from a register window fed from the ring's centre column. A face flux shared by
+// two cells is computed once (the x face between the pair; the z face between consecutive planes):
+// it is the same four products summed in the same order either way, so every cell's value is
+// bitwise fas_op's. Periodic images are written for cells within 2 of a face.
+constexpr int kFasTX = 16, kFasTY = 16, kFasThreads = kFasTX * kFasTY;
+constexpr int kFasBX = 2 * kFasTX + 4, kFasBY = kFasTY + 4, kFasPlane = kFasBX * kFasBY;
+constexpr int kFasLead = 2 + 3, kFasRing = kFasLead + 1;
+
+__global__ void __launch_bounds__(kFasThreads) k_fas_relax_pair(const double* __restrict__ u, double* out,
+                                                                const double* __restrict__ f, int n, int zd,
+                                                                FasCoef k, double neg_lambda)
+{
+    constexpr int R = 2, W = 5, L = kFasLead, Q = kFasRing, PM = kFasPlane, PX = kFasBX / 2;
+    __shared__ __align__(16) double ring[Q * PM];
+    const int S = n + 2 * kFasGhost;
+    const long long S2 = (long long)S * S;
+    const int x0 = blockIdx.x * 2 * kFasTX, y0 = blockIdx.y * kFasTY, z0 = blockIdx.z * zd;
+    const int z1 = min(z0 + zd, n);
+    const int lx = threadIdx.x % kFasTX, ly = threadIdx.x / kFasTX;
+    const int x = x0 + 2 * lx, y = y0 + ly;
+    const bool act = x < n && y < n;
+    constexpr int kMaxLoads = (PX * kFasBY + kFasThreads - 1) / kFasThreads;
+    const double* lp[kMaxLoads];
+    bool lv_[kMaxLoads];
+#pragma unroll
+    for (int q = 0; q < kMaxLoads; q++) {
+        const int i = threadIdx.x + q * kFasThreads;
+        const int hx = i % PX, hy = i / PX;
+        const int xx = x0 - R + 2 * hx, yy = y0 - R + hy;
+        const bool xo = hx < 1 || hx > kFasTX, yo = hy < R || hy >= kFasTY + R;
+        lv_[q] = i < PX * kFasBY && !(xo && yo) && xx < n + R && yy < n + R;
+        lp[q] = u + (xx + kFasGhost) + (long long)S * (yy + kFasGhost) + S2 * (z0 + kFasGhost);
+    }
+    const uint32_t ring0 = smem_u32(ring) + 16u * threadIdx.x;
+    auto stage = [&](int zz, int slot) {
+        if (zz < z1) {
+#pragma unroll
+            for (int q = 0; q < kMaxLoads; q++)
+                if (lv_[q]) {
+                    cp_async16(ring0 + 8u * (slot * PM + 2 * q * kFasThreads), lp[q]);
+                    lp[q] += S2;
+                }
+        }
+        cp_async_commit();
+    };
+    const double* col = u + fas_index(S, act ? x : 0, act ? y : 0, 0);   // (x, y, z = 0), pair-aligned
+    auto zcol = [&](int zz) -> double2 { return __ldg(reinterpret_cast<const double2*>(col + S2 * zz)); };
+#pragma unroll
+    for (int q = 0; q < L; q++) stage(z0 + q, q);
+    double w0[W], w1[W];
+    if (act) {
+#pragma unroll
+        for (int q = 0; q < 2 * R; q++) {
+            const double2 v = zcol(z0 - R + q);
+            w0[q] = v.x;
+            w1[q] = v.y;
+        }
+    }
+    double fz0 = 0.0, fz1 = 0.0;   // lower z-face flux of the current plane (carried from the one below)
+    if (act) {
+        fz0 = fas_flux(k, w0[0], w0[1], w0[2], w0[3]);
+        fz1 = fas_flux(k, w1[0], w1[1], w1[2], w1[3]);
+    }
+    const int sc = (ly + R) * kFasBX + (2 * lx + R);
+    const double* fp = f + (act ? x + (long long)n * (y + (long long)n * z0) : 0);
+    double* op = out + fas_index(S, act ? x : 0, act ? y : 0, z0);
+    const bool edge_xy = x < 2 || x + 1 >= n - 2 || y < 2 || y >= n - 2;
+    int qz = 0;
+    for (int z = z0; z < z1; z++) {
+        double2 fv = make_double2(0.0, 0.0);
+        if (act) fv = __ldg(reinterpret_cast<const double2*>(fp));
+        cp_async_wait<L - R - 1>();
+        __syncthreads();
+        const int qn = qz == 0 ? Q - 1 : qz - 1;
+        stage(z + L, qn);
+        if (act) {
+            int qr = qz + R;
+            if (qr >= Q) qr -= Q;
+            const double2 cn = z + R < z1 ? *reinterpret_cast<const double2*>(ring + qr * PM + sc) : zcol(z + R);
+            w0[2 * R] = cn.x;
+            w1[2 * R] = cn.y;
+            const double* pl = ring + qz * PM + sc;
+            const double2 xm = *reinterpret_cast<const double2*>(pl - 2);
+            const double2 xc = *reinterpret_cast<const double2*>(pl);
+            const double2 xq = *reinterpret_cast<const double2*>(pl + 2);
+            const double2 ym2 = *reinterpret_cast<const double2*>(pl - 2 * kFasBX);
+            const double2 ym1 = *reinterpret_cast<const double2*>(pl - kFasBX);
+            const double2 yp1 = *reinterpret_cast<const double2*>(pl + kFasBX);
+            const double2 yp2 = *reinterpret_cast<const double2*>(pl + 2 * kFasBX);
+            // x faces: below cell 0, between the pair, above cell 1
+            const double fxm = fas_flux(k, xm.x, xm.y, xc.x, xc.y);
+            const double fxc = fas_flux(k, xm.y, xc.x, xc.y, xq.x);
+            const double fxp = fas_flux(k, xc.x, xc.y, xq.x, xq.y);
+            const double gz0 = fas_flux(k, w0[1], w0[2], w0[3], w0[4]);
+            const double gz1 = fas_flux(k, w1[1], w1[2], w1[3], w1[4]);
+            double d0 = 0.0, d1 = 0.0;
+            d0 = dadd(d0, dmul(k.cp, fxc));
+            d0 = dadd(d0, dmul(k.c0, fxm));
+            d0 = dadd(d0, dmul(k.cp, fas_flux(k, ym1.x, xc.x, yp1.x, yp2.x)));
+            d0 = dadd(d0, dmul(k.c0, fas_flux(k, ym2.x, ym1.x, xc.x, yp1.x)));
+            d0 = dadd(d0, dmul(k.cp, gz0));
+            d0 = dadd(d0, dmul(k.c0, fz0));
+            d1 = dadd(d1, dmul(k.cp, fxp));
+            d1 = dadd(d1, dmul(k.c0, fxc));
+            d1 = dadd(d1, dmul(k.cp, fas_flux(k, ym1.y, xc.y, yp1.y, yp2.y)));
+            d1 = dadd(d1, dmul(k.c0, fas_flux(k, ym2.y, ym1.y, xc.y, yp1.y)));
+            d1 = dadd(d1, dmul(k.cp, gz1));
+            d1 = dadd(d1, dmul(k.c0, fz1));
+            fz0 = gz0;
+            fz1 = gz1;
+            const double r0 = dadd(dmul(dadd(0.0, d0), -1.0), fv.x);
+            const double r1 = dadd(dmul(dadd(0.0, d1), -1.0), fv.y);
+            double2 v;
+            v.x = dadd(xc.x, dmul(neg_lambda, r0));
+            v.y = dadd(xc.y, dmul(neg_lambda, r1));
+            *reinterpret_cast<double2*>(op) = v;
+            if (edge_xy || z < 2 || z >= n - 2) {
+                fas_images_n4(out, n, x, y, z, v.x);
+                fas_images_n4(out, n, x + 1, y, z, v.y);
+            }
+#pragma unroll
+            for (int q = 0; q < 2 * R; q++) {
+                w0[q] = w0[q + 1];
+                w1[q] = w1[q + 1];
+            }
+        }
+        op += S2;
+        fp += (long long)n * n;
+        qz = qz == Q - 1 ? 0 : qz + 1;
+    }
+    cp_async_wait<0>();
+}
+
 // coarse state = AvgDown(u) (with images) and its copy c0
 __global__ void __launch_bounds__(256) k_fas_average(const double* __restrict__ u, double* uc, double* c0, int nf)
 {
@@ -238,16 +419,37 @@ struct pb_fas {
     double* d_res = nullptr;
     double* h_res = nullptr;
     int num_pre = 6, num_post = 6, num_bottom = 10;
+    // the V-cycle plus the residual norm, captured once per parity of the finest level's buffer
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    int graph_cur[2] = {0, 0};           // the finest level's buffer after the captured cycle
+    cudaStream_t graph_stream = nullptr;
 };
 
 using namespace pb;
+
+// levels of edge >= kFasPairMin (even) sweep with the staged two-cells-per-thread kernel; smaller
+// ones have too few (x, y) columns to fill the GPU with z-streaming CTAs
+constexpr int kFasPairMin = 128;
 
 static int fas_relax(pb_fas* m, int l, int sweeps, cudaStream_t st)
 {
     FasLevel& L = m->lv[l];
     const long long n3 = (long long)L.n * L.n * L.n;
+    const bool pair = L.n >= kFasPairMin && L.n % 2 == 0;
+    dim3 grid;
+    int zd = 32;
+    if (pair) {
+        const int nbx = (L.n + 2 * kFasTX - 1) / (2 * kFasTX), nby = (L.n + kFasTY - 1) / kFasTY;
+        // z chunks shallow enough for about six waves of the 3 CTAs an SM holds (tail under ~15 %)
+        const long long want = 18LL * cached_sm_count();
+        while (zd > 4 && (long long)nbx * nby * ((L.n + zd - 1) / zd) < want) zd /= 2;
+        grid = dim3(nbx, nby, (L.n + zd - 1) / zd);
+    }
     for (int s = 0; s < sweeps; s++) {
-        k_fas_relax<<<grid_for(n3, 256), 256, 0, st>>>(L.u[L.cur], L.u[1 - L.cur], L.f, L.n, L.k, L.neg_lambda);
+        if (pair)
+            k_fas_relax_pair<<<grid, kFasThreads, 0, st>>>(L.u[L.cur], L.u[1 - L.cur], L.f, L.n, zd, L.k, L.neg_lambda);
+        else
+            k_fas_relax<<<grid_for(n3, 256), 256, 0, st>>>(L.u[L.cur], L.u[1 - L.cur], L.f, L.n, L.k, L.neg_lambda);
         PB_LAUNCH_CHECK();
         L.cur = 1 - L.cur;
     }
@@ -277,16 +479,30 @@ static int fas_vcycle(pb_fas* m, int l, cudaStream_t st)
     return fas_relax(m, l, m->num_post, st);
 }
 
-static int fas_resnorm(pb_fas* m, cudaStream_t st, double* out)
+// max |op(u) + f| on the finest level into the pinned host word (stream ordered, no wait)
+static int fas_enqueue_resnorm(pb_fas* m, cudaStream_t st)
 {
     FasLevel& T = m->lv.back();
     PB_CUDA(cudaMemsetAsync(m->d_res, 0, sizeof(double), st));
     k_fas_resnorm<<<grid_for((long long)T.n * T.n * T.n, 256), 256, 0, st>>>(T.u[T.cur], T.f, T.n, T.k, m->d_res);
     PB_LAUNCH_CHECK();
     PB_CUDA(cudaMemcpyAsync(m->h_res, m->d_res, sizeof(double), cudaMemcpyDeviceToHost, st));
+    return PB_OK;
+}
+
+static int fas_resnorm(pb_fas* m, cudaStream_t st, double* out)
+{
+    const int e = fas_enqueue_resnorm(m, st);
+    if (e != PB_OK) return e;
     PB_CUDA(cudaStreamSynchronize(st));
     *out = *m->h_res;
     return PB_OK;
+}
+
+static int fas_cycle_and_norm(pb_fas* m, cudaStream_t st)
+{
+    const int e = fas_vcycle(m, (int)m->lv.size() - 1, st);
+    return e != PB_OK ? e : fas_enqueue_resnorm(m, st);
 }
 
 static void fas_free(pb_fas* m)
@@ -299,6 +515,9 @@ static void fas_free(pb_fas* m)
     }
     cudaFree(m->d_res);
     cudaFreeHost(m->h_res);
+    for (int p = 0; p < 2; p++)
+        if (m->graph[p]) cudaGraphExecDestroy(m->graph[p]);
+    if (m->graph_stream) cudaStreamDestroy(m->graph_stream);
     delete m;
 }
 
@@ -357,8 +576,28 @@ int pb_fas_solve(pb_fas* m, const double* force, double* phi, int max_iter, doub
     if (hist) hist[0] = r0;
     int it = 0;
     while (it < max_iter) {
-        if ((e = fas_vcycle(m, (int)m->lv.size() - 1, st)) != PB_OK) return e;
-        if ((e = fas_resnorm(m, st, &r)) != PB_OK) return e;
+        const int par = T.cur;
+        if (!m->graph[par]) {
+            if (!m->graph_stream) PB_CUDA(cudaStreamCreateWithFlags(&m->graph_stream, cudaStreamNonBlocking));
+            cudaGraph_t g;
+            PB_CUDA(cudaStreamBeginCapture(m->graph_stream, cudaStreamCaptureModeThreadLocal));
+            e = fas_cycle_and_norm(m, m->graph_stream);
+            cudaError_t ce = cudaStreamEndCapture(m->graph_stream, &g);
+            if (e != PB_OK) {
+                if (ce == cudaSuccess) cudaGraphDestroy(g);
+                return e;
+            }
+            if (ce != cudaSuccess) { set_cuda_error(ce); return PB_ERR_CUDA; }
+            ce = cudaGraphInstantiate(&m->graph[par], g, 0);
+            cudaGraphDestroy(g);
+            if (ce != cudaSuccess) { m->graph[par] = nullptr; set_cuda_error(ce); return PB_ERR_CUDA; }
+            m->graph_cur[par] = T.cur;   // capture recorded the buffer flips without running them
+            T.cur = par;
+        }
+        PB_CUDA(cudaGraphLaunch(m->graph[par], st));
+        T.cur = m->graph_cur[par];
+        PB_CUDA(cudaStreamSynchronize(st));
+        r = *m->h_res;
         ++it;
         if (hist) hist[it] = r;
         if (r < tol * r0) break;

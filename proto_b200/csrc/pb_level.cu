@@ -189,13 +189,6 @@ constexpr int kLevelPrefetch = 3;                    // planes in flight beyond 
 __host__ __device__ constexpr int level_lead(int R) { return R + kLevelPrefetch; }
 __host__ __device__ constexpr int level_ring(int R) { return level_lead(R) + 1; }
 
-__device__ __forceinline__ void cp_async8(uint32_t dst, const void* src)
-{
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 template <class S>
 __global__ void __launch_bounds__(kLevelThreads) k_level_star_tiled(const double* __restrict__ u, double* out,
@@ -320,10 +313,6 @@ __global__ void __launch_bounds__(kLevelThreads) k_level_star_tiled(const double
 // per cell, so bitwise the one-cell paths.
 constexpr int kLevelPairPlaneMax = (64 + 4) * (8 + 4);   // (2tx+4)(ty+4) <= 816 for tx in {8, 16, 32}
 
-__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src)
-{
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
-}
 
 template <class S>
 __global__ void __launch_bounds__(kLevelThreads) k_level_star_pair(const double* __restrict__ u, double* out,

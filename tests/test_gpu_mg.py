@@ -188,3 +188,19 @@ def test_fas_against_port_64(pb, port):
     n2, h2 = port.mg_fas(N, levels, 6, 1e-10, -rho, p2)
     assert it == n2 and hist == list(h2)
     assert np.array_equal(phi.cpu().numpy(), p2)
+
+
+def test_fas_against_port_80_partial_tiles(pb, port):
+    """80^3 (staged two-cell sweeps with a partial x tile at the top level; 40^3 and below on the
+    one-cell kernel): residual history and solution bitwise the C restatement's."""
+    import torch
+    N, levels = 80, 4
+    rho = W.poisson_rho(N, seed=2).reshape(-1).copy()
+    mg = pb.FAS(N, levels)
+    phi = torch.zeros(N ** 3, dtype=torch.float64, device="cuda")
+    it, hist = mg.solve(torch.from_numpy(-rho).cuda(), phi, max_iter=3, tol=1e-10)
+    pb.device_check()
+    p2 = np.zeros(N ** 3)
+    n2, h2 = port.mg_fas(N, levels, 3, 1e-10, -rho, p2)
+    assert it == n2 and hist == list(h2)
+    assert np.array_equal(phi.cpu().numpy(), p2)

@@ -199,12 +199,26 @@ __global__ void __launch_bounds__(kSvUnit) k_sv_walk(const SvItem* __restrict__ 
     const long long total = hdr->total;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (long long w0 = (long long)blockIdx.x * kSvRows; w0 < total; w0 += (long long)gridDim.x * kSvRows) {
-        const SvItem& it = items[sv_find(unit0, count, w0)];
-        const int unit = (int)(w0 - it.unit0) + warp;
+        const SvItem* itp = items + sv_find(unit0, count, w0);
+        const int unit = (int)(w0 - itp->unit0) + warp;
+        const int units = itp->units;
         double m = 0.0;
-        if (unit < it.units) {
-            const int n = it.k.n;
-            const int zd = it.zd;
+        if (unit < units) {
+            // the item's fields, once, into registers
+            const RelaxCoef<float> k = itp->k;
+            const int n = k.n;
+            const int zd = itp->zd;
+            float* const in32 = itp->in;
+            float* const out32 = itp->out;
+            const float* const rhs = itp->rhs;
+            double* const u64 = itp->u64;
+            const double* const f64 = itp->f64;
+            const int sxd = itp->sxd;
+            const float alpha = itp->alpha;
+            const double alpha64 = itp->alpha64, beta64 = itp->beta64;
+            Coefs<V> cf;
+            if constexpr (OP == SV_K1) cf = itp->c64;
+            else cf = itp->c;
             int XC, ZC;
             sv_walk_units(n, zd, XC, ZC);
             const int y = unit % n, xc = (unit / n) % XC, zc = unit / (n * XC);
@@ -216,36 +230,52 @@ __global__ void __launch_bounds__(kSvUnit) k_sv_walk(const SvItem* __restrict__ 
             const V* src;
             int sx;
             if constexpr (OP == SV_K1) {
-                src = reinterpret_cast<const V*>(it.u64);
-                sx = it.sxd;
+                src = reinterpret_cast<const V*>(u64);
+                sx = sxd;
             } else {
-                src = reinterpret_cast<const V*>(it.in);
-                sx = it.k.sx;
+                src = reinterpret_cast<const V*>(in32);
+                sx = k.sx;
             }
-            const int Sy = sx, Sz = sx * (n + 2);
+            const int Sy = sx, Sz = sx * (n + 2), nn = n * n;
             const V* c = src + (long long)grown_index<V>(n, sx, act ? x : 0, y, z0);   // (x, y, z0)
-            Coefs<V> cf;
-            if constexpr (OP == SV_K1) cf = it.c64;
-            else cf = it.c;
             const int ey = edge_code(y, n), ex = act ? edge_code(x, n) : 0;
+            int i = (act ? x : 0) + n * (y + n * z0);
+            // plane z's loads are issued one plane ahead: +z, +-y, the chunk-end x neighbours and the
+            // pointwise inputs (rhs; f for the residual pass; u64 for the update)
             V zm = act ? c[-Sz] : V(0), z_ = act ? c[0] : V(0);
+            V zp_n = V(0), ym_n = V(0), yp_n = V(0), xme_n = V(0), xpe_n = V(0);
+            float r_n = 0.f;
+            double d_n = 0.0;
+            auto fetch = [&](const V* cc, int ii, int zz) {
+                if (!act) return;
+                zp_n = cc[Sz];
+                ym_n = cc[-Sy];
+                yp_n = cc[Sy];
+                if (lane == 0) xme_n = cc[-1];
+                if (last) xpe_n = cc[1];
+                if constexpr (OP == SV_K1) d_n = f64[ii];
+                else r_n = rhs[ii];
+                if constexpr (OP == SV_UPDATE) d_n = u64[grown_index<double>(n, sxd, x, y, zz)];
+            };
+            fetch(c, i, z0);
             for (int z = z0; z < z1; z++) {
-                const V zp = act ? c[Sz] : V(0);
+                const V zp = zp_n, ym = ym_n, yp = yp_n, xme = xme_n, xpe = xpe_n;
+                const float rr = r_n;
+                const double dd = d_n;
+                if (z + 1 < z1) fetch(c + Sz, i + nn, z + 1);
                 // neighbours along x from the lanes beside (the chunk's end lanes load them)
                 V xm = __shfl_up_sync(0xffffffffu, z_, 1);
                 V xp = __shfl_down_sync(0xffffffffu, z_, 1);
-                if (act && lane == 0) xm = c[-1];
-                if (last) xp = c[1];
+                if (lane == 0) xm = xme;
+                if (last) xp = xpe;
                 if (act) {
-                    const V ym = c[-Sy], yp = c[Sy];
-                    const int i = x + n * (y + n * z);
                     const int ez = edge_code(z, n);
                     // Laplacian insertion order: 0, +x, -x, +y, -y, +z, -z
                     if constexpr (OP == SV_K1) {
                         double res;
                         float al = 0.f;
-                        if (!it.k.helm) {
-                            res = dadd(0.0, it.f64[i]);
+                        if (!k.helm) {
+                            res = dadd(0.0, dd);
                             res = dadd(res, dmul(cf.c[0], (double)z_));
                             res = dadd(res, dmul(cf.c[1], (double)xp));
                             res = dadd(res, dmul(cf.c[2], (double)xm));
@@ -262,14 +292,14 @@ __global__ void __launch_bounds__(kSvUnit) k_sv_walk(const SvItem* __restrict__ 
                             lp = dadd(lp, dmul(cf.c[4], (double)ym));
                             lp = dadd(lp, dmul(cf.c[5], (double)zp));
                             lp = dadd(lp, dmul(cf.c[6], (double)zm));
-                            res = dsub(it.f64[i], dsub(dmul(it.alpha64, (double)z_), dmul(it.beta64, lp)));
-                            al = __double2float_rn(it.alpha64);
+                            res = dsub(dd, dsub(dmul(alpha64, (double)z_), dmul(beta64, lp)));
+                            al = __double2float_rn(alpha64);
                         }
                         m = upd_abs(m, res);
                         const float r32 = __double2float_rn(res);
-                        it.out[i] = r32;
-                        float* q = it.in + grown_index<float>(n, it.k.sx, x, y, z);
-                        store_with_images(it.in, n, it.k.sx, q, ex, ey, ez, relax_value(it.k, 0.f, 0.f, r32, al));
+                        out32[i] = r32;
+                        float* q = in32 + grown_index<float>(n, k.sx, x, y, z);
+                        store_with_images(in32, n, k.sx, q, ex, ey, ez, relax_value(k, 0.f, 0.f, r32, al));
                     } else {
                         float acc = 0.f;
                         acc = dadd(acc, dmul(cf.c[0], (float)z_));
@@ -279,19 +309,20 @@ __global__ void __launch_bounds__(kSvUnit) k_sv_walk(const SvItem* __restrict__ 
                         acc = dadd(acc, dmul(cf.c[4], (float)ym));
                         acc = dadd(acc, dmul(cf.c[5], (float)zp));
                         acc = dadd(acc, dmul(cf.c[6], (float)zm));
-                        const float v = relax_value(it.k, acc, (float)z_, it.rhs[i], it.alpha);
+                        const float v = relax_value(k, acc, (float)z_, rr, alpha);
                         if constexpr (OP == SV_RELAX) {
-                            const long long g = (c - src) + 0;
-                            store_with_images(it.out, n, sx, it.out + g, ex, ey, ez, v);
+                            const long long g = c - src;
+                            store_with_images(out32, n, sx, out32 + g, ex, ey, ez, v);
                         } else {
-                            double* q = it.u64 + grown_index<double>(n, it.sxd, x, y, z);
-                            store_with_images(it.u64, n, it.sxd, q, ex, ey, ez, dadd(*q, (double)v));
+                            double* q = u64 + grown_index<double>(n, sxd, x, y, z);
+                            store_with_images(u64, n, sxd, q, ex, ey, ez, dadd(dd, (double)v));
                         }
                     }
                 }
                 zm = z_;
                 z_ = zp;
                 c += Sz;
+                i += nn;
             }
         }
         if constexpr (OP == SV_K1) {
@@ -299,7 +330,7 @@ __global__ void __launch_bounds__(kSvUnit) k_sv_walk(const SvItem* __restrict__ 
                 const double w = __shfl_down_sync(0xffffffffu, m, o);
                 m = (m < w) ? w : m;
             }
-            if (lane == 0 && m > 0.0 && unit < it.units) atomic_max_nonneg(norms + it.slot, m);
+            if (lane == 0 && m > 0.0 && unit < units) atomic_max_nonneg(norms + itp->slot, m);
         }
     }
 }

@@ -217,8 +217,11 @@ RelaxCoef<float> level_coef(const pb_serve_params& p, const pb_serve_request& q,
     return k;
 }
 
-// units of the column-walk phases: rows x 32-wide x chunks x zd-deep z chunks
-long long walk_units(int e, int zd) { return (long long)e * ((e + 31) / 32) * ((e + zd - 1) / zd); }
+// units of the staged phases: 32 x 8 tiles x zd-deep z chunks, one CTA each
+long long ring_units(int e, int zd)
+{
+    return (long long)((e + kSvTX - 1) / kSvTX) * ((e + kSvTY - 1) / kSvTY) * ((e + zd - 1) / zd);
+}
 
 double level_hsqinv(int n, int d)
 {
@@ -269,24 +272,28 @@ std::vector<PhaseSlot> phase_plan(const pb_serve_params& p, int D)
 // buffer index holding a level's current solution just before each phase, following the
 // single-solve solver's ping-pong: depth 0 starts at 1 (the residual pass wrote phi[1]), deeper
 // levels start from zero (their first sweep writes phi[1])
-// Lays a phase's items out in unit order. Column-walk phases take the deepest z chunk (kSvZ, 8, 4
-// or 2 planes) that still gives every warp of the persistent grid a unit: deep chunks reuse more
-// z planes from registers, shallow ones keep a small batch from leaving most SMs idle.
-long long layout_items(std::vector<SvItem>& items, bool walk, long long warps)
+// Lays a phase's items out in unit order. Staged phases (a CTA per unit) take the deepest z chunk
+// (32, 16, 8 or 4 planes) that still gives every CTA of the persistent grid a unit: deep chunks
+// amortise the ring's fill, shallow ones keep a small batch from leaving most SMs idle. Row phases
+// (a warp per row) round each item to whole CTAs.
+long long layout_items(std::vector<SvItem>& items, bool staged, long long ctas)
 {
-    if (walk) {
-        int zd = kSvZ;
+    long long total = 0;
+    if (staged) {
+        int zd = 32;
         for (;; zd /= 2) {
             long long sum = 0;
-            for (const SvItem& it : items) sum += walk_units(it.k.n, zd);
-            if (sum >= warps || zd <= 2) break;
+            for (const SvItem& it : items) sum += ring_units(it.k.n, zd);
+            if (sum >= ctas || zd <= 4) break;
         }
         for (SvItem& it : items) {
             it.zd = zd;
-            it.units = (int)walk_units(it.k.n, zd);
+            it.units = (int)ring_units(it.k.n, zd);
+            it.unit0 = total;
+            total += it.units;
         }
+        return total;
     }
-    long long total = 0;
     for (SvItem& it : items) {
         it.unit0 = total;
         total += ((long long)it.units + kSvRows - 1) / kSvRows * kSvRows;
@@ -294,7 +301,7 @@ long long layout_items(std::vector<SvItem>& items, bool walk, long long warps)
     return total;
 }
 
-bool is_walk(int op) { return op == SV_RELAX || op == SV_UPDATE || op == SV_K1; }
+bool is_staged(int op) { return op == SV_RELAX || op == SV_UPDATE || op == SV_K1; }
 
 } // namespace
 
@@ -317,7 +324,7 @@ static int build_lists(pb_serve* sv)
         sv->h_unit0.assign((size_t)sv->max_phases * cap, 0);
     }
     sv->h_hdr.assign(sv->max_phases, SvPhaseHeader{0, 0});
-    const long long warps = (long long)sv->grid * kSvRows;
+    const long long ctas = sv->grid;
     // per solve: the buffer index of each level's current solution as the plan advances
     std::vector<std::vector<int>> cur(act.size());
     for (size_t a = 0; a < act.size(); a++) {
@@ -393,7 +400,7 @@ static int build_lists(pb_serve* sv)
             }
             items.push_back(it);
         }
-        const long long total = layout_items(items, is_walk(ps.op), warps);
+        const long long total = layout_items(items, is_staged(ps.op), ctas);
         std::copy(items.begin(), items.end(), sv->h_items.begin() + ph * cap);
         for (size_t k = 0; k < items.size(); k++) sv->h_unit0[ph * cap + k] = items[k].unit0;
         sv->h_hdr[ph] = SvPhaseHeader{(long long)items.size(), total};
@@ -423,7 +430,7 @@ static int build_lists(pb_serve* sv)
             it.c64 = lap7_coefs<double>(helm ? hs : -hs);
             items.push_back(it);
         }
-        const long long total = layout_items(items, true, warps);
+        const long long total = layout_items(items, true, ctas);
         std::copy(items.begin(), items.end(), sv->h_items.begin() + (size_t)ph * cap);
         for (size_t k = 0; k < items.size(); k++) sv->h_unit0[(size_t)ph * cap + k] = items[k].unit0;
         sv->h_hdr[ph] = SvPhaseHeader{(long long)items.size(), total};
@@ -493,12 +500,12 @@ static int launch_phase(pb_serve* sv, int slot, int op, double* norms, cudaStrea
     const long long* u0 = sv->d_unit0 + (size_t)slot * sv->p.max_active;
     const SvPhaseHeader* hdr = sv->d_hdr + slot;
     switch (op) {
-    case SV_RELAX: k_sv_walk<SV_RELAX, float><<<sv->grid, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
+    case SV_RELAX: k_sv_ring<SV_RELAX, float><<<sv->grid, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
     case SV_RELAX_FIRST: k_sv_phase<SV_RELAX_FIRST><<<sv->grid, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
     case SV_RESTRICT: k_sv_phase<SV_RESTRICT><<<sv->grid, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
     case SV_PROLONG: k_sv_phase<SV_PROLONG><<<sv->grid, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
-    case SV_K1: k_sv_walk<SV_K1, double><<<sv->grid, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
-    case SV_UPDATE: k_sv_walk<SV_UPDATE, float><<<sv->grid, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
+    case SV_K1: k_sv_ring<SV_K1, double><<<sv->grid, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
+    case SV_UPDATE: k_sv_ring<SV_UPDATE, float><<<sv->grid, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
     default: return PB_ERR_ARG;
     }
     PB_LAUNCH_CHECK();

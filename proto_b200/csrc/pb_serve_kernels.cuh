@@ -35,7 +35,7 @@ struct SvItem {
     int sxc;               // prolong: coarse pitch
     int sxd;               // K1 / update: pitch of u64
     int slot;              // solve slot (norms)
-    int zd;                // column-walk phases: z planes per unit (chosen per phase)
+    int zd;                // staged phases: z planes per unit (chosen per phase)
     int units;             // rows of this item
     long long unit0;       // first row (multiple of kSvRows)
 };
@@ -177,160 +177,174 @@ __global__ void __launch_bounds__(kSvUnit) k_sv_phase(const SvItem* __restrict__
     }
 }
 
-// The stencil phases (sweep, sweep + FP64 update, FP64 residual pass) as warp column walks: a unit
-// is (row y, 32-wide x chunk, z chunk of kSvZ planes); a warp's lanes take consecutive x and walk
-// z with a register window of the 7-point stencil's z taps; +-x come from neighbouring lanes
-// (shuffles; the chunk's end lanes load the cell beyond, a ghost image at the box faces), +-y are
-// direct loads. Terms are summed in the Laplacian's insertion order, so results are bitwise the
-// row kernel's.
-constexpr int kSvZ = 16;   // deepest z chunk (a phase with few units takes shallower ones)
+// The stencil phases (sweep, FP64 residual pass, last sweep + FP64 correction) with a CTA per
+// unit = (item, 32 x 8 tile of a level, chunk of zd planes): per plane the tile and its one-cell
+// x/y halo are staged into a ring of kSvRing shared-memory planes by 16-byte cp.async copies
+// (whole 16-byte chunks of grown rows: they never cross a row's pitch, so every copy stays inside
+// the level's buffer), kSvLead planes ahead of the plane being computed; z neighbours come from a
+// register window fed from the ring's centre column. Pointwise inputs (rhs, f, u64) are loaded at
+// the top of the plane so their latency overlaps the wait. Terms are summed in the Laplacian's
+// insertion order with the single-solve solver's epilogue arithmetic, so results are bitwise its.
+constexpr int kSvTX = 32, kSvTY = kSvUnit / 32;          // 32 x 8 cells, one per thread
+constexpr int kSvRowStride = 36;                          // staged row: grown x0 .. x0+35 (34 used)
+constexpr int kSvPlane = kSvRowStride * (kSvTY + 2);
+constexpr int kSvLead = 1 + 3, kSvRing = kSvLead + 1;
 
-__device__ __forceinline__ void sv_walk_units(int n, int zd, int& xc_count, int& zc_count)
+__device__ __forceinline__ void sv_ring_units(int n, int zd, int& xt, int& yt, int& zt)
 {
-    xc_count = (n + 31) / 32;
-    zc_count = (n + zd - 1) / zd;
+    xt = (n + kSvTX - 1) / kSvTX;
+    yt = (n + kSvTY - 1) / kSvTY;
+    zt = (n + zd - 1) / zd;
 }
 
 template <int OP, typename V>
-__global__ void __launch_bounds__(kSvUnit) k_sv_walk(const SvItem* __restrict__ items, const long long* __restrict__ unit0,
+__global__ void __launch_bounds__(kSvUnit) k_sv_ring(const SvItem* __restrict__ items, const long long* __restrict__ unit0,
                                                      const SvPhaseHeader* __restrict__ hdr, double* norms)
 {
+    constexpr int L = kSvLead, Q = kSvRing, PM = kSvPlane, RS = kSvRowStride;
+    constexpr int CE = 16 / sizeof(V);                    // elements per 16-byte chunk
+    constexpr int NCH = (kSvTX + 2 + CE - 1) / CE;        // chunks per staged row
+    __shared__ __align__(16) V ring[Q * PM];
     const int count = (int)hdr->count;
     const long long total = hdr->total;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (long long w0 = (long long)blockIdx.x * kSvRows; w0 < total; w0 += (long long)gridDim.x * kSvRows) {
-        const SvItem* itp = items + sv_find(unit0, count, w0);
-        const int unit = (int)(w0 - itp->unit0) + warp;
-        const int units = itp->units;
-        double m = 0.0;
-        if (unit < units) {
-            // the item's fields, once, into registers
-            const RelaxCoef<float> k = itp->k;
-            const int n = k.n;
-            const int zd = itp->zd;
-            float* const in32 = itp->in;
-            float* const out32 = itp->out;
-            const float* const rhs = itp->rhs;
-            double* const u64 = itp->u64;
-            const double* const f64 = itp->f64;
-            const int sxd = itp->sxd;
-            const float alpha = itp->alpha;
-            const double alpha64 = itp->alpha64, beta64 = itp->beta64;
-            Coefs<V> cf;
-            if constexpr (OP == SV_K1) cf = itp->c64;
-            else cf = itp->c;
-            int XC, ZC;
-            sv_walk_units(n, zd, XC, ZC);
-            const int y = unit % n, xc = (unit / n) % XC, zc = unit / (n * XC);
-            const int x = xc * 32 + lane;
-            const bool act = x < n;
-            const bool last = act && (lane == 31 || x == n - 1);
-            const int z0 = zc * zd, z1 = min(z0 + zd, n);
-            // source field (FP32 level for the sweeps, FP64 u for the residual pass)
-            const V* src;
-            int sx;
-            if constexpr (OP == SV_K1) {
-                src = reinterpret_cast<const V*>(u64);
-                sx = sxd;
-            } else {
-                src = reinterpret_cast<const V*>(in32);
-                sx = k.sx;
+    const uint32_t ring0 = smem_u32(ring);
+    for (long long u = blockIdx.x; u < total; u += gridDim.x) {
+        const SvItem* itp = items + sv_find(unit0, count, u);
+        const int unit = (int)(u - itp->unit0);
+        const RelaxCoef<float> k = itp->k;
+        const int n = k.n;
+        const int zd = itp->zd;
+        float* const in32 = itp->in;
+        float* const out32 = itp->out;
+        const float* const rhs = itp->rhs;
+        double* const u64 = itp->u64;
+        const double* const f64 = itp->f64;
+        const int sxd = itp->sxd;
+        const float alpha = itp->alpha;
+        const double alpha64 = itp->alpha64, beta64 = itp->beta64;
+        Coefs<V> cf;
+        if constexpr (OP == SV_K1) cf = itp->c64;
+        else cf = itp->c;
+        int XT, YT, ZT;
+        sv_ring_units(n, zd, XT, YT, ZT);
+        const int x0 = (unit % XT) * kSvTX, y0 = ((unit / XT) % YT) * kSvTY, z0 = (unit / (XT * YT)) * zd;
+        const int z1 = min(z0 + zd, n);
+        const V* src;
+        int sx;
+        if constexpr (OP == SV_K1) {
+            src = reinterpret_cast<const V*>(u64);
+            sx = sxd;
+        } else {
+            src = reinterpret_cast<const V*>(in32);
+            sx = k.sx;
+        }
+        const long long Sz = (long long)sx * (n + 2);
+        // this thread's staging chunk: row r (y = y0 - 1 + r), chunk c (grown x = x0 + c*CE)
+        const int sr = threadIdx.x / NCH, sc_ = threadIdx.x % NCH;
+        const int gx = x0 + sc_ * CE, gy = y0 - 1 + sr;
+        const bool stg = threadIdx.x < NCH * (kSvTY + 2) && gx < min(x0 + kSvTX + 2, n + 2) && gy <= n;
+        const V* sp = src + (stg ? (long long)gx + (long long)sx * (gy + 1) + Sz * (z0 + 1) : 0);
+        const uint32_t sdst = ring0 + (uint32_t)sizeof(V) * (sr * RS + sc_ * CE);
+        auto stage = [&](int zz, int slot) {
+            if (stg && zz < z1) {
+                cp_async16(sdst + (uint32_t)sizeof(V) * slot * PM, sp);
+                sp += Sz;
             }
-            const int Sy = sx, Sz = sx * (n + 2), nn = n * n;
-            const V* c = src + (long long)grown_index<V>(n, sx, act ? x : 0, y, z0);   // (x, y, z0)
-            const int ey = edge_code(y, n), ex = act ? edge_code(x, n) : 0;
-            int i = (act ? x : 0) + n * (y + n * z0);
-            // plane z's loads are issued one plane ahead: +z, +-y, the chunk-end x neighbours and the
-            // pointwise inputs (rhs; f for the residual pass; u64 for the update)
-            V zm = act ? c[-Sz] : V(0), z_ = act ? c[0] : V(0);
-            V zp_n = V(0), ym_n = V(0), yp_n = V(0), xme_n = V(0), xpe_n = V(0);
-            float r_n = 0.f;
-            double d_n = 0.0;
-            auto fetch = [&](const V* cc, int ii, int zz) {
-                if (!act) return;
-                zp_n = cc[Sz];
-                ym_n = cc[-Sy];
-                yp_n = cc[Sy];
-                if (lane == 0) xme_n = cc[-1];
-                if (last) xpe_n = cc[1];
-                if constexpr (OP == SV_K1) d_n = f64[ii];
-                else r_n = rhs[ii];
-                if constexpr (OP == SV_UPDATE) d_n = u64[grown_index<double>(n, sxd, x, y, zz)];
-            };
-            fetch(c, i, z0);
-            for (int z = z0; z < z1; z++) {
-                const V zp = zp_n, ym = ym_n, yp = yp_n, xme = xme_n, xpe = xpe_n;
-                const float rr = r_n;
-                const double dd = d_n;
-                if (z + 1 < z1) fetch(c + Sz, i + nn, z + 1);
-                // neighbours along x from the lanes beside (the chunk's end lanes load them)
-                V xm = __shfl_up_sync(0xffffffffu, z_, 1);
-                V xp = __shfl_down_sync(0xffffffffu, z_, 1);
-                if (lane == 0) xm = xme;
-                if (last) xp = xpe;
-                if (act) {
-                    const int ez = edge_code(z, n);
-                    // Laplacian insertion order: 0, +x, -x, +y, -y, +z, -z
-                    if constexpr (OP == SV_K1) {
-                        double res;
-                        float al = 0.f;
-                        if (!k.helm) {
-                            res = dadd(0.0, dd);
-                            res = dadd(res, dmul(cf.c[0], (double)z_));
-                            res = dadd(res, dmul(cf.c[1], (double)xp));
-                            res = dadd(res, dmul(cf.c[2], (double)xm));
-                            res = dadd(res, dmul(cf.c[3], (double)yp));
-                            res = dadd(res, dmul(cf.c[4], (double)ym));
-                            res = dadd(res, dmul(cf.c[5], (double)zp));
-                            res = dadd(res, dmul(cf.c[6], (double)zm));
-                        } else {
-                            double lp = 0.0;
-                            lp = dadd(lp, dmul(cf.c[0], (double)z_));
-                            lp = dadd(lp, dmul(cf.c[1], (double)xp));
-                            lp = dadd(lp, dmul(cf.c[2], (double)xm));
-                            lp = dadd(lp, dmul(cf.c[3], (double)yp));
-                            lp = dadd(lp, dmul(cf.c[4], (double)ym));
-                            lp = dadd(lp, dmul(cf.c[5], (double)zp));
-                            lp = dadd(lp, dmul(cf.c[6], (double)zm));
-                            res = dsub(dd, dsub(dmul(alpha64, (double)z_), dmul(beta64, lp)));
-                            al = __double2float_rn(alpha64);
-                        }
-                        m = upd_abs(m, res);
-                        const float r32 = __double2float_rn(res);
-                        out32[i] = r32;
-                        float* q = in32 + grown_index<float>(n, k.sx, x, y, z);
-                        store_with_images(in32, n, k.sx, q, ex, ey, ez, relax_value(k, 0.f, 0.f, r32, al));
+            cp_async_commit();
+        };
+#pragma unroll
+        for (int q = 0; q < L; q++) stage(z0 + q, q);
+        const int x = x0 + lane, y = y0 + warp;
+        const bool act = x < n && y < n;
+        const V* col = src + (long long)grown_index<V>(n, sx, act ? x : 0, act ? y : 0, z0);   // (x, y, z0)
+        V zm = act ? col[-Sz] : V(0), z_ = act ? col[0] : V(0);
+        const int ey = act ? edge_code(y, n) : 0, ex = act ? edge_code(x, n) : 0;
+        const int cidx = (warp + 1) * RS + lane + 1;
+        int i = (act ? x + n * (y + n * z0) : 0);
+        double m = 0.0;
+        int qz = 0;
+        for (int z = z0; z < z1; z++) {
+            float rr = 0.f;
+            double dd = 0.0;
+            if (act) {
+                if constexpr (OP == SV_K1) dd = f64[i];
+                else rr = rhs[i];
+                if constexpr (OP == SV_UPDATE) dd = u64[grown_index<double>(n, sxd, x, y, z)];
+            }
+            cp_async_wait<L - 2>();   // this thread's copies of plane z + 1 have landed
+            __syncthreads();          // everyone's have; everyone is done with plane z - 1
+            stage(z + L, qz == 0 ? Q - 1 : qz - 1);
+            if (act) {
+                int q1 = qz + 1;
+                if (q1 >= Q) q1 -= Q;
+                const V zp = z + 1 < z1 ? ring[q1 * PM + cidx] : col[Sz];
+                const V* pl = ring + qz * PM + cidx;
+                const V xm = pl[-1], xp = pl[1], ym = pl[-RS], yp = pl[RS];
+                const int ez = edge_code(z, n);
+                // Laplacian insertion order: 0, +x, -x, +y, -y, +z, -z
+                if constexpr (OP == SV_K1) {
+                    double res;
+                    float al = 0.f;
+                    if (!k.helm) {
+                        res = dadd(0.0, dd);
+                        res = dadd(res, dmul(cf.c[0], (double)z_));
+                        res = dadd(res, dmul(cf.c[1], (double)xp));
+                        res = dadd(res, dmul(cf.c[2], (double)xm));
+                        res = dadd(res, dmul(cf.c[3], (double)yp));
+                        res = dadd(res, dmul(cf.c[4], (double)ym));
+                        res = dadd(res, dmul(cf.c[5], (double)zp));
+                        res = dadd(res, dmul(cf.c[6], (double)zm));
                     } else {
-                        float acc = 0.f;
-                        acc = dadd(acc, dmul(cf.c[0], (float)z_));
-                        acc = dadd(acc, dmul(cf.c[1], (float)xp));
-                        acc = dadd(acc, dmul(cf.c[2], (float)xm));
-                        acc = dadd(acc, dmul(cf.c[3], (float)yp));
-                        acc = dadd(acc, dmul(cf.c[4], (float)ym));
-                        acc = dadd(acc, dmul(cf.c[5], (float)zp));
-                        acc = dadd(acc, dmul(cf.c[6], (float)zm));
-                        const float v = relax_value(k, acc, (float)z_, rr, alpha);
-                        if constexpr (OP == SV_RELAX) {
-                            const long long g = c - src;
-                            store_with_images(out32, n, sx, out32 + g, ex, ey, ez, v);
-                        } else {
-                            double* q = u64 + grown_index<double>(n, sxd, x, y, z);
-                            store_with_images(u64, n, sxd, q, ex, ey, ez, dadd(dd, (double)v));
-                        }
+                        double lp = 0.0;
+                        lp = dadd(lp, dmul(cf.c[0], (double)z_));
+                        lp = dadd(lp, dmul(cf.c[1], (double)xp));
+                        lp = dadd(lp, dmul(cf.c[2], (double)xm));
+                        lp = dadd(lp, dmul(cf.c[3], (double)yp));
+                        lp = dadd(lp, dmul(cf.c[4], (double)ym));
+                        lp = dadd(lp, dmul(cf.c[5], (double)zp));
+                        lp = dadd(lp, dmul(cf.c[6], (double)zm));
+                        res = dsub(dd, dsub(dmul(alpha64, (double)z_), dmul(beta64, lp)));
+                        al = __double2float_rn(alpha64);
+                    }
+                    m = upd_abs(m, res);
+                    const float r32 = __double2float_rn(res);
+                    out32[i] = r32;
+                    float* q = in32 + grown_index<float>(n, k.sx, x, y, z);
+                    store_with_images(in32, n, k.sx, q, ex, ey, ez, relax_value(k, 0.f, 0.f, r32, al));
+                } else {
+                    float acc = 0.f;
+                    acc = dadd(acc, dmul(cf.c[0], (float)z_));
+                    acc = dadd(acc, dmul(cf.c[1], (float)xp));
+                    acc = dadd(acc, dmul(cf.c[2], (float)xm));
+                    acc = dadd(acc, dmul(cf.c[3], (float)yp));
+                    acc = dadd(acc, dmul(cf.c[4], (float)ym));
+                    acc = dadd(acc, dmul(cf.c[5], (float)zp));
+                    acc = dadd(acc, dmul(cf.c[6], (float)zm));
+                    const float v = relax_value(k, acc, (float)z_, rr, alpha);
+                    if constexpr (OP == SV_RELAX) {
+                        const long long g = grown_index<float>(n, sx, x, y, z);
+                        store_with_images(out32, n, sx, out32 + g, ex, ey, ez, v);
+                    } else {
+                        double* q = u64 + grown_index<double>(n, sxd, x, y, z);
+                        store_with_images(u64, n, sxd, q, ex, ey, ez, dadd(dd, (double)v));
                     }
                 }
                 zm = z_;
                 z_ = zp;
-                c += Sz;
-                i += nn;
             }
+            col += Sz;
+            i += n * n;
+            qz = qz == Q - 1 ? 0 : qz + 1;
         }
+        cp_async_wait<0>();
+        __syncthreads();              // the ring is free for the next unit
         if constexpr (OP == SV_K1) {
             for (int o = 16; o > 0; o >>= 1) {
                 const double w = __shfl_down_sync(0xffffffffu, m, o);
                 m = (m < w) ? w : m;
             }
-            if (lane == 0 && m > 0.0 && unit < units) atomic_max_nonneg(norms + itp->slot, m);
+            if (lane == 0 && m > 0.0) atomic_max_nonneg(norms + itp->slot, m);
         }
     }
 }

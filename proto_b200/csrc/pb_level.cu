@@ -12,6 +12,8 @@
 #include <map>
 #include <vector>
 
+#include <type_traits>
+
 #include "pb_internal.cuh"
 #include "pb_stencil_impl.cuh"
 
@@ -315,11 +317,13 @@ constexpr int kLevelPairPlaneMax = (64 + 4) * (8 + 4);   // (2tx+4)(ty+4) <= 816
 
 
 template <class S>
-__global__ void __launch_bounds__(kLevelThreads) k_level_star_pair(const double* __restrict__ u, double* out,
+__global__ void __launch_bounds__(kLevelThreads, 4) k_level_star_pair(const double* __restrict__ u, double* out,
                                                                    const PatchTile* __restrict__ tiles,
                                                                    Coefs<double> cf, double a, int euler)
 {
-    constexpr int R = S::R, W = 2 * R + 1, L = level_lead(R), Q = level_ring(R), PM = kLevelPairPlaneMax;
+    // ring of Q = 2R+1 planes, lead L = Q-1: the z loop is unrolled by Q so ring slots and the
+    // register window's slots are compile-time constants at every step (no window moves)
+    constexpr int R = S::R, W = 2 * R + 1, Q = W, L = Q - 1, PM = kLevelPairPlaneMax;
     static_assert(R == 2, "cell pairs line up with 16-byte boundaries for a halo of 2");
     __shared__ __align__(16) double ring[Q * PM];
     const PatchTile t = tiles[blockIdx.x];
@@ -331,7 +335,7 @@ __global__ void __launch_bounds__(kLevelThreads) k_level_star_pair(const double*
     const int lx = threadIdx.x % tx, ly = threadIdx.x / tx;
     const int x = t.x0 + 2 * lx, y = t.y0 + ly;
     const bool act = x < nx && y < ny;
-    const int z1 = min(t.z0 + t.zd, nz);
+    const int z0 = t.z0, z1 = min(t.z0 + t.zd, nz);
     constexpr int kMaxLoads = (PM / 2 + kLevelThreads - 1) / kLevelThreads;
     const double* lp[kMaxLoads];
     long long ls[kMaxLoads];
@@ -391,31 +395,32 @@ __global__ void __launch_bounds__(kLevelThreads) k_level_star_pair(const double*
         return __ldg(reinterpret_cast<const double2*>(q));
     };
 #pragma unroll
-    for (int k = 0; k < L; k++) stage(t.z0 + k, k);
+    for (int k = 0; k < L; k++) stage(z0 + k, k);
+    // window slot of plane p: (p - z0 + R) mod W
     double w0[W], w1[W];
     if (act) {
 #pragma unroll
         for (int k = 0; k < 2 * R; k++) {
-            const double2 v = zcol(t.z0 - R + k);
+            const double2 v = zcol(z0 - R + k);
             w0[k] = v.x;
             w1[k] = v.y;
         }
     }
     double* op = out + t.off + cxy + Sxy * t.z0;
     const int sc = (ly + R) * BX + (2 * lx + R);   // even: pairs are 16-byte aligned in the ring
-    int qz = 0;
-    for (int z = t.z0; z < z1; z++) {
-        cp_async_wait<L - R - 1>();
-        __syncthreads();
-        const int qn = qz == 0 ? Q - 1 : qz - 1;
-        stage(z + L, qn);
-        const double* pl = ring + qz * PM + sc;
+    // one plane; J = (z - z0) mod Q, so plane z sits in ring slot J and window slot J + R
+    auto step = [&](auto Jc, int z) {
+        constexpr int J = decltype(Jc)::value;
+        cp_async_wait<L - R - 1>();   // this thread's copies of plane z + R have landed
+        __syncthreads();              // everyone's have; everyone is done with plane z - 1
+        stage(z + L, (J + L) % Q);    // into the slot of plane z - 1
         if (act) {
-            int qr = qz + R;
-            if (qr >= Q) qr -= Q;
-            const double2 cn = z + R < z1 ? *reinterpret_cast<const double2*>(ring + qr * PM + sc) : zcol(z + R);
-            w0[2 * R] = cn.x;
-            w1[2 * R] = cn.y;
+            constexpr int qr = (J + R) % Q, wn = (J + 2 * R) % W;
+            const double2 cn =
+                z + R < z1 ? *reinterpret_cast<const double2*>(ring + qr * PM + sc) : zcol(z + R);
+            w0[wn] = cn.x;
+            w1[wn] = cn.y;
+            const double* pl = ring + J * PM + sc;
             const double2 xm = *reinterpret_cast<const double2*>(pl - 2);   // x-2, x-1
             const double2 xc = *reinterpret_cast<const double2*>(pl);       // x, x+1
             const double2 xp = *reinterpret_cast<const double2*>(pl + 2);   // x+2, x+3
@@ -429,8 +434,9 @@ __global__ void __launch_bounds__(kLevelThreads) k_level_star_pair(const double*
                 const int ox = S::off(j, 0), oy = S::off(j, 1), oz = S::off(j, 2);
                 double v0, v1;
                 if (oz != 0 || (ox == 0 && oy == 0)) {
-                    v0 = w0[R + oz];
-                    v1 = w1[R + oz];
+                    const int ws = (J + R + oz + W) % W;
+                    v0 = w0[ws];
+                    v1 = w1[ws];
                 } else if (oy != 0) {
                     const double2 q = oy == 1 ? yp1 : oy == -1 ? ym1 : oy == 2 ? yp2 : ym2;
                     v0 = q.x;
@@ -442,18 +448,30 @@ __global__ void __launch_bounds__(kLevelThreads) k_level_star_pair(const double*
                 a0 = dadd(a0, dmul(cf.c[j], v0));
                 a1 = dadd(a1, dmul(cf.c[j], v1));
             }
+            constexpr int wc = (J + R) % W;
             double2 r;
-            r.x = euler ? dadd(w0[R], dmul(a, a0)) : a0;
-            r.y = euler ? dadd(w1[R], dmul(a, a1)) : a1;
+            r.x = euler ? dadd(w0[wc], dmul(a, a0)) : a0;
+            r.y = euler ? dadd(w1[wc], dmul(a, a1)) : a1;
             *reinterpret_cast<double2*>(op) = r;
-#pragma unroll
-            for (int k = 0; k < 2 * R; k++) {
-                w0[k] = w0[k + 1];
-                w1[k] = w1[k + 1];
-            }
         }
         op += Sxy;
-        qz = qz == Q - 1 ? 0 : qz + 1;
+    };
+    using I0 = std::integral_constant<int, 0>;
+    using I1 = std::integral_constant<int, 1>;
+    using I2 = std::integral_constant<int, 2>;
+    using I3 = std::integral_constant<int, 3>;
+    using I4 = std::integral_constant<int, 4>;
+    static_assert(Q == 5, "the unrolled loop below has five steps");
+    for (int z = z0; z < z1; z += Q) {
+        step(I0{}, z);
+        if (z + 1 >= z1) break;
+        step(I1{}, z + 1);
+        if (z + 2 >= z1) break;
+        step(I2{}, z + 2);
+        if (z + 3 >= z1) break;
+        step(I3{}, z + 3);
+        if (z + 4 >= z1) break;
+        step(I4{}, z + 4);
     }
     cp_async_wait<0>();
 }

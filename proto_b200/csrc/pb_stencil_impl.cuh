@@ -22,7 +22,8 @@ struct TableArgs {
 struct StarTune {
     enum Mode { AUTO = 0, TMA = 1, SIMPLE = 2 };
     int mode = AUTO;
-    long long min_tma_points = 1 << 18;   // smaller boxes are launch/latency bound: simple kernel
+    long long min_tma_points = 1 << 19;   // smaller boxes (64^3 and below) are launch/latency bound:
+                                          // the simple kernel finishes them sooner
     int zc = 0;                          // z chunk per CTA; 0 = occupancy-based heuristic
     int ty = 8;                          // CTA tile height
     int yb = 2;                          // rows per consumer thread

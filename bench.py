@@ -206,7 +206,8 @@ def run_amr_level(pb, torch, steps=100, reps=5, cpu=True, tune=True):
            "interior_cells": interior, "us_per_step": t * 1e6, "steps_per_s": 1.0 / t,
            "gpts_per_s": interior / t / 1e9, "gbs_algorithmic": 16.0 * interior / t / 1e9,
            "frac_of_hbm": 16.0 * interior / t / 1e9 / peak, "tiles": lv.tiles(),
-           "gpu_launches_per_step": 2}
+           "gpu_launches_per_step": 1,   # fused step: the tensor-product tiling needs no exchange launch
+           }
     try:   # the reference's own per-patch stepping on one host core, one step
         from oracle.oracle import Ref
         if cpu and Ref.available():

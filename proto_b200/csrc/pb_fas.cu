@@ -13,6 +13,7 @@
 // residual history and the solution are bitwise the reference's. Kernels that write a state also
 // write its periodic ghost images.
 #include <cmath>
+#include <cstring>
 #include <vector>
 
 #include "pb_internal.cuh"
@@ -387,6 +388,128 @@ __global__ void __launch_bounds__(256) k_fas_unpack(const double* __restrict__ u
     }
 }
 
+// ---- the levels of edge <= kFasCoarseEdge in one CTA ------------------------------------------
+// The same per-cell operations as the kernels above, in the same order (sweeps, averaging,
+// coarse force, recursion, correction), each phase a block-stride loop followed by a barrier;
+// the state stays in the levels' own (L2-resident) buffers. One launch replaces about thirty
+// launch-bound ones; a 16^3 level already costs more FP64 work than one SM does quickly, so it
+// keeps its own launches.
+constexpr int kFasCoarseEdge = 8, kFasCoarseMax = 8, kFasCoarseThreads = 512;
+
+struct FasCoarseLevel {
+    int n;
+    FasCoef k;
+    double neg_lambda;
+    double* u[2];
+    double* f;
+    double* c0;
+};
+struct FasCoarseArgs {
+    FasCoarseLevel lv[kFasCoarseMax];   // 0 = coarsest
+    int top;                            // index of the entry level
+    int num_pre, num_post, num_bottom;
+};
+
+#define FAS_BLOCK_LOOP(total) for (long long i = threadIdx.x; i < (total); i += blockDim.x)
+
+__device__ void fas_blk_relax(const FasCoarseLevel& L, int from, int sweeps)
+{
+    const int n = L.n, S = n + 2 * kFasGhost;
+    const long long n3 = (long long)n * n * n;
+    int c = from;
+    for (int s = 0; s < sweeps; s++) {
+        const double* u = L.u[c];
+        double* out = L.u[1 - c];
+        FAS_BLOCK_LOOP(n3)
+        {
+            int x, y, z;
+            fas_cell(i, n, x, y, z);
+            const long long g = fas_index(S, x, y, z);
+            const double res = dadd(fas_op(u, g, S, L.k), L.f[i]);
+            fas_store(out, n, x, y, z, dadd(u[g], dmul(L.neg_lambda, res)));
+        }
+        __syncthreads();
+        c = 1 - c;
+    }
+}
+
+__global__ void __launch_bounds__(kFasCoarseThreads) k_fas_coarse_cycle(FasCoarseArgs a)
+{
+    // Every level is entered with its state in buffer 0 (the entry level by its parent, the others
+    // by the averaging below), so the buffer holding a level's state is fixed by the sweep counts:
+    // after the pre-sweeps (and through the correction) pre & 1; at the end post-sweeps included,
+    // (pre + post) & 1; the coarsest level's after its sweeps, bottom & 1.
+    const int c_pre = a.num_pre & 1, c_end = (a.num_pre + a.num_post) & 1, c_bot = a.num_bottom & 1;
+    // down: pre-sweeps, coarse state and force
+    for (int l = a.top; l >= 1; l--) {
+        const FasCoarseLevel& L = a.lv[l];
+        const FasCoarseLevel& C = a.lv[l - 1];
+        fas_blk_relax(L, 0, a.num_pre);
+        const int nf = L.n, nc = C.n, Sf = nf + 2 * kFasGhost;
+        const long long nc3 = (long long)nc * nc * nc;
+        const double* u = L.u[c_pre];
+        FAS_BLOCK_LOOP(nc3)
+        {   // k_fas_average
+            int x, y, z;
+            fas_cell(i, nc, x, y, z);
+            double acc = 0.0;
+#pragma unroll
+            for (int c = 0; c < 8; c++)
+                acc = dadd(acc, dmul(0.125, u[fas_index(Sf, 2 * x + (c & 1), 2 * y + ((c >> 1) & 1), 2 * z + (c >> 2))]));
+            fas_store(C.u[0], nc, x, y, z, acc);
+            C.c0[i] = acc;
+        }
+        FAS_BLOCK_LOOP(nc3)
+        {   // k_fas_restrict
+            int x, y, z;
+            fas_cell(i, nc, x, y, z);
+            double acc = 0.0;
+#pragma unroll
+            for (int c = 0; c < 8; c++) {
+                const int fx = 2 * x + (c & 1), fy = 2 * y + ((c >> 1) & 1), fz = 2 * z + (c >> 2);
+                const double res = dadd(fas_op(u, fas_index(Sf, fx, fy, fz), Sf, L.k),
+                                        L.f[fx + (long long)nf * (fy + (long long)nf * fz)]);
+                acc = dadd(acc, dmul(0.125, res));
+            }
+            C.f[i] = acc;
+        }
+        __syncthreads();
+        const int Sc = nc + 2 * kFasGhost;
+        FAS_BLOCK_LOOP(nc3)
+        {   // k_fas_force
+            int x, y, z;
+            fas_cell(i, nc, x, y, z);
+            C.f[i] = dsub(C.f[i], fas_op(C.u[0], fas_index(Sc, x, y, z), Sc, C.k));
+        }
+        __syncthreads();
+    }
+    fas_blk_relax(a.lv[0], 0, a.num_bottom);
+    // up: correction from the level below, post-sweeps
+    for (int l = 1; l <= a.top; l++) {
+        const FasCoarseLevel& L = a.lv[l];
+        const FasCoarseLevel& C = a.lv[l - 1];
+        const int nf = L.n, nc = C.n, Sc = nc + 2 * kFasGhost, Sf = nf + 2 * kFasGhost;
+        const long long nc3 = (long long)nc * nc * nc, nf3 = (long long)nf * nf * nf;
+        FAS_BLOCK_LOOP(nc3)
+        {   // k_fas_delta
+            int x, y, z;
+            fas_cell(i, nc, x, y, z);
+            C.c0[i] = dmul(dsub(C.c0[i], C.u[l - 1 == 0 ? c_bot : c_end][fas_index(Sc, x, y, z)]), -1.0);
+        }
+        __syncthreads();
+        double* u = L.u[c_pre];
+        FAS_BLOCK_LOOP(nf3)
+        {   // k_fas_correct
+            int x, y, z;
+            fas_cell(i, nf, x, y, z);
+            const double d = C.c0[x / 2 + (long long)nc * (y / 2 + (long long)nc * (z / 2))];
+            fas_store(u, nf, x, y, z, dadd(u[fas_index(Sf, x, y, z)], dmul(1.0, d)));
+        }
+        __syncthreads();
+        fas_blk_relax(L, c_pre, a.num_post);
+    }
+}
+
 struct FasLevel {
     int n;
     double dx;
@@ -456,8 +579,30 @@ static int fas_relax(pb_fas* m, int l, int sweeps, cudaStream_t st)
     return PB_OK;
 }
 
+// every level of edge <= kFasCoarseEdge (l and below) in one single-CTA launch; level l's state
+// starts at buffer 0 (its parent has just averaged into it) and ends at the parity of its sweeps
+static int fas_coarse(pb_fas* m, int l, cudaStream_t st)
+{
+    FasCoarseArgs a;
+    memset(&a, 0, sizeof(a));
+    for (int q = 0; q <= l; q++) {
+        const FasLevel& L = m->lv[q];
+        a.lv[q] = FasCoarseLevel{L.n, L.k, L.neg_lambda, {L.u[0], L.u[1]}, L.f, L.c0};
+    }
+    a.top = l;
+    a.num_pre = m->num_pre;
+    a.num_post = m->num_post;
+    a.num_bottom = m->num_bottom;
+    k_fas_coarse_cycle<<<1, kFasCoarseThreads, 0, st>>>(a);
+    PB_LAUNCH_CHECK();
+    FasLevel& T = m->lv[l];
+    T.cur = l == 0 ? (T.cur + m->num_bottom) & 1 : (T.cur + m->num_pre + m->num_post) & 1;
+    return PB_OK;
+}
+
 static int fas_vcycle(pb_fas* m, int l, cudaStream_t st)
 {
+    if (m->lv[l].n <= kFasCoarseEdge && l < kFasCoarseMax && l < (int)m->lv.size() - 1) return fas_coarse(m, l, st);
     if (l == 0) return fas_relax(m, l, m->num_bottom, st);
     FasLevel& L = m->lv[l];
     FasLevel& C = m->lv[l - 1];

@@ -385,24 +385,29 @@ __global__ void __launch_bounds__(256) k_resid_restrict(const T* __restrict__ ph
 }
 static inline dim3 restrict_grid(int nf) { return dim3((nf / 2 + 31) / 32, (nf / 2 + 7) / 8, nf / 2); }
 
-// phi += 1.0 * delta_c(p/2) on the valid box, periodic images included. Block (32, 8): a thread
-// owns the two fine cells of one coarse cell in x.
+// phi += 1.0 * delta_c(p/2) on the valid box, periodic images included. Block (32, 8) over a
+// 64 x 8 tile of fine cells: each thread takes fine x and x + 32, so every warp access is 32
+// consecutive cells.
 template <typename T>
 __global__ void __launch_bounds__(256) k_prolong(T* phi, const T* __restrict__ delta_c, int nf, int sxf, int sxc)
 {
     const int nc = nf / 2;
-    const int cx = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
-    if (cx >= nc || y >= nf) return;
-    const T d = delta_c[grown_index<T>(nc, sxc, cx, y / 2, z / 2)];
+    const int y = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
+    if (y >= nf) return;
     const int ey = edge_code(y, nf), ez = edge_code(z, nf);
+    const T* drow = delta_c + grown_index<T>(nc, sxc, 0, y / 2, z / 2);
+    T* prow = phi + grown_index<T>(nf, sxf, 0, y, z);
 #pragma unroll
     for (int v = 0; v < 2; v++) {
-        const int x = 2 * cx + v;
-        T* q = phi + grown_index<T>(nf, sxf, x, y, z);
-        store_with_images(phi, nf, sxf, q, edge_code(x, nf), ey, ez, dadd(*q, dmul(T(1), d)));
+        const int x = blockIdx.x * 64 + v * 32 + threadIdx.x;
+        if (x < nf) {
+            const T d = __ldg(drow + x / 2);
+            T* q = prow + x;
+            store_with_images(phi, nf, sxf, q, edge_code(x, nf), ey, ez, dadd(*q, dmul(T(1), d)));
+        }
     }
 }
-static inline dim3 prolong_grid(int nf) { return dim3((nf / 2 + 31) / 32, (nf + 7) / 8, nf); }
+static inline dim3 prolong_grid(int nf) { return dim3((nf + 63) / 64, (nf + 7) / 8, nf); }
 
 // n^3 <-> grown layout with periodic ghost images
 template <typename T>

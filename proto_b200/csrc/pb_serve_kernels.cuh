@@ -178,14 +178,15 @@ __global__ void __launch_bounds__(kSvUnit) k_sv_phase(const SvItem* __restrict__
 }
 
 // The stencil phases (sweep, FP64 residual pass, last sweep + FP64 correction) with a CTA per
-// unit = (item, 32 x 8 tile of a level, chunk of zd planes): per plane the tile and its one-cell
-// x/y halo are staged into a ring of kSvRing shared-memory planes by 16-byte cp.async copies
-// (whole 16-byte chunks of grown rows: they never cross a row's pitch, so every copy stays inside
-// the level's buffer), kSvLead planes ahead of the plane being computed; z neighbours come from a
-// register window fed from the ring's centre column. Pointwise inputs (rhs, f, u64) are loaded at
-// the top of the plane so their latency overlaps the wait. Terms are summed in the Laplacian's
-// insertion order with the single-solve solver's epilogue arithmetic, so results are bitwise its.
-constexpr int kSvTX = 32, kSvTY = kSvUnit / 32;          // 32 x 8 cells, one per thread
+// unit = (item, 32 x 16 tile of a level, chunk of zd planes); each thread owns two cells, (x, y)
+// and (x, y + 1). Per plane the tile and its one-cell x/y halo are staged into a ring of kSvRing
+// shared-memory planes by 16-byte cp.async copies (whole 16-byte chunks of grown rows: they never
+// cross a row's pitch, so every copy stays inside the level's buffer), kSvLead planes ahead of
+// the plane being computed; z neighbours come from register windows fed from the ring. Pointwise
+// inputs (rhs, f, u64) are loaded at the top of the plane so their latency overlaps the wait.
+// Terms are summed in the Laplacian's insertion order with the single-solve solver's epilogue
+// arithmetic, so results are bitwise its.
+constexpr int kSvTX = 32, kSvTY = 2 * (kSvUnit / 32);    // 32 x 16 cells, two per thread (in y)
 constexpr int kSvRowStride = 36;                          // staged row: grown x0 .. x0+35 (34 used)
 constexpr int kSvPlane = kSvRowStride * (kSvTY + 2);
 constexpr int kSvLead = 1 + 3, kSvRing = kSvLead + 1;
@@ -198,12 +199,14 @@ __device__ __forceinline__ void sv_ring_units(int n, int zd, int& xt, int& yt, i
 }
 
 template <int OP, typename V>
-__global__ void __launch_bounds__(kSvUnit) k_sv_ring(const SvItem* __restrict__ items, const long long* __restrict__ unit0,
+__global__ void __launch_bounds__(kSvUnit, 3) k_sv_ring(const SvItem* __restrict__ items, const long long* __restrict__ unit0,
                                                      const SvPhaseHeader* __restrict__ hdr, double* norms)
 {
     constexpr int L = kSvLead, Q = kSvRing, PM = kSvPlane, RS = kSvRowStride;
     constexpr int CE = 16 / sizeof(V);                    // elements per 16-byte chunk
     constexpr int NCH = (kSvTX + 2 + CE - 1) / CE;        // chunks per staged row
+    constexpr int NST = NCH * (kSvTY + 2);                // chunks per staged plane
+    constexpr int KL = (NST + kSvUnit - 1) / kSvUnit;     // chunks per thread
     __shared__ __align__(16) V ring[Q * PM];
     const int count = (int)hdr->count;
     const long long total = hdr->total;
@@ -240,98 +243,140 @@ __global__ void __launch_bounds__(kSvUnit) k_sv_ring(const SvItem* __restrict__ 
             sx = k.sx;
         }
         const long long Sz = (long long)sx * (n + 2);
-        // this thread's staging chunk: row r (y = y0 - 1 + r), chunk c (grown x = x0 + c*CE)
-        const int sr = threadIdx.x / NCH, sc_ = threadIdx.x % NCH;
-        const int gx = x0 + sc_ * CE, gy = y0 - 1 + sr;
-        const bool stg = threadIdx.x < NCH * (kSvTY + 2) && gx < min(x0 + kSvTX + 2, n + 2) && gy <= n;
-        const V* sp = src + (stg ? (long long)gx + (long long)sx * (gy + 1) + Sz * (z0 + 1) : 0);
-        const uint32_t sdst = ring0 + (uint32_t)sizeof(V) * (sr * RS + sc_ * CE);
+        // this thread's staging chunks: row r (y = y0 - 1 + r), chunk c (grown x = x0 + c*CE)
+        const V* sp[KL];
+        uint32_t sdst[KL];
+        bool stg[KL];
+#pragma unroll
+        for (int q = 0; q < KL; q++) {
+            const int t = threadIdx.x + q * kSvUnit;
+            const int sr = t / NCH, sc_ = t % NCH;
+            const int gx = x0 + sc_ * CE, gy = y0 - 1 + sr;
+            stg[q] = t < NST && gx < min(x0 + kSvTX + 2, n + 2) && gy <= n;
+            sp[q] = src + (stg[q] ? (long long)gx + (long long)sx * (gy + 1) + Sz * (z0 + 1) : 0);
+            sdst[q] = ring0 + (uint32_t)sizeof(V) * (sr * RS + sc_ * CE);
+        }
         auto stage = [&](int zz, int slot) {
-            if (stg && zz < z1) {
-                cp_async16(sdst + (uint32_t)sizeof(V) * slot * PM, sp);
-                sp += Sz;
+            if (zz < z1) {
+#pragma unroll
+                for (int q = 0; q < KL; q++)
+                    if (stg[q]) {
+                        cp_async16(sdst[q] + (uint32_t)sizeof(V) * slot * PM, sp[q]);
+                        sp[q] += Sz;
+                    }
             }
             cp_async_commit();
         };
 #pragma unroll
         for (int q = 0; q < L; q++) stage(z0 + q, q);
-        const int x = x0 + lane, y = y0 + warp;
-        const bool act = x < n && y < n;
-        const V* col = src + (long long)grown_index<V>(n, sx, act ? x : 0, act ? y : 0, z0);   // (x, y, z0)
-        V zm = act ? col[-Sz] : V(0), z_ = act ? col[0] : V(0);
-        const int ey = act ? edge_code(y, n) : 0, ex = act ? edge_code(x, n) : 0;
-        const int cidx = (warp + 1) * RS + lane + 1;
-        int i = (act ? x + n * (y + n * z0) : 0);
+        const int x = x0 + lane, ya = y0 + 2 * warp;
+        const bool act0 = x < n && ya < n, act1 = x < n && ya + 1 < n;
+        const V* col = src + (long long)grown_index<V>(n, sx, act0 ? x : 0, act0 ? ya : 0, z0);   // (x, ya, z0)
+        V zm0 = V(0), zc0 = V(0), zm1 = V(0), zc1 = V(0);
+        if (act0) {
+            zm0 = col[-Sz];
+            zc0 = col[0];
+        }
+        if (act1) {
+            zm1 = col[sx - Sz];
+            zc1 = col[sx];
+        }
+        const int ex = act0 ? edge_code(x, n) : 0;
+        const int ey0 = act0 ? edge_code(ya, n) : 0, ey1 = act1 ? edge_code(ya + 1, n) : 0;
+        const int cidx = (2 * warp + 1) * RS + lane + 1;   // cell (x, ya) in a ring plane
+        int i = act0 ? x + n * (ya + n * z0) : 0;          // (x, ya, z) in the n^3 fields
         double m = 0.0;
+        // one cell: the stencil taps, the plane's pointwise inputs and the outputs of this phase
+        auto cell = [&](int yy, int zz, int ey, int ez, int ii, V zm, V zc, V zp, V xm, V xp, V ym, V yp, float rr,
+                        double dd) {
+            // Laplacian insertion order: 0, +x, -x, +y, -y, +z, -z
+            if constexpr (OP == SV_K1) {
+                double res;
+                float al = 0.f;
+                if (!k.helm) {
+                    res = dadd(0.0, dd);
+                    res = dadd(res, dmul(cf.c[0], (double)zc));
+                    res = dadd(res, dmul(cf.c[1], (double)xp));
+                    res = dadd(res, dmul(cf.c[2], (double)xm));
+                    res = dadd(res, dmul(cf.c[3], (double)yp));
+                    res = dadd(res, dmul(cf.c[4], (double)ym));
+                    res = dadd(res, dmul(cf.c[5], (double)zp));
+                    res = dadd(res, dmul(cf.c[6], (double)zm));
+                } else {
+                    double lp = 0.0;
+                    lp = dadd(lp, dmul(cf.c[0], (double)zc));
+                    lp = dadd(lp, dmul(cf.c[1], (double)xp));
+                    lp = dadd(lp, dmul(cf.c[2], (double)xm));
+                    lp = dadd(lp, dmul(cf.c[3], (double)yp));
+                    lp = dadd(lp, dmul(cf.c[4], (double)ym));
+                    lp = dadd(lp, dmul(cf.c[5], (double)zp));
+                    lp = dadd(lp, dmul(cf.c[6], (double)zm));
+                    res = dsub(dd, dsub(dmul(alpha64, (double)zc), dmul(beta64, lp)));
+                    al = __double2float_rn(alpha64);
+                }
+                m = upd_abs(m, res);
+                const float r32 = __double2float_rn(res);
+                out32[ii] = r32;
+                float* q = in32 + grown_index<float>(n, k.sx, x, yy, zz);
+                store_with_images(in32, n, k.sx, q, ex, ey, ez, relax_value(k, 0.f, 0.f, r32, al));
+            } else {
+                float acc = 0.f;
+                acc = dadd(acc, dmul(cf.c[0], (float)zc));
+                acc = dadd(acc, dmul(cf.c[1], (float)xp));
+                acc = dadd(acc, dmul(cf.c[2], (float)xm));
+                acc = dadd(acc, dmul(cf.c[3], (float)yp));
+                acc = dadd(acc, dmul(cf.c[4], (float)ym));
+                acc = dadd(acc, dmul(cf.c[5], (float)zp));
+                acc = dadd(acc, dmul(cf.c[6], (float)zm));
+                const float v = relax_value(k, acc, (float)zc, rr, alpha);
+                if constexpr (OP == SV_RELAX) {
+                    float* q = out32 + grown_index<float>(n, sx, x, yy, zz);
+                    store_with_images(out32, n, sx, q, ex, ey, ez, v);
+                } else {
+                    double* q = u64 + grown_index<double>(n, sxd, x, yy, zz);
+                    store_with_images(u64, n, sxd, q, ex, ey, ez, dadd(dd, (double)v));
+                }
+            }
+        };
         int qz = 0;
         for (int z = z0; z < z1; z++) {
-            float rr = 0.f;
-            double dd = 0.0;
-            if (act) {
-                if constexpr (OP == SV_K1) dd = f64[i];
-                else rr = rhs[i];
-                if constexpr (OP == SV_UPDATE) dd = u64[grown_index<double>(n, sxd, x, y, z)];
+            float r0 = 0.f, r1 = 0.f;
+            double d0 = 0.0, d1 = 0.0;
+            if constexpr (OP == SV_K1) {
+                if (act0) d0 = f64[i];
+                if (act1) d1 = f64[i + n];
+            } else {
+                if (act0) r0 = rhs[i];
+                if (act1) r1 = rhs[i + n];
+            }
+            if constexpr (OP == SV_UPDATE) {
+                if (act0) d0 = u64[grown_index<double>(n, sxd, x, ya, z)];
+                if (act1) d1 = u64[grown_index<double>(n, sxd, x, ya + 1, z)];
             }
             cp_async_wait<L - 2>();   // this thread's copies of plane z + 1 have landed
             __syncthreads();          // everyone's have; everyone is done with plane z - 1
             stage(z + L, qz == 0 ? Q - 1 : qz - 1);
-            if (act) {
+            if (act0) {
                 int q1 = qz + 1;
                 if (q1 >= Q) q1 -= Q;
-                const V zp = z + 1 < z1 ? ring[q1 * PM + cidx] : col[Sz];
                 const V* pl = ring + qz * PM + cidx;
-                const V xm = pl[-1], xp = pl[1], ym = pl[-RS], yp = pl[RS];
-                const int ez = edge_code(z, n);
-                // Laplacian insertion order: 0, +x, -x, +y, -y, +z, -z
-                if constexpr (OP == SV_K1) {
-                    double res;
-                    float al = 0.f;
-                    if (!k.helm) {
-                        res = dadd(0.0, dd);
-                        res = dadd(res, dmul(cf.c[0], (double)z_));
-                        res = dadd(res, dmul(cf.c[1], (double)xp));
-                        res = dadd(res, dmul(cf.c[2], (double)xm));
-                        res = dadd(res, dmul(cf.c[3], (double)yp));
-                        res = dadd(res, dmul(cf.c[4], (double)ym));
-                        res = dadd(res, dmul(cf.c[5], (double)zp));
-                        res = dadd(res, dmul(cf.c[6], (double)zm));
-                    } else {
-                        double lp = 0.0;
-                        lp = dadd(lp, dmul(cf.c[0], (double)z_));
-                        lp = dadd(lp, dmul(cf.c[1], (double)xp));
-                        lp = dadd(lp, dmul(cf.c[2], (double)xm));
-                        lp = dadd(lp, dmul(cf.c[3], (double)yp));
-                        lp = dadd(lp, dmul(cf.c[4], (double)ym));
-                        lp = dadd(lp, dmul(cf.c[5], (double)zp));
-                        lp = dadd(lp, dmul(cf.c[6], (double)zm));
-                        res = dsub(dd, dsub(dmul(alpha64, (double)z_), dmul(beta64, lp)));
-                        al = __double2float_rn(alpha64);
-                    }
-                    m = upd_abs(m, res);
-                    const float r32 = __double2float_rn(res);
-                    out32[i] = r32;
-                    float* q = in32 + grown_index<float>(n, k.sx, x, y, z);
-                    store_with_images(in32, n, k.sx, q, ex, ey, ez, relax_value(k, 0.f, 0.f, r32, al));
+                V zp0, zp1;
+                if (z + 1 < z1) {
+                    zp0 = ring[q1 * PM + cidx];
+                    zp1 = ring[q1 * PM + cidx + RS];
                 } else {
-                    float acc = 0.f;
-                    acc = dadd(acc, dmul(cf.c[0], (float)z_));
-                    acc = dadd(acc, dmul(cf.c[1], (float)xp));
-                    acc = dadd(acc, dmul(cf.c[2], (float)xm));
-                    acc = dadd(acc, dmul(cf.c[3], (float)yp));
-                    acc = dadd(acc, dmul(cf.c[4], (float)ym));
-                    acc = dadd(acc, dmul(cf.c[5], (float)zp));
-                    acc = dadd(acc, dmul(cf.c[6], (float)zm));
-                    const float v = relax_value(k, acc, (float)z_, rr, alpha);
-                    if constexpr (OP == SV_RELAX) {
-                        const long long g = grown_index<float>(n, sx, x, y, z);
-                        store_with_images(out32, n, sx, out32 + g, ex, ey, ez, v);
-                    } else {
-                        double* q = u64 + grown_index<double>(n, sxd, x, y, z);
-                        store_with_images(u64, n, sxd, q, ex, ey, ez, dadd(dd, (double)v));
-                    }
+                    zp0 = col[Sz];
+                    zp1 = act1 ? col[Sz + sx] : V(0);
                 }
-                zm = z_;
-                z_ = zp;
+                const V ym = pl[-RS], xm0 = pl[-1], xp0 = pl[1];
+                const V xm1 = pl[RS - 1], xp1 = pl[RS + 1], c1 = pl[RS], yp1 = pl[2 * RS];
+                const int ez = edge_code(z, n);
+                cell(ya, z, ey0, ez, i, zm0, zc0, zp0, xm0, xp0, ym, c1, r0, d0);
+                if (act1) cell(ya + 1, z, ey1, ez, i + n, zm1, zc1, zp1, xm1, xp1, zc0, yp1, r1, d1);
+                zm0 = zc0;
+                zc0 = zp0;
+                zm1 = zc1;
+                zc1 = zp1;
             }
             col += Sz;
             i += n * n;

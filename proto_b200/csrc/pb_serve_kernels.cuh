@@ -4,10 +4,13 @@
 // memory; the kernels are persistent (grid fixed, work read from the list), so a captured CUDA
 // graph of a whole cycle stays valid while solves come and go.
 //
-// Work units are grid rows (one (y, z) pair; a restriction's rows are coarse rows). A block takes
-// kSvRows consecutive rows, one warp per row, lanes striding along x (coalesced). Each item's rows
-// start at a multiple of kSvRows, so a chunk lies in one item: the block finds it with one binary
-// search over the phase's compact array of first rows.
+// Two kinds of work unit. The stencil phases (sweeps, the FP64 residual pass, the fused update)
+// take a CTA per tile of a level and stage its planes through shared memory (k_sv_ring). The
+// pointwise phases (restriction, prolongation, the first sweep from zero) take grid rows (one (y,
+// z) pair; a restriction's rows are coarse rows): a block takes kSvRows consecutive rows, one warp
+// per row, lanes striding along x (coalesced), and each item's rows start at a multiple of
+// kSvRows so a chunk lies in one item. Either way a block finds its item with one binary search
+// over the phase's compact array of first units.
 // The per-cell arithmetic is the single-solve solver's (same helpers, same order), so a solve's
 // result does not depend on what else is in the batch.
 #pragma once
@@ -71,13 +74,14 @@ __global__ void __launch_bounds__(kSvUnit) k_sv_phase(const SvItem* __restrict__
                                                       const long long* __restrict__ unit0,
                                                       const SvPhaseHeader* __restrict__ hdr, double* norms)
 {
+    static_assert(OP == SV_RELAX_FIRST || OP == SV_RESTRICT || OP == SV_PROLONG, "row phases only");
+    (void)norms;
     const int count = (int)hdr->count;
     const long long total = hdr->total;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (long long w0 = (long long)blockIdx.x * kSvRows; w0 < total; w0 += (long long)gridDim.x * kSvRows) {
         const SvItem& it = items[sv_find(unit0, count, w0)];
         const int row = (int)(w0 - it.unit0) + warp;
-        double m = 0.0;
         if (row < it.units) {
             const int n = it.k.n, sx = it.k.sx;
             if constexpr (OP == SV_RESTRICT) {
@@ -103,26 +107,7 @@ __global__ void __launch_bounds__(kSvUnit) k_sv_phase(const SvItem* __restrict__
                 const int ey = edge_code(y, n), ez = edge_code(z, n);
                 const long long g0 = grown_index<float>(n, sx, 0, y, z);   // valid cell x = 0 of the row
                 const long long i0 = (long long)row * n;                    // its n^3 index
-                if constexpr (OP == SV_RELAX || OP == SV_UPDATE) {
-                    const long long Sy = sx, Sz = (long long)sx * (n + 2);
-                    const long long gd0 = OP == SV_UPDATE ? grown_index<double>(n, it.sxd, 0, y, z) : 0;
-                    for (int x = lane; x < n; x += 32) {
-                        const long long g = g0 + x;
-                        float acc = 0.f;
-#pragma unroll
-                        for (int j = 0; j < ShapeLap7::NT; j++) {
-                            const long long o = ShapeLap7::off(j, 0) + Sy * ShapeLap7::off(j, 1) + Sz * ShapeLap7::off(j, 2);
-                            acc = dadd(acc, dmul(it.c.c[j], it.in[g + o]));
-                        }
-                        const float v = relax_value(it.k, acc, it.in[g], it.rhs[i0 + x], it.alpha);
-                        if constexpr (OP == SV_RELAX) {
-                            store_with_images(it.out, n, sx, it.out + g, edge_code(x, n), ey, ez, v);
-                        } else {
-                            double* q = it.u64 + gd0 + x;
-                            store_with_images(it.u64, n, it.sxd, q, edge_code(x, n), ey, ez, dadd(*q, (double)v));
-                        }
-                    }
-                } else if constexpr (OP == SV_RELAX_FIRST) {
+                if constexpr (OP == SV_RELAX_FIRST) {
                     for (int x = lane; x < n; x += 32)
                         store_with_images(it.out, n, sx, it.out + g0 + x, edge_code(x, n), ey, ez,
                                           relax_value(it.k, 0.f, 0.f, it.rhs[i0 + x], it.alpha));
@@ -132,47 +117,8 @@ __global__ void __launch_bounds__(kSvUnit) k_sv_phase(const SvItem* __restrict__
                         float* q = it.in + g0 + x;
                         store_with_images(it.in, n, sx, q, edge_code(x, n), ey, ez, dadd(*q, dmul(1.f, d[x / 2])));
                     }
-                } else if constexpr (OP == SV_K1) {
-                    // FP64 residual of u64, its max-norm, the FP32 right-hand side and the first FP32 sweep
-                    const int sxd = it.sxd;
-                    const long long Sy = sxd, Sz = (long long)sxd * (n + 2);
-                    const long long gd0 = grown_index<double>(n, sxd, 0, y, z);
-                    const float al = it.k.helm ? __double2float_rn(it.alpha64) : 0.f;
-                    for (int x = lane; x < n; x += 32) {
-                        const long long g = gd0 + x;
-                        double res;
-                        if (!it.k.helm) {
-                            res = dadd(0.0, it.f64[i0 + x]);
-#pragma unroll
-                            for (int j = 0; j < ShapeLap7::NT; j++) {
-                                const long long o = ShapeLap7::off(j, 0) + Sy * ShapeLap7::off(j, 1) + Sz * ShapeLap7::off(j, 2);
-                                res = dadd(res, dmul(it.c64.c[j], it.u64[g + o]));
-                            }
-                        } else {
-                            double lp = 0.0;
-#pragma unroll
-                            for (int j = 0; j < ShapeLap7::NT; j++) {
-                                const long long o = ShapeLap7::off(j, 0) + Sy * ShapeLap7::off(j, 1) + Sz * ShapeLap7::off(j, 2);
-                                lp = dadd(lp, dmul(it.c64.c[j], it.u64[g + o]));
-                            }
-                            res = dsub(it.f64[i0 + x], dsub(dmul(it.alpha64, it.u64[g]), dmul(it.beta64, lp)));
-                        }
-                        m = upd_abs(m, res);
-                        const float r32 = __double2float_rn(res);
-                        it.out[i0 + x] = r32;   // the level's rho
-                        store_with_images(it.in, n, sx, it.in + g0 + x, edge_code(x, n), ey, ez,
-                                          relax_value(it.k, 0.f, 0.f, r32, al));
-                    }
                 }
             }
-        }
-        if constexpr (OP == SV_K1) {
-            // a warp's row lies in one item: one max per warp, one atomic per warp
-            for (int o = 16; o > 0; o >>= 1) {
-                const double w = __shfl_down_sync(0xffffffffu, m, o);
-                m = (m < w) ? w : m;
-            }
-            if (lane == 0 && m > 0.0 && row < it.units) atomic_max_nonneg(norms + it.slot, m);
         }
     }
 }

@@ -44,6 +44,7 @@ MAX_ITER = 100
 CYCLES_PER_SOLVE = 16   # V(4,4) cycles this workload takes to 1e-10 (FP64, bitwise equal on CPU and GPU)
 STENCIL_BYTES = 8 * (258 ** 3 + 256 ** 3)          # algorithmic bytes of dst |= L(src), 256^3
 RELAX_BYTES = 24 * 256 ** 3                        # read phi, read rho, write phi_new
+SERVE_MAX_ACTIVE = 128                             # serving: solves in one batched cycle at most
 
 
 def measured_peaks():
@@ -354,14 +355,14 @@ def run_serving(pb, count):
     from proto_b200 import serving as S
     trace = S.make_trace(count=count)
     pool = S.rhs_pool([r["n"] for r in trace])
-    eng = pb.Serve(150 << 30, max_active=64, tol=1e-8)
-    ring = S._Ring([r["n"] for r in trace], 12)
+    eng = pb.Serve(150 << 30, max_active=SERVE_MAX_ACTIVE, tol=1e-8)
+    ring = S._Ring([r["n"] for r in trace], SERVE_MAX_ACTIVE // 4)
     warm = trace[:min(len(trace), 400)]
     S.serve_trace(pb, warm, pool, realtime=False, engine=eng, ring=ring)
     S.fp64_trace(pb, warm[:100], pool, realtime=False)
     out = {"workload": "%d requests, Poisson arrivals 200/s (seed 4), edge log-uniform [32,192] step 16, "
                        "Poisson/Helmholtz 50/50, alpha~U[0,1], 4 sine modes, tol 1e-8" % count,
-           "hbm_budget_gb": 150, "max_active": 64}
+           "hbm_budget_gb": 150, "max_active": SERVE_MAX_ACTIVE}
     for mode, rt in (("saturated", False), ("arrival_rate", True)):
         a, ka = S.serve_trace(pb, trace, pool, realtime=rt, keep=20, engine=eng, ring=ring)
         b, kb = S.fp64_trace(pb, trace, pool, realtime=rt, keep=20)

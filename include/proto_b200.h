@@ -250,9 +250,10 @@ int pb_fas_solve(pb_fas* m, const double* force, double* phi, int max_iter, doub
  * Periodic Poisson/Helmholtz solves of different edges, solved together: each admitted solve keeps
  * its hierarchy on the device; one pb_serve_step runs one mixed-precision V-cycle (FP32 cycle,
  * FP64 residual, correction and norm) for every in-flight solve, each cycle phase one launch for
- * all of them, the whole step one CUDA graph. Solves are admitted between steps while slots and
- * the HBM budget allow, and retired when their max-norm residual drops below tol times the first
- * one. Per solve the arithmetic is pb_mg's PB_MG_MIXED solver's (constant alpha, levels = every
+ * all of them, the whole step one CUDA graph. Solves are admitted between steps while the HBM
+ * budget allows (up to max_active at a time with their right-hand side on its way to the device,
+ * on a stream of its own), take a slot once the upload has landed and a slot is free, and are
+ * retired when their max-norm residual drops below tol times the first one. Per solve the arithmetic is pb_mg's PB_MG_MIXED solver's (constant alpha, levels = every
  * halving, bottom = nu_bottom sweeps), so each result is the same alone and in any mix.
  * An edge must halve down to <= 16 (n = m * 2^k with m <= 16). */
 enum { PB_SERVE_WAITING = 0, PB_SERVE_ACTIVE = 1, PB_SERVE_DONE = 2, PB_SERVE_FAILED = 3 };
@@ -279,8 +280,8 @@ int pb_serve_destroy(pb_serve* sv);
 int pb_serve_submit(pb_serve* sv, const pb_serve_request* q, long long* ticket);
 /* Admits what fits, runs one cycle for every in-flight solve and retires the finished ones; a
  * retired solve's result is copied to its out buffer in the background. *active counts solves in
- * flight plus results still on their way (keep stepping while it is non-zero); active / waiting
- * may be NULL. */
+ * flight plus results still on their way, *waiting the queued solves plus those whose right-hand
+ * side is still uploading (keep stepping while either is non-zero); active / waiting may be NULL. */
 int pb_serve_step(pb_serve* sv, int* active, int* waiting);
 /* Tickets completed since the last poll (up to cap): their results are in their out buffers. */
 int pb_serve_poll(pb_serve* sv, long long* tickets, int cap, int* n);

@@ -40,6 +40,7 @@ struct SvHier {
     double* f64 = nullptr;              // n^3 (also the staging buffer of the result)
     int sxd = 0;
     size_t bytes = 0;
+    void* slab = nullptr;               // one allocation holds every buffer above
 };
 
 struct SvSolve {
@@ -66,6 +67,13 @@ struct pb_serve {
     long long next_ticket = 1;
     std::map<long long, SvSolve> solves;
     std::deque<long long> waiting;
+    // admitted solves whose right-hand side is on its way to the device (upload stream); they take
+    // a slot once it has landed, so uploads overlap the cycles of the solves already in flight
+    struct Loading {
+        long long ticket;
+        cudaEvent_t landed;
+    };
+    std::deque<Loading> loading;
     std::vector<long long> slots;       // slot -> ticket (0: free)
     std::vector<long long> completed;   // tickets done since the last poll
     std::multimap<int, SvHier*> cache;  // idle hierarchies by edge
@@ -79,21 +87,24 @@ struct pb_serve {
     std::vector<Pending> pending;
     std::vector<cudaEvent_t> free_events;
     cudaStream_t cst = nullptr;         // copy stream for results
+    cudaStream_t ust = nullptr;         // upload stream for admitted solves
     size_t held = 0;                    // bytes of all hierarchies (busy and idle)
     // phase lists (device + host mirror)
     int max_phases = 0;
     SvItem* d_items = nullptr;
     long long* d_unit0 = nullptr;       // per phase: first rows of its items (compact, for the search)
     SvPhaseHeader* d_hdr = nullptr;
-    std::vector<SvItem> h_items;
-    std::vector<long long> h_unit0;
-    std::vector<SvPhaseHeader> h_hdr;
+    // host mirrors in pinned memory (the copies to the device are asynchronous; each step ends with
+    // a stream synchronisation, so a mirror is rebuilt only after its last copy has landed)
+    SvItem* h_items = nullptr;
+    long long* h_unit0 = nullptr;
+    SvPhaseHeader* h_hdr = nullptr;
     CoarseArgs<float>* d_cargs = nullptr;
     CoarseOffsets* d_coffs = nullptr;
     int* d_ccount = nullptr;
-    std::vector<CoarseArgs<float>> h_cargs;
-    int h_ccount = 0;
-    std::vector<CoarseOffsets> h_coffs;
+    CoarseArgs<float>* h_cargs = nullptr;
+    int* h_ccount = nullptr;
+    CoarseOffsets* h_coffs = nullptr;
     double* d_norms = nullptr;          // per slot: residual norm of the step
     double* d_r0 = nullptr;             // per slot: first residual norm
     double* h_norms = nullptr;          // pinned
@@ -125,53 +136,79 @@ bool edge_ok(int n)
 
 void hier_free(SvHier* h)
 {
-    for (size_t l = 0; l < h->phi0.size(); l++) {
-        cudaFree(h->phi0[l]);
-        cudaFree(h->phi1[l]);
-        cudaFree(h->rhs[l]);
-        cudaFree(h->alpha[l]);
-    }
-    cudaFree(h->u64);
-    cudaFree(h->f64);
+    cudaFree(h->slab);
     delete h;
+}
+
+// Walks the buffers of an n-edge hierarchy in slab order (256-byte aligned offsets): per level the
+// two grown FP32 solutions, rho and (edge <= 16) alpha, then the grown FP64 solution and the FP64
+// right-hand side. place(level, kind, offset, bytes) sees each; the return value is the slab size.
+template <class F>
+size_t hier_layout(int n, F&& place)
+{
+    size_t off = 0;
+    auto put = [&](int l, int kind, size_t b) {
+        place(l, kind, off, b);
+        off += (b + 255) / 256 * 256;
+    };
+    int l = 0;
+    for (int e = n;; e /= 2, l++) {
+        const size_t g = sizeof(float) * (size_t)grown_pitch<float>(e) * (e + 2) * (e + 2);
+        const size_t c = sizeof(float) * (size_t)e * e * e;
+        put(l, 0, g);
+        put(l, 1, g);
+        put(l, 2, c);
+        if (e <= kCoarseEdge) put(l, 3, c);
+        if (e % 2 != 0 || e == 1) break;
+    }
+    put(-1, 4, sizeof(double) * (size_t)grown_pitch<double>(n) * (n + 2) * (n + 2));
+    put(-1, 5, sizeof(double) * (size_t)n * n * n);
+    return off;
 }
 
 size_t hier_bytes(int n)
 {
-    size_t b = 0;
-    for (int e = n;; e /= 2) {
-        const size_t g = (size_t)grown_pitch<float>(e) * (e + 2) * (e + 2), c = (size_t)e * e * e;
-        b += 4 * (2 * g + c) + (e <= kCoarseEdge ? 4 * c : 0);
-        if (e % 2 != 0 || e == 1) break;
-    }
-    b += 8 * (size_t)grown_pitch<double>(n) * (n + 2) * (n + 2) + 8 * (size_t)n * n * n;
-    return b;
+    return hier_layout(n, [](int, int, size_t, size_t) {});
 }
 
+// One cudaMalloc per hierarchy (admission stays cheap); the FP32 solutions start at zero (their
+// ghost images included), set on stream st.
 SvHier* hier_alloc(int n, cudaStream_t st)
 {
     SvHier* h = new SvHier;
     h->n = n;
-    bool ok = true;
-    for (int e = n;; e /= 2) {
-        h->edge.push_back(e);
-        h->sx.push_back(grown_pitch<float>(e));
-        const size_t g = sizeof(float) * (size_t)h->sx.back() * (e + 2) * (e + 2), c = sizeof(float) * (size_t)e * e * e;
-        float *a = nullptr, *b = nullptr, *r = nullptr, *al = nullptr;
-        ok = ok && cudaMalloc(&a, g) == cudaSuccess && cudaMalloc(&b, g) == cudaSuccess && cudaMalloc(&r, c) == cudaSuccess;
-        if (ok && e <= kCoarseEdge) ok = cudaMalloc(&al, c) == cudaSuccess;
-        if (ok) ok = cudaMemsetAsync(a, 0, g, st) == cudaSuccess && cudaMemsetAsync(b, 0, g, st) == cudaSuccess;
-        h->phi0.push_back(a);
-        h->phi1.push_back(b);
-        h->rhs.push_back(r);
-        h->alpha.push_back(al);
-        if (e % 2 != 0 || e == 1) break;
+    const size_t total = hier_bytes(n);
+    if (cudaMalloc(&h->slab, total) != cudaSuccess) {
+        cudaGetLastError();
+        delete h;
+        return nullptr;
     }
+    unsigned char* base = static_cast<unsigned char*>(h->slab);
+    bool ok = true;
+    hier_layout(n, [&](int l, int kind, size_t off, size_t b) {
+        if (l >= (int)h->edge.size()) {
+            const int e = n >> l;
+            h->edge.push_back(e);
+            h->sx.push_back(grown_pitch<float>(e));
+            h->phi0.push_back(nullptr);
+            h->phi1.push_back(nullptr);
+            h->rhs.push_back(nullptr);
+            h->alpha.push_back(nullptr);
+        }
+        void* q = base + off;
+        switch (kind) {
+        case 0: h->phi0[l] = static_cast<float*>(q); break;
+        case 1: h->phi1[l] = static_cast<float*>(q); break;
+        case 2: h->rhs[l] = static_cast<float*>(q); break;
+        case 3: h->alpha[l] = static_cast<float*>(q); break;
+        case 4: h->u64 = static_cast<double*>(q); break;
+        default: h->f64 = static_cast<double*>(q); break;
+        }
+        if (kind <= 1) ok = ok && cudaMemsetAsync(q, 0, b, st) == cudaSuccess;
+    });
     h->nlev = (int)h->edge.size();
     h->sxd = grown_pitch<double>(n);
-    const size_t gd = sizeof(double) * (size_t)h->sxd * (n + 2) * (n + 2);
-    ok = ok && cudaMalloc(&h->u64, gd) == cudaSuccess && cudaMalloc(&h->f64, sizeof(double) * (size_t)n * n * n) == cudaSuccess;
-    h->bytes = hier_bytes(n);
+    h->bytes = total;
     if (!ok) {
         cudaGetLastError();
         hier_free(h);
@@ -319,11 +356,7 @@ static int build_lists(pb_serve* sv)
     sv->depth_now = D;
     const std::vector<PhaseSlot> plan = phase_plan(p, std::max(D, 1));
     const int cap = (int)p.max_active;
-    if (sv->h_items.size() != (size_t)sv->max_phases * cap) {
-        sv->h_items.assign((size_t)sv->max_phases * cap, SvItem{});
-        sv->h_unit0.assign((size_t)sv->max_phases * cap, 0);
-    }
-    sv->h_hdr.assign(sv->max_phases, SvPhaseHeader{0, 0});
+    for (int ph = 0; ph < sv->max_phases; ph++) sv->h_hdr[ph] = SvPhaseHeader{0, 0};
     const long long ctas = sv->grid;
     // per solve: the buffer index of each level's current solution as the plan advances
     std::vector<std::vector<int>> cur(act.size());
@@ -401,7 +434,7 @@ static int build_lists(pb_serve* sv)
             items.push_back(it);
         }
         const long long total = layout_items(items, is_staged(ps.op), ctas);
-        std::copy(items.begin(), items.end(), sv->h_items.begin() + ph * cap);
+        std::copy(items.begin(), items.end(), sv->h_items + ph * cap);
         for (size_t k = 0; k < items.size(); k++) sv->h_unit0[ph * cap + k] = items[k].unit0;
         sv->h_hdr[ph] = SvPhaseHeader{(long long)items.size(), total};
     }
@@ -431,13 +464,13 @@ static int build_lists(pb_serve* sv)
             items.push_back(it);
         }
         const long long total = layout_items(items, true, ctas);
-        std::copy(items.begin(), items.end(), sv->h_items.begin() + (size_t)ph * cap);
+        std::copy(items.begin(), items.end(), sv->h_items + (size_t)ph * cap);
         for (size_t k = 0; k < items.size(); k++) sv->h_unit0[(size_t)ph * cap + k] = items[k].unit0;
         sv->h_hdr[ph] = SvPhaseHeader{(long long)items.size(), total};
     }
     // coarse-cycle arguments (entry level = depth s.depth)
-    sv->h_cargs.assign(cap, CoarseArgs<float>{});
-    sv->h_coffs.assign(cap, CoarseOffsets{});
+    memset(sv->h_cargs, 0, sizeof(CoarseArgs<float>) * cap);
+    memset(sv->h_coffs, 0, sizeof(CoarseOffsets) * cap);
     int nc = 0;
     size_t smem_max = 0;
     for (size_t a = 0; a < act.size(); a++) {
@@ -478,18 +511,16 @@ static int build_lists(pb_serve* sv)
     (void)smem_max;
     // the phases of this depth's plan and the residual-pass slot (the last one)
     const size_t used = plan.size() * cap;
-    PB_CUDA(cudaMemcpyAsync(sv->d_items, sv->h_items.data(), sizeof(SvItem) * used, cudaMemcpyHostToDevice, sv->st));
-    PB_CUDA(cudaMemcpyAsync(sv->d_unit0, sv->h_unit0.data(), sizeof(long long) * used, cudaMemcpyHostToDevice, sv->st));
+    PB_CUDA(cudaMemcpyAsync(sv->d_items, sv->h_items, sizeof(SvItem) * used, cudaMemcpyHostToDevice, sv->st));
+    PB_CUDA(cudaMemcpyAsync(sv->d_unit0, sv->h_unit0, sizeof(long long) * used, cudaMemcpyHostToDevice, sv->st));
     const size_t last = (size_t)(sv->max_phases - 1) * cap;
-    PB_CUDA(cudaMemcpyAsync(sv->d_items + last, sv->h_items.data() + last, sizeof(SvItem) * cap, cudaMemcpyHostToDevice, sv->st));
-    PB_CUDA(cudaMemcpyAsync(sv->d_unit0 + last, sv->h_unit0.data() + last, sizeof(long long) * cap, cudaMemcpyHostToDevice, sv->st));
-    PB_CUDA(cudaMemcpyAsync(sv->d_hdr, sv->h_hdr.data(), sizeof(SvPhaseHeader) * sv->h_hdr.size(), cudaMemcpyHostToDevice, sv->st));
-    PB_CUDA(cudaMemcpyAsync(sv->d_cargs, sv->h_cargs.data(), sizeof(CoarseArgs<float>) * cap, cudaMemcpyHostToDevice, sv->st));
-    PB_CUDA(cudaMemcpyAsync(sv->d_coffs, sv->h_coffs.data(), sizeof(CoarseOffsets) * cap, cudaMemcpyHostToDevice, sv->st));
-    sv->h_ccount = nc;
-    PB_CUDA(cudaMemcpyAsync(sv->d_ccount, &sv->h_ccount, sizeof(int), cudaMemcpyHostToDevice, sv->st));
-    // (copies from pageable host memory return once the source is staged, so the mirrors may be
-    // rebuilt right away)
+    PB_CUDA(cudaMemcpyAsync(sv->d_items + last, sv->h_items + last, sizeof(SvItem) * cap, cudaMemcpyHostToDevice, sv->st));
+    PB_CUDA(cudaMemcpyAsync(sv->d_unit0 + last, sv->h_unit0 + last, sizeof(long long) * cap, cudaMemcpyHostToDevice, sv->st));
+    PB_CUDA(cudaMemcpyAsync(sv->d_hdr, sv->h_hdr, sizeof(SvPhaseHeader) * sv->max_phases, cudaMemcpyHostToDevice, sv->st));
+    PB_CUDA(cudaMemcpyAsync(sv->d_cargs, sv->h_cargs, sizeof(CoarseArgs<float>) * nc, cudaMemcpyHostToDevice, sv->st));
+    PB_CUDA(cudaMemcpyAsync(sv->d_coffs, sv->h_coffs, sizeof(CoarseOffsets) * nc, cudaMemcpyHostToDevice, sv->st));
+    *sv->h_ccount = nc;
+    PB_CUDA(cudaMemcpyAsync(sv->d_ccount, sv->h_ccount, sizeof(int), cudaMemcpyHostToDevice, sv->st));
     sv->lists_dirty = false;
     return PB_OK;
 }
@@ -532,16 +563,26 @@ static int enqueue_step(pb_serve* sv, int D, cudaStream_t st)
     return PB_OK;
 }
 
+static cudaEvent_t take_event(pb_serve* sv)
+{
+    if (sv->free_events.empty()) {
+        for (int k = 0; k < 8; k++) {
+            cudaEvent_t e;
+            if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return nullptr;
+            sv->free_events.push_back(e);
+        }
+    }
+    cudaEvent_t e = sv->free_events.back();
+    sv->free_events.pop_back();
+    return e;
+}
+
+// Admission, in request order, while the HBM budget allows and fewer than max_active solves are
+// loading: the solve takes a hierarchy (a cached one of its edge, else a new one, dropping idle
+// hierarchies of other edges to make room) and its right-hand side goes up on the upload stream.
 static int admit(pb_serve* sv)
 {
-    while (!sv->waiting.empty()) {
-        int slot = -1;
-        for (int i = 0; i < (int)sv->slots.size(); i++)
-            if (!sv->slots[i]) {
-                slot = i;
-                break;
-            }
-        if (slot < 0) return PB_OK;
+    while (!sv->waiting.empty() && (int)sv->loading.size() < sv->p.max_active) {
         SvSolve& s = sv->solves[sv->waiting.front()];
         const int n = s.req.n;
         SvHier* h = nullptr;
@@ -559,30 +600,63 @@ static int admit(pb_serve* sv)
                 sv->cache.erase(v);
             }
             if (sv->held + need > (size_t)sv->p.hbm_budget) return PB_OK;   // wait for memory
-            h = hier_alloc(n, sv->st);
+            h = hier_alloc(n, sv->ust);
             if (!h) return PB_OK;
             sv->held += h->bytes;
         }
+        cudaEvent_t landed = take_event(sv);
+        if (!landed) {
+            sv->cache.insert({n, h});
+            return PB_ERR_CUDA;
+        }
         sv->waiting.pop_front();
         s.h = h;
-        s.slot = slot;
         s.state = PB_SERVE_ACTIVE;
         s.depth = batched_depth(h);
         s.alpha_lv = level_alphas(s.req.alpha, h->nlev);
-        s.fresh = true;
-        sv->slots[slot] = s.ticket;
         // initial guess zero, right-hand side in; constant alpha on the coarse levels
         const size_t n3 = (size_t)n * n * n;
-        PB_CUDA(cudaMemsetAsync(h->u64, 0, sizeof(double) * (size_t)h->sxd * (n + 2) * (n + 2), sv->st));
-        PB_CUDA(cudaMemcpyAsync(h->f64, s.req.rhs, sizeof(double) * n3, cudaMemcpyHostToDevice, sv->st));
+        PB_CUDA(cudaMemsetAsync(h->u64, 0, sizeof(double) * (size_t)h->sxd * (n + 2) * (n + 2), sv->ust));
+        PB_CUDA(cudaMemcpyAsync(h->f64, s.req.rhs, sizeof(double) * n3, cudaMemcpyHostToDevice, sv->ust));
         if (s.req.form == PB_MG_HELMHOLTZ)
             for (int d = 0; d < h->nlev; d++)
                 if (h->alpha[d]) {
                     const long long c = (long long)h->edge[d] * h->edge[d] * h->edge[d];
-                    k_sv_fill<<<grid_for(c, 256), 256, 0, sv->st>>>(h->alpha[d], c, s.alpha_lv[d]);
+                    k_sv_fill<<<grid_for(c, 256), 256, 0, sv->ust>>>(h->alpha[d], c, s.alpha_lv[d]);
                     PB_LAUNCH_CHECK();
                 }
+        PB_CUDA(cudaEventRecord(landed, sv->ust));
+        sv->loading.push_back({s.ticket, landed});
+    }
+    return PB_OK;
+}
+
+// Loaded solves take free slots in admission order. With nothing in flight the oldest upload is
+// waited for, so a step always has work once anything is loading.
+static int join(pb_serve* sv)
+{
+    bool any = false;
+    for (long long t : sv->slots) any = any || t;
+    while (!sv->loading.empty()) {
+        int slot = -1;
+        for (int i = 0; i < (int)sv->slots.size(); i++)
+            if (!sv->slots[i]) {
+                slot = i;
+                break;
+            }
+        if (slot < 0) return PB_OK;
+        const pb_serve::Loading q = sv->loading.front();
+        cudaError_t r = any ? cudaEventQuery(q.landed) : cudaEventSynchronize(q.landed);
+        if (r == cudaErrorNotReady) return PB_OK;
+        if (r != cudaSuccess) { set_cuda_error(r); return PB_ERR_CUDA; }
+        sv->loading.pop_front();
+        sv->free_events.push_back(q.landed);
+        SvSolve& s = sv->solves[q.ticket];
+        s.slot = slot;
+        s.fresh = true;
+        sv->slots[slot] = s.ticket;
         sv->lists_dirty = true;
+        any = true;
     }
     return PB_OK;
 }
@@ -594,18 +668,12 @@ static int retire(pb_serve* sv, SvSolve& s, int state)
     SvHier* h = s.h;
     const int n = h->n;
     const size_t n3 = (size_t)n * n * n;
-    cudaEvent_t packed, done;
-    if (sv->free_events.size() < 2) {
-        for (int k = 0; k < 8; k++) {
-            cudaEvent_t e;
-            PB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-            sv->free_events.push_back(e);
-        }
+    cudaEvent_t packed = take_event(sv);
+    cudaEvent_t done = packed ? take_event(sv) : nullptr;
+    if (!done) {
+        if (packed) sv->free_events.push_back(packed);
+        return PB_ERR_CUDA;
     }
-    packed = sv->free_events.back();
-    sv->free_events.pop_back();
-    done = sv->free_events.back();
-    sv->free_events.pop_back();
     k_sv_pack_out<<<grid_for((long long)n3, 256), 256, 0, sv->st>>>(h->u64, h->f64, n, h->sxd);
     PB_LAUNCH_CHECK();
     PB_CUDA(cudaEventRecord(packed, sv->st));
@@ -659,6 +727,13 @@ int pb_serve_create(const pb_serve_params* p, pb_serve** out)
     const size_t cap = (size_t)p->max_active;
     bool ok = cudaStreamCreateWithFlags(&sv->st, cudaStreamNonBlocking) == cudaSuccess &&
               cudaStreamCreateWithFlags(&sv->cst, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&sv->ust, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaMallocHost(&sv->h_items, sizeof(SvItem) * cap * sv->max_phases) == cudaSuccess &&
+              cudaMallocHost(&sv->h_unit0, sizeof(long long) * cap * sv->max_phases) == cudaSuccess &&
+              cudaMallocHost(&sv->h_hdr, sizeof(SvPhaseHeader) * sv->max_phases) == cudaSuccess &&
+              cudaMallocHost(&sv->h_cargs, sizeof(CoarseArgs<float>) * cap) == cudaSuccess &&
+              cudaMallocHost(&sv->h_coffs, sizeof(CoarseOffsets) * cap) == cudaSuccess &&
+              cudaMallocHost(&sv->h_ccount, sizeof(int)) == cudaSuccess &&
               cudaMalloc(&sv->d_items, sizeof(SvItem) * cap * sv->max_phases) == cudaSuccess &&
               cudaMalloc(&sv->d_unit0, sizeof(long long) * cap * sv->max_phases) == cudaSuccess &&
               cudaMalloc(&sv->d_hdr, sizeof(SvPhaseHeader) * sv->max_phases) == cudaSuccess &&
@@ -699,6 +774,8 @@ int pb_serve_destroy(pb_serve* sv)
     if (!sv) return PB_OK;
     if (sv->st) cudaStreamSynchronize(sv->st);
     if (sv->cst) cudaStreamSynchronize(sv->cst);
+    if (sv->ust) cudaStreamSynchronize(sv->ust);
+    for (auto& q : sv->loading) cudaEventDestroy(q.landed);
     for (auto& q : sv->pending) {
         hier_free(q.h);
         cudaEventDestroy(q.done);
@@ -718,8 +795,15 @@ int pb_serve_destroy(pb_serve* sv)
     cudaFree(sv->d_r0);
     cudaFreeHost(sv->h_norms);
     cudaFreeHost(sv->h_r0);
+    cudaFreeHost(sv->h_items);
+    cudaFreeHost(sv->h_unit0);
+    cudaFreeHost(sv->h_hdr);
+    cudaFreeHost(sv->h_cargs);
+    cudaFreeHost(sv->h_coffs);
+    cudaFreeHost(sv->h_ccount);
     if (sv->st) cudaStreamDestroy(sv->st);
     if (sv->cst) cudaStreamDestroy(sv->cst);
+    if (sv->ust) cudaStreamDestroy(sv->ust);
     delete sv;
     return PB_OK;
 }
@@ -756,6 +840,7 @@ int pb_serve_step(pb_serve* sv, int* active, int* waiting)
     int e;
     if ((e = drain(sv, false)) != PB_OK) return e;
     if ((e = admit(sv)) != PB_OK) return e;
+    if ((e = join(sv)) != PB_OK) return e;
     sv->t_stage[0] += lap(t0);
     bool any = false;
     for (long long t : sv->slots) any = any || t;
@@ -818,7 +903,7 @@ int pb_serve_step(pb_serve* sv, int* active, int* waiting)
     int na = (int)sv->pending.size();
     for (long long t : sv->slots) na += t ? 1 : 0;
     if (active) *active = na;
-    if (waiting) *waiting = (int)sv->waiting.size();
+    if (waiting) *waiting = (int)(sv->waiting.size() + sv->loading.size());
     return PB_OK;
 }
 

@@ -251,9 +251,12 @@ int pb_fas_solve(pb_fas* m, const double* force, double* phi, int max_iter, doub
  * its hierarchy on the device; one pb_serve_step runs one mixed-precision V-cycle (FP32 cycle,
  * FP64 residual, correction and norm) for every in-flight solve, each cycle phase one launch for
  * all of them, the whole step one CUDA graph. Solves are admitted between steps while the HBM
- * budget allows (up to max_active at a time with their right-hand side on its way to the device,
- * on a stream of its own), take a slot once the upload has landed and a slot is free, and are
- * retired when their max-norm residual drops below tol times the first one. Per solve the arithmetic is pb_mg's PB_MG_MIXED solver's (constant alpha, levels = every
+ * budget allows, up to max(2, max_active / 4) at a time with their right-hand side on its way to
+ * the device (an upload stream of its own; hierarchies come from a stream-ordered pool of the
+ * engine). An admitted solve takes a free slot in the same step when no requests are queued (light
+ * load), else in the first step after its upload has landed (uploads overlap the running cycles).
+ * Solves are retired when their max-norm residual drops below tol times the first one. Per solve
+ * the arithmetic is pb_mg's PB_MG_MIXED solver's (constant alpha, levels = every
  * halving, bottom = nu_bottom sweeps), so each result is the same alone and in any mix.
  * An edge must halve down to <= 16 (n = m * 2^k with m <= 16). */
 enum { PB_SERVE_WAITING = 0, PB_SERVE_ACTIVE = 1, PB_SERVE_DONE = 2, PB_SERVE_FAILED = 3 };

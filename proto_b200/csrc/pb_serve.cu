@@ -88,6 +88,7 @@ struct pb_serve {
     std::vector<cudaEvent_t> free_events;
     cudaStream_t cst = nullptr;         // copy stream for results
     cudaStream_t ust = nullptr;         // upload stream for admitted solves
+    cudaMemPool_t pool = nullptr;       // device memory of the hierarchies
     size_t held = 0;                    // bytes of all hierarchies (busy and idle)
     // phase lists (device + host mirror)
     int max_phases = 0;
@@ -113,7 +114,8 @@ struct pb_serve {
     std::map<int, cudaGraphExec_t> graphs;
     bool lists_dirty = true;
     int depth_now = 0;
-    int grid = 0;                       // persistent grid of the phase kernels
+    int grid = 0;                       // persistent grid of the row-phase kernels
+    int ring_grid = 0;                  // persistent grid of the staged kernels: every CTA resident
     size_t coarse_smem = 0;
     double t_stage[5] = {0, 0, 0, 0, 0};   // host seconds: admit, lists, residual pass, cycle, retire
     long long steps = 0;
@@ -134,9 +136,12 @@ bool edge_ok(int n)
     return e <= kCoarseEdge;
 }
 
-void hier_free(SvHier* h)
+// Hierarchies come from the engine's own stream-ordered memory pool (release threshold = the HBM
+// budget): freed slabs stay with the pool for later admissions, and neither allocating nor freeing
+// waits for the device.
+void hier_free(SvHier* h, cudaStream_t st)
 {
-    cudaFree(h->slab);
+    cudaFreeAsync(h->slab, st);
     delete h;
 }
 
@@ -171,14 +176,14 @@ size_t hier_bytes(int n)
     return hier_layout(n, [](int, int, size_t, size_t) {});
 }
 
-// One cudaMalloc per hierarchy (admission stays cheap); the FP32 solutions start at zero (their
-// ghost images included), set on stream st.
-SvHier* hier_alloc(int n, cudaStream_t st)
+// One allocation per hierarchy, ordered on stream st; the FP32 solutions start at zero (their ghost
+// images included), set on st as well.
+SvHier* hier_alloc(int n, cudaMemPool_t pool, cudaStream_t st)
 {
     SvHier* h = new SvHier;
     h->n = n;
     const size_t total = hier_bytes(n);
-    if (cudaMalloc(&h->slab, total) != cudaSuccess) {
+    if (cudaMallocFromPoolAsync(&h->slab, total, pool, st) != cudaSuccess) {
         cudaGetLastError();
         delete h;
         return nullptr;
@@ -211,10 +216,23 @@ SvHier* hier_alloc(int n, cudaStream_t st)
     h->bytes = total;
     if (!ok) {
         cudaGetLastError();
-        hier_free(h);
+        hier_free(h, st);
         return nullptr;
     }
     return h;
+}
+
+bool make_pool(int device, size_t keep, cudaMemPool_t* out)
+{
+    cudaMemPoolProps pp;
+    memset(&pp, 0, sizeof(pp));
+    pp.allocType = cudaMemAllocationTypePinned;
+    pp.handleTypes = cudaMemHandleTypeNone;
+    pp.location.type = cudaMemLocationTypeDevice;
+    pp.location.id = device;
+    if (cudaMemPoolCreate(out, &pp) != cudaSuccess) return false;
+    uint64_t thr = keep;
+    return cudaMemPoolSetAttribute(*out, cudaMemPoolAttrReleaseThreshold, &thr) == cudaSuccess;
 }
 
 int batched_depth(const SvHier* h)
@@ -357,7 +375,6 @@ static int build_lists(pb_serve* sv)
     const std::vector<PhaseSlot> plan = phase_plan(p, std::max(D, 1));
     const int cap = (int)p.max_active;
     for (int ph = 0; ph < sv->max_phases; ph++) sv->h_hdr[ph] = SvPhaseHeader{0, 0};
-    const long long ctas = sv->grid;
     // per solve: the buffer index of each level's current solution as the plan advances
     std::vector<std::vector<int>> cur(act.size());
     for (size_t a = 0; a < act.size(); a++) {
@@ -433,7 +450,7 @@ static int build_lists(pb_serve* sv)
             }
             items.push_back(it);
         }
-        const long long total = layout_items(items, is_staged(ps.op), ctas);
+        const long long total = layout_items(items, is_staged(ps.op), is_staged(ps.op) ? sv->ring_grid : sv->grid);
         std::copy(items.begin(), items.end(), sv->h_items + ph * cap);
         for (size_t k = 0; k < items.size(); k++) sv->h_unit0[ph * cap + k] = items[k].unit0;
         sv->h_hdr[ph] = SvPhaseHeader{(long long)items.size(), total};
@@ -463,7 +480,7 @@ static int build_lists(pb_serve* sv)
             it.c64 = lap7_coefs<double>(helm ? hs : -hs);
             items.push_back(it);
         }
-        const long long total = layout_items(items, true, ctas);
+        const long long total = layout_items(items, true, sv->ring_grid);
         std::copy(items.begin(), items.end(), sv->h_items + (size_t)ph * cap);
         for (size_t k = 0; k < items.size(); k++) sv->h_unit0[(size_t)ph * cap + k] = items[k].unit0;
         sv->h_hdr[ph] = SvPhaseHeader{(long long)items.size(), total};
@@ -531,12 +548,12 @@ static int launch_phase(pb_serve* sv, int slot, int op, double* norms, cudaStrea
     const long long* u0 = sv->d_unit0 + (size_t)slot * sv->p.max_active;
     const SvPhaseHeader* hdr = sv->d_hdr + slot;
     switch (op) {
-    case SV_RELAX: k_sv_ring<SV_RELAX, float><<<sv->grid, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
+    case SV_RELAX: k_sv_ring<SV_RELAX, float><<<sv->ring_grid, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
     case SV_RELAX_FIRST: k_sv_phase<SV_RELAX_FIRST><<<sv->grid, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
     case SV_RESTRICT: k_sv_phase<SV_RESTRICT><<<sv->grid, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
     case SV_PROLONG: k_sv_phase<SV_PROLONG><<<sv->grid, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
-    case SV_K1: k_sv_ring<SV_K1, double><<<sv->grid, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
-    case SV_UPDATE: k_sv_ring<SV_UPDATE, float><<<sv->grid, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
+    case SV_K1: k_sv_ring<SV_K1, double><<<sv->ring_grid, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
+    case SV_UPDATE: k_sv_ring<SV_UPDATE, float><<<sv->ring_grid, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
     default: return PB_ERR_ARG;
     }
     PB_LAUNCH_CHECK();
@@ -577,12 +594,14 @@ static cudaEvent_t take_event(pb_serve* sv)
     return e;
 }
 
-// Admission, in request order, while the HBM budget allows and fewer than max_active solves are
-// loading: the solve takes a hierarchy (a cached one of its edge, else a new one, dropping idle
+// Admission, in request order, while the HBM budget allows and fewer than max(2, max_active / 4)
+// solves are loading (a few steps' worth of retirements: more would only hold hierarchies idle):
+// the solve takes a hierarchy (a cached one of its edge, else a new one, dropping idle
 // hierarchies of other edges to make room) and its right-hand side goes up on the upload stream.
 static int admit(pb_serve* sv)
 {
-    while (!sv->waiting.empty() && (int)sv->loading.size() < sv->p.max_active) {
+    const int max_loading = std::max(2, sv->p.max_active / 4);
+    while (!sv->waiting.empty() && (int)sv->loading.size() < max_loading) {
         SvSolve& s = sv->solves[sv->waiting.front()];
         const int n = s.req.n;
         SvHier* h = nullptr;
@@ -596,11 +615,11 @@ static int admit(pb_serve* sv)
             while (sv->held + need > (size_t)sv->p.hbm_budget && !sv->cache.empty()) {
                 auto v = sv->cache.begin();
                 sv->held -= v->second->bytes;
-                hier_free(v->second);
+                hier_free(v->second, sv->ust);
                 sv->cache.erase(v);
             }
             if (sv->held + need > (size_t)sv->p.hbm_budget) return PB_OK;   // wait for memory
-            h = hier_alloc(n, sv->ust);
+            h = hier_alloc(n, sv->pool, sv->ust);
             if (!h) return PB_OK;
             sv->held += h->bytes;
         }
@@ -631,12 +650,15 @@ static int admit(pb_serve* sv)
     return PB_OK;
 }
 
-// Loaded solves take free slots in admission order. With nothing in flight the oldest upload is
-// waited for, so a step always has work once anything is loading.
+// Loaded solves take free slots in admission order. Under a backlog (requests still queued) a solve
+// whose upload has not landed waits for the next step, so uploads overlap the running cycles; with
+// no backlog, or nothing in flight, the upload is waited for and the solve joins this step (light
+// load: latency first).
 static int join(pb_serve* sv)
 {
     bool any = false;
     for (long long t : sv->slots) any = any || t;
+    const bool backlog = !sv->waiting.empty();
     while (!sv->loading.empty()) {
         int slot = -1;
         for (int i = 0; i < (int)sv->slots.size(); i++)
@@ -646,7 +668,7 @@ static int join(pb_serve* sv)
             }
         if (slot < 0) return PB_OK;
         const pb_serve::Loading q = sv->loading.front();
-        cudaError_t r = any ? cudaEventQuery(q.landed) : cudaEventSynchronize(q.landed);
+        cudaError_t r = (any && backlog) ? cudaEventQuery(q.landed) : cudaEventSynchronize(q.landed);
         if (r == cudaErrorNotReady) return PB_OK;
         if (r != cudaSuccess) { set_cuda_error(r); return PB_ERR_CUDA; }
         sv->loading.pop_front();
@@ -728,6 +750,7 @@ int pb_serve_create(const pb_serve_params* p, pb_serve** out)
     bool ok = cudaStreamCreateWithFlags(&sv->st, cudaStreamNonBlocking) == cudaSuccess &&
               cudaStreamCreateWithFlags(&sv->cst, cudaStreamNonBlocking) == cudaSuccess &&
               cudaStreamCreateWithFlags(&sv->ust, cudaStreamNonBlocking) == cudaSuccess &&
+              make_pool(sv->device, (size_t)p->hbm_budget, &sv->pool) &&
               cudaMallocHost(&sv->h_items, sizeof(SvItem) * cap * sv->max_phases) == cudaSuccess &&
               cudaMallocHost(&sv->h_unit0, sizeof(long long) * cap * sv->max_phases) == cudaSuccess &&
               cudaMallocHost(&sv->h_hdr, sizeof(SvPhaseHeader) * sv->max_phases) == cudaSuccess &&
@@ -746,6 +769,13 @@ int pb_serve_create(const pb_serve_params* p, pb_serve** out)
               cudaMallocHost(&sv->h_r0, sizeof(double) * cap) == cudaSuccess;
     if (ok) {
         sv->grid = cached_sm_count() * 8;
+        // the staged kernels take whole units per CTA: a grid of exactly the resident CTAs spreads
+        // the units evenly (a larger one would run in partial waves)
+        int o1 = 0, o2 = 0, o3 = 0;
+        ok = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o1, k_sv_ring<SV_RELAX, float>, kSvUnit, 0) == cudaSuccess &&
+             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o2, k_sv_ring<SV_K1, double>, kSvUnit, 0) == cudaSuccess &&
+             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o3, k_sv_ring<SV_UPDATE, float>, kSvUnit, 0) == cudaSuccess;
+        sv->ring_grid = cached_sm_count() * std::max(1, std::min(o1, std::min(o2, o3)));
         // coarse part: the largest arena (edge 16, Helmholtz) fits in shared memory
         CoarseArgs<float> ca;
         memset(&ca, 0, sizeof(ca));
@@ -757,7 +787,7 @@ int pb_serve_create(const pb_serve_params* p, pb_serve** out)
             ca.lv[i].k.sx = grown_pitch<float>(e);
         }
         sv->coarse_smem = coarse_smem_layout(ca, 1, nullptr);
-        ok = cudaFuncSetAttribute(k_coarse_cycle_batch<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        ok = ok && cudaFuncSetAttribute(k_coarse_cycle_batch<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)sv->coarse_smem) == cudaSuccess;
     }
     if (!ok) {
@@ -777,14 +807,16 @@ int pb_serve_destroy(pb_serve* sv)
     if (sv->ust) cudaStreamSynchronize(sv->ust);
     for (auto& q : sv->loading) cudaEventDestroy(q.landed);
     for (auto& q : sv->pending) {
-        hier_free(q.h);
+        hier_free(q.h, sv->ust);
         cudaEventDestroy(q.done);
     }
     for (cudaEvent_t e : sv->free_events) cudaEventDestroy(e);
     for (auto& g : sv->graphs) cudaGraphExecDestroy(g.second);
     for (auto& s : sv->solves)
-        if (s.second.h) hier_free(s.second.h);
-    for (auto& c : sv->cache) hier_free(c.second);
+        if (s.second.h) hier_free(s.second.h, sv->ust);
+    for (auto& c : sv->cache) hier_free(c.second, sv->ust);
+    if (sv->ust) cudaStreamSynchronize(sv->ust);
+    if (sv->pool) cudaMemPoolDestroy(sv->pool);
     cudaFree(sv->d_items);
     cudaFree(sv->d_unit0);
     cudaFree(sv->d_hdr);

@@ -124,15 +124,17 @@ __global__ void __launch_bounds__(kSvUnit) k_sv_phase(const SvItem* __restrict__
 }
 
 // The stencil phases (sweep, FP64 residual pass, last sweep + FP64 correction) with a CTA per
-// unit = (item, 32 x 16 tile of a level, chunk of zd planes); each thread owns two cells, (x, y)
-// and (x, y + 1). Per plane the tile and its one-cell x/y halo are staged into a ring of kSvRing
+// unit = (item, 32 x 16 tile of a level, chunk of zd planes); each thread owns kSvYC cells in
+// consecutive rows, (x, y) .. (x, y + kSvYC - 1), so each thread carries that many independent
+// accumulation chains and the per-plane barrier and staging are shared by as many cells. Per plane the tile and its one-cell x/y halo are staged into a ring of kSvRing
 // shared-memory planes by 16-byte cp.async copies (whole 16-byte chunks of grown rows: they never
 // cross a row's pitch, so every copy stays inside the level's buffer), kSvLead planes ahead of
 // the plane being computed; z neighbours come from register windows fed from the ring. Pointwise
 // inputs (rhs, f, u64) are loaded at the top of the plane so their latency overlaps the wait.
 // Terms are summed in the Laplacian's insertion order with the single-solve solver's epilogue
 // arithmetic, so results are bitwise its.
-constexpr int kSvTX = 32, kSvTY = 2 * (kSvUnit / 32);    // 32 x 16 cells, two per thread (in y)
+constexpr int kSvYC = 2;                                  // cells per thread (consecutive rows)
+constexpr int kSvTX = 32, kSvTY = kSvYC * (kSvUnit / 32); // 32 x 16 cells
 constexpr int kSvRowStride = 36;                          // staged row: grown x0 .. x0+35 (34 used)
 constexpr int kSvPlane = kSvRowStride * (kSvTY + 2);
 constexpr int kSvLead = 1 + 3, kSvRing = kSvLead + 1;
@@ -215,22 +217,23 @@ __global__ void __launch_bounds__(kSvUnit, 3) k_sv_ring(const SvItem* __restrict
         };
 #pragma unroll
         for (int q = 0; q < L; q++) stage(z0 + q, q);
-        const int x = x0 + lane, ya = y0 + 2 * warp;
-        const bool act0 = x < n && ya < n, act1 = x < n && ya + 1 < n;
-        const V* col = src + (long long)grown_index<V>(n, sx, act0 ? x : 0, act0 ? ya : 0, z0);   // (x, ya, z0)
-        V zm0 = V(0), zc0 = V(0), zm1 = V(0), zc1 = V(0);
-        if (act0) {
-            zm0 = col[-Sz];
-            zc0 = col[0];
+        constexpr int YC = kSvYC;
+        const int x = x0 + lane, ya = y0 + YC * warp;      // this thread's cells: (x, ya + r), r < YC
+        const bool xin = x < n;
+        const V* col = src + (long long)grown_index<V>(n, sx, xin ? x : 0, ya < n ? ya : 0, z0);   // (x, ya, z0)
+        bool act[YC];
+        int ey[YC];
+        V zm[YC], zc[YC];
+#pragma unroll
+        for (int r = 0; r < YC; r++) {
+            act[r] = xin && ya + r < n;
+            ey[r] = act[r] ? edge_code(ya + r, n) : 0;
+            zm[r] = act[r] ? col[r * sx - Sz] : V(0);
+            zc[r] = act[r] ? col[r * sx] : V(0);
         }
-        if (act1) {
-            zm1 = col[sx - Sz];
-            zc1 = col[sx];
-        }
-        const int ex = act0 ? edge_code(x, n) : 0;
-        const int ey0 = act0 ? edge_code(ya, n) : 0, ey1 = act1 ? edge_code(ya + 1, n) : 0;
-        const int cidx = (2 * warp + 1) * RS + lane + 1;   // cell (x, ya) in a ring plane
-        int i = act0 ? x + n * (ya + n * z0) : 0;          // (x, ya, z) in the n^3 fields
+        const int ex = xin ? edge_code(x, n) : 0;
+        const int cidx = (YC * warp + 1) * RS + lane + 1;  // cell (x, ya) in a ring plane
+        int i = act[0] ? x + n * (ya + n * z0) : 0;        // (x, ya, z) in the n^3 fields
         double m = 0.0;
         // one cell: the stencil taps, the plane's pointwise inputs and the outputs of this phase
         auto cell = [&](int yy, int zz, int ey, int ez, int ii, V zm, V zc, V zp, V xm, V xp, V ym, V yp, float rr,
@@ -286,43 +289,51 @@ __global__ void __launch_bounds__(kSvUnit, 3) k_sv_ring(const SvItem* __restrict
         };
         int qz = 0;
         for (int z = z0; z < z1; z++) {
-            float r0 = 0.f, r1 = 0.f;
-            double d0 = 0.0, d1 = 0.0;
-            if constexpr (OP == SV_K1) {
-                if (act0) d0 = f64[i];
-                if (act1) d1 = f64[i + n];
-            } else {
-                if (act0) r0 = rhs[i];
-                if (act1) r1 = rhs[i + n];
-            }
-            if constexpr (OP == SV_UPDATE) {
-                if (act0) d0 = u64[grown_index<double>(n, sxd, x, ya, z)];
-                if (act1) d1 = u64[grown_index<double>(n, sxd, x, ya + 1, z)];
+            float rr[YC];
+            double dd[YC];
+#pragma unroll
+            for (int r = 0; r < YC; r++) {
+                rr[r] = 0.f;
+                dd[r] = 0.0;
+                if constexpr (OP == SV_K1) {
+                    if (act[r]) dd[r] = f64[i + r * n];
+                } else {
+                    if (act[r]) rr[r] = rhs[i + r * n];
+                }
+                if constexpr (OP == SV_UPDATE) {
+                    if (act[r]) dd[r] = u64[grown_index<double>(n, sxd, x, ya + r, z)];
+                }
             }
             cp_async_wait<L - 2>();   // this thread's copies of plane z + 1 have landed
             __syncthreads();          // everyone's have; everyone is done with plane z - 1
             stage(z + L, qz == 0 ? Q - 1 : qz - 1);
-            if (act0) {
+            if (act[0]) {
                 int q1 = qz + 1;
                 if (q1 >= Q) q1 -= Q;
                 const V* pl = ring + qz * PM + cidx;
-                V zp0, zp1;
+                V zp[YC];
                 if (z + 1 < z1) {
-                    zp0 = ring[q1 * PM + cidx];
-                    zp1 = ring[q1 * PM + cidx + RS];
+#pragma unroll
+                    for (int r = 0; r < YC; r++) zp[r] = ring[q1 * PM + cidx + r * RS];
                 } else {
-                    zp0 = col[Sz];
-                    zp1 = act1 ? col[Sz + sx] : V(0);
+#pragma unroll
+                    for (int r = 0; r < YC; r++) zp[r] = act[r] ? col[Sz + r * sx] : V(0);
                 }
-                const V ym = pl[-RS], xm0 = pl[-1], xp0 = pl[1];
-                const V xm1 = pl[RS - 1], xp1 = pl[RS + 1], c1 = pl[RS], yp1 = pl[2 * RS];
                 const int ez = edge_code(z, n);
-                cell(ya, z, ey0, ez, i, zm0, zc0, zp0, xm0, xp0, ym, c1, r0, d0);
-                if (act1) cell(ya + 1, z, ey1, ez, i + n, zm1, zc1, zp1, xm1, xp1, zc0, yp1, r1, d1);
-                zm0 = zc0;
-                zc0 = zp0;
-                zm1 = zc1;
-                zc1 = zp1;
+#pragma unroll
+                for (int r = 0; r < YC; r++) {
+                    if (!act[r]) break;
+                    // y neighbours: this thread's rows from registers, the tile's edge rows from the ring
+                    const V ym = r == 0 ? pl[-RS] : zc[r - 1];
+                    const V yp = (r + 1 < YC && act[r + 1]) ? zc[r + 1] : pl[(r + 1) * RS];
+                    cell(ya + r, z, ey[r], ez, i + r * n, zm[r], zc[r], zp[r], pl[r * RS - 1], pl[r * RS + 1], ym, yp,
+                         rr[r], dd[r]);
+                }
+#pragma unroll
+                for (int r = 0; r < YC; r++) {
+                    zm[r] = zc[r];
+                    zc[r] = zp[r];
+                }
             }
             col += Sz;
             i += n * n;

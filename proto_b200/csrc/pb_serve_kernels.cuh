@@ -234,9 +234,36 @@ __global__ void __launch_bounds__(kSvUnit, 3) k_sv_ring(const SvItem* __restrict
         const int ex = xin ? edge_code(x, n) : 0;
         const int cidx = (YC * warp + 1) * RS + lane + 1;  // cell (x, ya) in a ring plane
         int i = act[0] ? x + n * (ya + n * z0) : 0;        // (x, ya, z) in the n^3 fields
+        // the grown field this phase writes (RELAX: out32, K1: in32, UPDATE: u64): cell (x, ya, z0),
+        // advanced one plane per z step, and the offsets of the periodic images of this thread's
+        // cells (x and y per thread and row, z per plane; 0 where there is none)
+        using Wt = std::conditional_t<OP == SV_UPDATE, double, float>;
+        Wt* const wbase = OP == SV_UPDATE ? reinterpret_cast<Wt*>(u64) : reinterpret_cast<Wt*>(OP == SV_K1 ? in32 : out32);
+        const int wsx = OP == SV_UPDATE ? sxd : k.sx;
+        const long long wSz = (long long)wsx * (n + 2);
+        Wt* wp = wbase + (act[0] ? grown_index<Wt>(n, wsx, x, ya, z0) : 0);
+        const int oxo = ex == 1 ? n : (ex == 2 ? -n : 0);
+        int oyo[YC];
+#pragma unroll
+        for (int r = 0; r < YC; r++) oyo[r] = ey[r] == 1 ? n * wsx : (ey[r] == 2 ? -n * wsx : 0);
+        const long long ozn = (long long)n * wSz;
         double m = 0.0;
+        // v at q (a valid cell) and at its periodic images (the stores store_with_images makes)
+        auto put = [&](Wt* q, int oy, long long oz, Wt v) {
+            *q = v;
+            if ((oxo | oy) == 0 && oz == 0) return;
+            if (oxo) q[oxo] = v;
+            if (oy) q[oy] = v;
+            if (oxo && oy) q[oxo + oy] = v;
+            if (oz) {
+                q[oz] = v;
+                if (oxo) q[oz + oxo] = v;
+                if (oy) q[oz + oy] = v;
+                if (oxo && oy) q[oz + oxo + oy] = v;
+            }
+        };
         // one cell: the stencil taps, the plane's pointwise inputs and the outputs of this phase
-        auto cell = [&](int yy, int zz, int ey, int ez, int ii, V zm, V zc, V zp, V xm, V xp, V ym, V yp, float rr,
+        auto cell = [&](Wt* q, int oy, long long oz, int ii, V zm, V zc, V zp, V xm, V xp, V ym, V yp, float rr,
                         double dd) {
             // Laplacian insertion order: 0, +x, -x, +y, -y, +z, -z
             if constexpr (OP == SV_K1) {
@@ -266,8 +293,7 @@ __global__ void __launch_bounds__(kSvUnit, 3) k_sv_ring(const SvItem* __restrict
                 m = upd_abs(m, res);
                 const float r32 = __double2float_rn(res);
                 out32[ii] = r32;
-                float* q = in32 + grown_index<float>(n, k.sx, x, yy, zz);
-                store_with_images(in32, n, k.sx, q, ex, ey, ez, relax_value(k, 0.f, 0.f, r32, al));
+                put(q, oy, oz, relax_value(k, 0.f, 0.f, r32, al));
             } else {
                 float acc = 0.f;
                 acc = dadd(acc, dmul(cf.c[0], (float)zc));
@@ -278,13 +304,8 @@ __global__ void __launch_bounds__(kSvUnit, 3) k_sv_ring(const SvItem* __restrict
                 acc = dadd(acc, dmul(cf.c[5], (float)zp));
                 acc = dadd(acc, dmul(cf.c[6], (float)zm));
                 const float v = relax_value(k, acc, (float)zc, rr, alpha);
-                if constexpr (OP == SV_RELAX) {
-                    float* q = out32 + grown_index<float>(n, sx, x, yy, zz);
-                    store_with_images(out32, n, sx, q, ex, ey, ez, v);
-                } else {
-                    double* q = u64 + grown_index<double>(n, sxd, x, yy, zz);
-                    store_with_images(u64, n, sxd, q, ex, ey, ez, dadd(dd, (double)v));
-                }
+                if constexpr (OP == SV_RELAX) put(q, oy, oz, v);
+                else put(q, oy, oz, dadd(dd, (double)v));
             }
         };
         int qz = 0;
@@ -301,7 +322,7 @@ __global__ void __launch_bounds__(kSvUnit, 3) k_sv_ring(const SvItem* __restrict
                     if (act[r]) rr[r] = rhs[i + r * n];
                 }
                 if constexpr (OP == SV_UPDATE) {
-                    if (act[r]) dd[r] = u64[grown_index<double>(n, sxd, x, ya + r, z)];
+                    if (act[r]) dd[r] = wp[r * wsx];
                 }
             }
             cp_async_wait<L - 2>();   // this thread's copies of plane z + 1 have landed
@@ -319,15 +340,15 @@ __global__ void __launch_bounds__(kSvUnit, 3) k_sv_ring(const SvItem* __restrict
 #pragma unroll
                     for (int r = 0; r < YC; r++) zp[r] = act[r] ? col[Sz + r * sx] : V(0);
                 }
-                const int ez = edge_code(z, n);
+                const long long oz = z == 0 ? ozn : (z == n - 1 ? -ozn : 0);
 #pragma unroll
                 for (int r = 0; r < YC; r++) {
                     if (!act[r]) break;
                     // y neighbours: this thread's rows from registers, the tile's edge rows from the ring
                     const V ym = r == 0 ? pl[-RS] : zc[r - 1];
                     const V yp = (r + 1 < YC && act[r + 1]) ? zc[r + 1] : pl[(r + 1) * RS];
-                    cell(ya + r, z, ey[r], ez, i + r * n, zm[r], zc[r], zp[r], pl[r * RS - 1], pl[r * RS + 1], ym, yp,
-                         rr[r], dd[r]);
+                    cell(wp + r * wsx, oyo[r], oz, i + r * n, zm[r], zc[r], zp[r], pl[r * RS - 1], pl[r * RS + 1], ym,
+                         yp, rr[r], dd[r]);
                 }
 #pragma unroll
                 for (int r = 0; r < YC; r++) {
@@ -336,6 +357,7 @@ __global__ void __launch_bounds__(kSvUnit, 3) k_sv_ring(const SvItem* __restrict
                 }
             }
             col += Sz;
+            wp += wSz;
             i += n * n;
             qz = qz == Q - 1 ? 0 : qz + 1;
         }

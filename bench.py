@@ -94,7 +94,7 @@ class Clocks:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
@@ -349,7 +349,8 @@ def profile_serving(pb, torch, count=16, n=96, steps=2):
     one serving engine (public API, pinned host buffers), `steps` V-cycles for all of them."""
     from proto_b200 import serving as S
     from proto_b200 import workloads as W
-    eng = pb.Serve(8 << 30, max_active=count, tol=1e-30, max_cycles=steps)
+    # max_active = 4 * count: up to count solves load at once, so all of them run from the first cycle
+    eng = pb.Serve(8 << 30, max_active=4 * count, tol=1e-30, max_cycles=steps)
     f = S.pinned(n ** 3)
     f[:] = W.sine_modes_rhs(n, seed=5, modes=4).reshape(-1)
     outs = [S.pinned(n ** 3) for _ in range(count)]
@@ -471,12 +472,15 @@ def main():
         phi.zero_()
         return mg.solve(rho, phi)
 
+    # clocks are sampled from before the first timed region to after the last multigrid one (the
+    # timed regions are short; the sampler needs a moment to start)
+    clocks = Clocks(local)
+    clocks.start()
+    time.sleep(0.5)
     for _ in range(max(args.warmup, 3)):
         it, hist = one_solve()
     iters = it
     barrier()
-    clocks = Clocks(local)
-    clocks.start()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     per_solve = []
     ev0.record(stream)
@@ -489,7 +493,6 @@ def main():
         assert it == iters
     ev1.record(stream)
     barrier()
-    clk = clocks.stop()
     t_dev = ev0.elapsed_time(ev1) / 1000.0
     lat = sorted(a.elapsed_time(b) for a, b in per_solve)
     t_max = max_over_ranks(t_dev)
@@ -601,6 +604,7 @@ def main():
     b.record(stream)
     barrier()
     t_rx32 = a.elapsed_time(b) / 1000.0 / reps
+    clk = clocks.stop()
     pb.device_check()
     value_m = whole_job_rate(world, args.steps, t_mx)
     amr = None if world > 1 else run_amr_level(pb, torch)

@@ -80,8 +80,8 @@ int pb_stencil_apply_f32(const pb_stencil* s, const float* src, pb_box src_box,
  * sweeps (xv = 2 applies to boxes of even x extent; others use xv = 1). min_tma_points < 0 keeps
  * the current threshold. */
 int pb_star_tune_set(int mode, int zc, int ty, int yb, int xv, long long min_tma_points);
-/* Depth of the TMA kernel's shared-memory ring (0: up to 2R+4 planes, as deep as two CTAs per SM
- * allow; else 2R+1..16) and whether
+/* Depth of the TMA kernel's shared-memory ring (0: up to 2R+4 planes, 2R+3 with two x points per
+ * thread, as deep as two CTAs per SM allow; else 2R+1..16) and whether
  * per-point auxiliary fields of fused kernels (multigrid right-hand sides) are staged through it
  * by TMA (1) or read from global memory (0). */
 int pb_star_tune_ring(int nst, int aux_smem);

@@ -91,9 +91,10 @@ int launch_star_tma(const T* src, StarGeom g, const Coefs<T>& cf, const Epi& epi
     }
     const size_t stage = (size_t)SM::PLANE + aux_bytes;
     if (nst <= 0) {
-        // deepest ring (up to 2R+4 planes) that still lets the CTAs the registers allow share an SM
+        // deepest ring (up to 2R+4 planes; 2R+3 for two x points per thread, measured faster for
+        // the 256^3 FP64 sweep) that still lets the CTAs the registers allow share an SM
         const int per_sm = star_min_blocks(TY, YB, XV);
-        nst = 2 * R + 4;
+        nst = XV > 1 ? 2 * R + 3 : 2 * R + 4;
         while (nst > 2 * R + 1 && (size_t)per_sm * (nst * stage + 16 * nst + 1024) > 227 * 1024) nst--;
     }
     if (nst < 2 * R + 1 || nst > 16) return PB_ERR_ARG;

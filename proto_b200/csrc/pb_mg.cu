@@ -226,6 +226,25 @@ static int launch_resnorm(pb_mg* mg, MGLevel<double>& L, cudaStream_t st)
                                   default_star_tune(), level_aux(mg, L.rhs, L.alpha, L), 2);
 }
 
+// FP64, nu1 >= 1: the norm of the finest level's state fused with the next cycle's first sweep,
+// which goes to the other buffer (L.cur is left on the state measured)
+static bool fuse_norm(const pb_mg* mg) { return !is_mixed(mg) && mg->p.nu1 >= 1 && mg->p.levels >= 1; }
+
+static int launch_relax_norm(pb_mg* mg, MGLevel<double>& L, cudaStream_t st)
+{
+    PB_CUDA(cudaMemsetAsync(mg->d_res, 0, sizeof(double), st));
+    EpiRelaxNorm<double> epi;
+    epi.out = L.phi[1 - L.cur];
+    epi.k = relax_coef(mg, L);
+    epi.c2 = lap7_coefs<double>(L.hsqinv);
+    epi.beta = mg->p.beta;
+    epi.result = mg->d_res;
+    epi.m = 0.0;
+    const double s = is_helm(mg) ? L.hsqinv : mg->p.omega / 6.0;
+    return launch_star<ShapeLap7>(L.phi[L.cur], grown_box(L), valid_box(L), lap7_coefs<double>(s), epi, st,
+                                  default_star_tune(), level_aux(mg, L.rhs, L.alpha, L), 2);
+}
+
 // MIXED: FP64 residual of u64 + norm + FP32 right-hand side + first FP32 sweep of the finest level
 static int launch_res64(pb_mg* mg, cudaStream_t st)
 {
@@ -396,6 +415,12 @@ static int cycle_and_norm(pb_mg* mg, cudaStream_t st)
         mg->lv32[top].cur = 1;   // the residual pass left the first sweep in phi[1]
         if ((e = vcycle(mg, mg->lv32, top, false, 1, true, st)) != PB_OK) return e;
         if ((e = launch_res64(mg, st)) != PB_OK) return e;
+    } else if (fuse_norm(mg)) {
+        const int top = (int)mg->lv.size() - 1;
+        MGLevel<double>& T = mg->lv[top];
+        T.cur = 1 - T.cur;   // the previous fused pass left this cycle's first sweep in the other buffer
+        if ((e = vcycle(mg, mg->lv, top, false, 1, false, st)) != PB_OK) return e;
+        if ((e = launch_relax_norm(mg, T, st)) != PB_OK) return e;
     } else {
         const int top = (int)mg->lv.size() - 1;
         if ((e = vcycle(mg, mg->lv, top, false, 0, false, st)) != PB_OK) return e;
@@ -593,7 +618,8 @@ int pb_mg_solve(pb_mg* mg, const double* rhs, double* phi, int* iters, double* h
         T->cur = 0;
         k_pack_in<double><<<grid_for(n3, 256), 256, 0, st>>>(phi, T->phi[0], n, T->sx);
         PB_LAUNCH_CHECK();
-        if ((e = launch_resnorm(mg, *T, st)) != PB_OK) return e;
+        e = fuse_norm(mg) ? launch_relax_norm(mg, *T, st) : launch_resnorm(mg, *T, st);
+        if (e != PB_OK) return e;
     }
     PB_CUDA(cudaMemcpyAsync(mg->h_res, mg->d_res, sizeof(double), cudaMemcpyDeviceToHost, st));
     PB_CUDA(cudaStreamSynchronize(st));
@@ -658,9 +684,10 @@ int pb_mg_launches_per_cycle(const pb_mg_params* p)
     if (params_ok(p) != PB_OK) return -1;
     // levels top..1: nu1 + nu2 sweeps, one restriction, one prolongation; the bottom solve; one norm
     // (mixed: the first pre-sweep and the last post-sweep fuse into the residual and update passes,
-    // and the residual pass replaces the norm). Levels at or below the fused edge: one launch.
+    // and the residual pass replaces the norm; FP64 with nu1 >= 1: the norm rides on the next
+    // cycle's first sweep). Levels at or below the fused edge: one launch.
     const int per = p->nu1 + p->nu2 + 2;
-    const int mixed = p->precision == PB_MG_MIXED ? 1 : 0;
+    const int mixed = (p->precision == PB_MG_MIXED || (p->nu1 >= 1 && p->levels >= 1)) ? 1 : 0;
     const int ft = fused_top(*p);
     if (ft >= 0) return (p->levels - ft) * per - mixed + 1 + 1;
     const int bottom = p->bottom == PB_MG_BOTTOM_DIRECT ? 1 : p->nu_bottom;

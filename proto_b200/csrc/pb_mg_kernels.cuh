@@ -249,6 +249,46 @@ struct EpiResnorm {
     __device__ __forceinline__ void end_block() const { block_max_atomic(m, result); }
 };
 
+// A Jacobi sweep fused with the max-norm residual of the state it reads: the norm the solver tests
+// after a cycle is taken during the next cycle's first sweep (the sweep writes the other buffer,
+// so the state measured stays intact for the caller if it has converged). acc is the smoother's
+// sum (relax_value, as EpiRelax), acc2 the operator's: (0 - f) + L(u, 1/h^2) for the Poisson form,
+// L(u, 1/h^2) for the Helmholtz form, both in the Laplacian's term order, so the norm is bitwise
+// EpiResnorm's. Auxiliary fields: 0 = rho (= f), 1 = alpha (Helmholtz).
+template <typename T>
+struct EpiRelaxNorm {
+    T* out;
+    RelaxCoef<T> k;
+    Coefs<T> c2;         // L(., 1/h^2)
+    T beta;
+    double* result;
+    double m;
+    using Row = PeriodicRow<T>;
+    static constexpr bool kZEdge = true;
+    static constexpr bool kTwoSums = true;
+    static constexpr int kAux = 2;
+    __device__ __forceinline__ Row row(int x, int y, int z0, bool active) const { return periodic_row(out, k.n, k.sx, x, y, z0, active); }
+    __device__ __forceinline__ bool z_edge(int z) const { return z == 0 || z == k.n - 1; }
+    __device__ __forceinline__ T init(const Row&, int, int, const AuxCtx&) const { return T(0); }
+    __device__ __forceinline__ T init2(const Row& r, int, int, const AuxCtx& ax) const
+    {
+        if (k.helm || !r.active()) return T(0);
+        return dsub(T(0), ax.get<T>(0));
+    }
+    template <bool ZE>
+    __device__ __forceinline__ void finish2(const Row& r, int zo, int pv, T acc, T acc2, T c, const AuxCtx& ax)
+    {
+        if (!r.active()) return;
+        const T rho = ax.get<T>(0);
+        const T al = k.helm ? ax.get<T>(1) : T(0);
+        store_row<ZE>(out, k.n, k.sx, r, zo, pv, relax_value(k, acc, c, rho, al));
+        if (!k.helm) m = upd_abs(m, (double)acc2);
+        else m = upd_abs(m, (double)dsub(rho, dsub(dmul(al, c), dmul(beta, acc2))));
+    }
+    __device__ __forceinline__ void end_warp() const { warp_max_atomic(m, result); }
+    __device__ __forceinline__ void end_block() const { block_max_atomic(m, result); }
+};
+
 // Mixed precision, one pass over the FP64 state u (auxiliary fields: 0 = f, 1 = alpha):
 //   r = (0 + f) + L(u, -1/h^2)  |  r = f - (alpha*u - beta*L(u, 1/h^2))   (FP64)
 //   norm = max |r|; rhs32 = float(r); first FP32 sweep of the next cycle from e = 0 into e32.

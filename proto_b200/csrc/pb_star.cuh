@@ -48,6 +48,14 @@ struct Coefs {
     T c[13];
 };
 
+// Epilogues that need a second weighted sum of the same taps (a residual beside a relaxation)
+// declare kTwoSums = true and provide c2 (its coefficients), init2 and finish2; the kernels then
+// carry a second accumulator, summed in the same term order. Others are unaffected.
+template <class E, class = void>
+struct two_sums : std::false_type {};
+template <class E>
+struct two_sums<E, std::void_t<decltype(E::kTwoSums)>> : std::integral_constant<bool, E::kTwoSums> {};
+
 // Geometry of one star application. Index-box point (x,y,z), 0 <= x < nx ..., maps to source-local
 // coordinates (x+ox, y+oy, z+oz) in a field of extents (Sx, Sy, Sz).
 struct StarGeom {
@@ -333,6 +341,8 @@ __global__ void __launch_bounds__(kStarTX * (TY / YB) + 32, star_min_blocks(TY, 
 #pragma unroll
                 for (int k = 0; k < NA; k++) ax.p[k] = ab[k] + r * arow[k] + v * es[k];
                 T acc = epi.init(rows[r], zo, v, ax);
+                [[maybe_unused]] T acc2 = T(0);
+                if constexpr (two_sums<Epi>::value) acc2 = epi.init2(rows[r], zo, v, ax);
 #pragma unroll
                 for (int j = 0; j < S::NT; j++) {
                     const int ox = S::off(j, 0), oy = S::off(j, 1), oz = S::off(j, 2);
@@ -343,8 +353,10 @@ __global__ void __launch_bounds__(kStarTX * (TY / YB) + 32, star_min_blocks(TY, 
                     else if (ox == 0 && r + oy >= 0 && r + oy < YB) val = win[r + oy][v][IC];   // this thread's row
                     else val = pc[sc0 + (r + oy) * SM::BX + v + ox];
                     acc = dadd(acc, dmul(cf.c[j], val));
+                    if constexpr (two_sums<Epi>::value) acc2 = dadd(acc2, dmul(epi.c2.c[j], val));
                 }
-                epi.template finish<ZE>(rows[r], zo, v, acc, win[r][v][IC], ax);
+                if constexpr (two_sums<Epi>::value) epi.template finish2<ZE>(rows[r], zo, v, acc, acc2, win[r][v][IC], ax);
+                else epi.template finish<ZE>(rows[r], zo, v, acc, win[r][v][IC], ax);
             }
         }
         __syncwarp();
@@ -393,15 +405,24 @@ __global__ void __launch_bounds__(256) k_star_simple(const T* __restrict__ src, 
         }
         const typename Epi::Row row = epi.row(x, y, z, true);
         T acc = epi.init(row, 0, 0, ax);
+        [[maybe_unused]] T acc2 = T(0);
+        if constexpr (two_sums<Epi>::value) acc2 = epi.init2(row, 0, 0, ax);
 #pragma unroll
         for (int j = 0; j < S::NT; j++) {
             const long long o = S::off(j, 0) + Sx * S::off(j, 1) + Sxy * S::off(j, 2);
-            acc = dadd(acc, dmul(cf.c[j], __ldg(src + base + o)));
+            const T val = __ldg(src + base + o);
+            acc = dadd(acc, dmul(cf.c[j], val));
+            if constexpr (two_sums<Epi>::value) acc2 = dadd(acc2, dmul(epi.c2.c[j], val));
         }
         bool ze = false;
         if constexpr (Epi::kZEdge) ze = epi.z_edge(z);
-        if (ze) epi.template finish<true>(row, 0, 0, acc, __ldg(src + base), ax);
-        else epi.template finish<false>(row, 0, 0, acc, __ldg(src + base), ax);
+        if constexpr (two_sums<Epi>::value) {
+            if (ze) epi.template finish2<true>(row, 0, 0, acc, acc2, __ldg(src + base), ax);
+            else epi.template finish2<false>(row, 0, 0, acc, acc2, __ldg(src + base), ax);
+        } else {
+            if (ze) epi.template finish<true>(row, 0, 0, acc, __ldg(src + base), ax);
+            else epi.template finish<false>(row, 0, 0, acc, __ldg(src + base), ax);
+        }
     }
     epi.end_block();
 }

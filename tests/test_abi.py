@@ -93,17 +93,19 @@ def test_multigrid_parameter_rules():
     L = pb.lib()
     lp = L.pb_mg_launches_per_cycle
     try:
-        # one launch per step: (nu1 + nu2 + 2) per level above the coarsest, the bottom, the norm
+        # one launch per step: (nu1 + nu2 + 2) per level above the coarsest, the bottom, the norm;
+        # with nu1 >= 1 the FP64 norm rides on the next cycle's first sweep
         assert L.pb_mg_coarse_edge(0) == 0
-        assert lp(ctypes.byref(P(n=256, levels=6, nu1=4, nu2=4, nu_bottom=10).c)) == 6 * 10 + 10 + 1
-        assert lp(ctypes.byref(P(n=256, levels=5, nu1=4, nu2=4, bottom=1).c)) == 5 * 10 + 1 + 1
+        assert lp(ctypes.byref(P(n=256, levels=6, nu1=4, nu2=4, nu_bottom=10).c)) == 6 * 10 + 10
+        assert lp(ctypes.byref(P(n=256, levels=6, nu1=0, nu2=4, nu_bottom=10).c)) == 6 * 6 + 10 + 1
+        assert lp(ctypes.byref(P(n=256, levels=5, nu1=4, nu2=4, bottom=1).c)) == 5 * 10 + 1
         assert lp(ctypes.byref(P(n=256, levels=6, nu1=4, nu2=4, nu_bottom=10, precision=pb.MG_MIXED).c)) == 6 * 10 + 10
         # levels of edge <= 16 (16, 8, 4 here) as one launch
         assert L.pb_mg_coarse_edge(16) == 0
-        assert lp(ctypes.byref(P(n=256, levels=6, nu1=4, nu2=4, nu_bottom=10).c)) == 4 * 10 + 1 + 1
+        assert lp(ctypes.byref(P(n=256, levels=6, nu1=4, nu2=4, nu_bottom=10).c)) == 4 * 10 + 1
         assert lp(ctypes.byref(P(n=256, levels=6, nu1=4, nu2=4, precision=pb.MG_MIXED).c)) == 4 * 10 - 1 + 1 + 1
         # the finest grid always runs step by step, even when its edge is small
-        assert lp(ctypes.byref(P(n=16, levels=2, nu1=4, nu2=4, nu_bottom=10).c)) == 1 * 10 + 1 + 1
+        assert lp(ctypes.byref(P(n=16, levels=2, nu1=4, nu2=4, nu_bottom=10).c)) == 1 * 10 + 1
         assert L.pb_mg_coarse_edge(-1) == -1
     finally:
         L.pb_mg_coarse_edge(16)

@@ -417,6 +417,7 @@ def main():
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-precision", action="store_true", help="skip the 384^3 mixed-precision section")
     ap.add_argument("--no-fas", action="store_true", help="skip the FAS (LevelMultigridSolver) section")
+    ap.add_argument("--no-amr", action="store_true", help="skip the AMR-level section (and its tile autotuning)")
     ap.add_argument("--profile-kernels", action="store_true",
                     help="run one 256^3 FP64 sweep, one FP32 sweep and one Stencil::apply, then exit (for ncu)")
     ap.add_argument("--profile-level", action="store_true",
@@ -607,7 +608,7 @@ def main():
     clk = clocks.stop()
     pb.device_check()
     value_m = whole_job_rate(world, args.steps, t_mx)
-    amr = None if world > 1 else run_amr_level(pb, torch)
+    amr = None if (world > 1 or args.no_amr) else run_amr_level(pb, torch)
     precision = None if (world > 1 or args.no_precision) else run_precision(pb, torch)
     fas = None if (world > 1 or args.no_fas) else run_fas(pb, torch, cpu=not args.no_cpu_baseline)
     # the serving replay is a one-GPU measurement (replicas add nothing to it)

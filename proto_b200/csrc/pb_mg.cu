@@ -355,8 +355,9 @@ static int vcycle(pb_mg* mg, std::vector<MGLevel<T>>& lv, int l, bool zero_start
         MGLevel<T>& C = lv[l - 1];
         if ((e = relax_sweeps(mg, L, mg->p.nu1 - pre_done, zero_start && !pre_done, st)) != PB_OK) return e;
         const double s = is_helm(mg) ? L.hsqinv : -L.hsqinv;
-        k_resid_restrict<T><<<restrict_grid(L.n), dim3(32, 8), 0, st>>>(L.phi[L.cur], L.rhs, L.alpha, C.rhs, L.n, L.sx,
-                                                                       is_helm(mg), lap7_coefs<T>(s), (T)mg->p.beta);
+        const int czc = restrict_z_chunk(L.n, cached_sm_count());
+        k_resid_restrict_z<T><<<restrict_z_grid(L.n, czc), dim3(32, 8), 0, st>>>(
+            L.phi[L.cur], L.rhs, L.alpha, C.rhs, L.n, L.sx, is_helm(mg), lap7_coefs<T>(s), (T)mg->p.beta, czc);
         PB_LAUNCH_CHECK();
         if ((e = vcycle(mg, lv, l - 1, true, 0, false, st)) != PB_OK) return e;
         k_prolong<T><<<prolong_grid(L.n), dim3(32, 8), 0, st>>>(L.phi[L.cur], C.phi[C.cur], L.n, L.sx, C.sx);

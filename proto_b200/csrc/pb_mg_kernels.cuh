@@ -425,6 +425,104 @@ __global__ void __launch_bounds__(256) k_resid_restrict(const T* __restrict__ ph
 }
 static inline dim3 restrict_grid(int nf) { return dim3((nf / 2 + 31) / 32, (nf / 2 + 7) / 8, nf / 2); }
 
+// The same coarse right-hand side, marching in z. Block (32, 8): lane = fine x (32 consecutive
+// fine cells, coalesced), threadIdx.y = coarse row cy (fine rows 2cy, 2cy+1); the block walks
+// coarse planes [cz0, cz0 + czc). Each fine row keeps phi at the fine planes 2cz-1 .. 2cz+2 in a
+// register window (two new planes per coarse plane), and the y taps between the thread's two rows
+// come from registers, so a fine cell costs about five loads instead of eight. Each fine residual
+// is fine_residual's arithmetic (taps in the Laplacian's order); the even lane of a pair gathers
+// its neighbour's four residuals by shuffle and sums the eight children in Box([0,1]^3) order.
+template <typename T>
+__global__ void __launch_bounds__(256) k_resid_restrict_z(const T* __restrict__ phi, const T* __restrict__ rhs,
+                                                          const T* __restrict__ alpha, T* rhs_c, int nf, int sx,
+                                                          int helm, Coefs<T> cf, T beta, int czc)
+{
+    const int nc = nf / 2;
+    const int fx = blockIdx.x * 32 + threadIdx.x, cy = blockIdx.y * 8 + threadIdx.y;
+    const int cz0 = blockIdx.z * czc, cz1 = min(cz0 + czc, nc);
+    const bool act = fx < nf && cy < nc;          // warp-uniform in y; x lanes beyond nf idle
+    const long long Sy = sx, Sz = (long long)sx * (nf + 2);
+    const T eighth = T(1.0 / 8);
+    const int fy0 = 2 * cy;
+    // grown address of (fx, fy0, fz) = base + fz * Sz; rows fy0 and fy0 + 1
+    const T* base = phi + (act ? grown_index<T>(nf, sx, fx, fy0, 0) : 0);
+    T w[2][4];                                    // [row][fine plane 2cz-1 .. 2cz+2]
+    if (act) {
+#pragma unroll
+        for (int r = 0; r < 2; r++) {
+            w[r][2] = base[r * Sy + (long long)(2 * cz0 - 1) * Sz];
+            w[r][3] = base[r * Sy + (long long)(2 * cz0) * Sz];
+        }
+    }
+    for (int cz = cz0; cz < cz1; cz++) {
+        T res[2][2];                              // [row][fine plane 2cz, 2cz+1]
+        if (act) {
+#pragma unroll
+            for (int r = 0; r < 2; r++) {
+                w[r][0] = w[r][2];
+                w[r][1] = w[r][3];
+                w[r][2] = base[r * Sy + (long long)(2 * cz + 1) * Sz];
+                w[r][3] = base[r * Sy + (long long)(2 * cz + 2) * Sz];
+            }
+#pragma unroll
+            for (int pz = 0; pz < 2; pz++) {
+                const int fz = 2 * cz + pz;
+#pragma unroll
+                for (int r = 0; r < 2; r++) {
+                    const T* q = base + r * Sy + (long long)fz * Sz;
+                    const long long fi = fx + (long long)nf * ((fy0 + r) + (long long)nf * fz);
+                    const T c = w[r][pz + 1];
+                    // taps in the Laplacian's order: 0, +x, -x, +y, -y, +z, -z
+                    const T t[7] = {c, q[1], q[-1], r == 0 ? w[1][pz + 1] : q[Sy], r == 1 ? w[0][pz + 1] : q[-Sy],
+                                    w[r][pz + 2], w[r][pz]};
+                    const T rho = __ldg(rhs + fi);
+                    if (!helm) {
+                        T v = dadd(T(0), rho);
+#pragma unroll
+                        for (int j = 0; j < 7; j++) v = dadd(v, dmul(cf.c[j], t[j]));
+                        res[r][pz] = v;
+                    } else {
+                        T lp = T(0);
+#pragma unroll
+                        for (int j = 0; j < 7; j++) lp = dadd(lp, dmul(cf.c[j], t[j]));
+                        res[r][pz] = dsub(rho, dsub(dmul(__ldg(alpha + fi), c), dmul(beta, lp)));
+                    }
+                }
+            }
+        } else {
+            res[0][0] = res[0][1] = res[1][0] = res[1][1] = T(0);
+        }
+        // children k = dx + 2 dy + 4 dz; dx = 1 lives in the odd lane
+        T odd[2][2];
+#pragma unroll
+        for (int r = 0; r < 2; r++)
+#pragma unroll
+            for (int pz = 0; pz < 2; pz++) odd[r][pz] = __shfl_down_sync(0xffffffffu, res[r][pz], 1);
+        if (act && (fx & 1) == 0) {
+            T acc = T(0);
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                const int dx = k & 1, dy = (k >> 1) & 1, dz = k >> 2;
+                acc = dadd(acc, dmul(eighth, dx ? odd[dy][dz] : res[dy][dz]));
+            }
+            rhs_c[fx / 2 + (long long)nc * (cy + (long long)nc * cz)] = acc;
+        }
+    }
+}
+// z chunk: about two waves of 8 blocks per SM
+static inline int restrict_z_chunk(int nf, int sms)
+{
+    const int nc = nf / 2;
+    const long long bxy = (long long)((nf + 31) / 32) * ((nc + 7) / 8);
+    const long long want = 2LL * sms * 8;
+    int czc = (int)((nc * bxy + want - 1) / want);
+    return czc < 1 ? 1 : (czc > nc ? nc : czc);
+}
+static inline dim3 restrict_z_grid(int nf, int czc)
+{
+    return dim3((nf + 31) / 32, (nf / 2 + 7) / 8, (nf / 2 + czc - 1) / czc);
+}
+
 // phi += 1.0 * delta_c(p/2) on the valid box, periodic images included. Block (32, 8) over a
 // 64 x 8 tile of fine cells: each thread takes fine x and x + 32, so every warp access is 32
 // consecutive cells.

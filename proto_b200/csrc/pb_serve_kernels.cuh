@@ -85,22 +85,65 @@ __global__ void __launch_bounds__(kSvUnit) k_sv_phase(const SvItem* __restrict__
         if (row < it.units) {
             const int n = it.k.n, sx = it.k.sx;
             if constexpr (OP == SV_RESTRICT) {
-                // a row of coarse cells of the (n/2)^3 level below; 8 fine residuals each, Box([0,1]^3) order
+                // a row of coarse cells of the (n/2)^3 level below. Lanes take consecutive fine x of
+                // the two fine rows and two fine planes under the row (coalesced); the taps those
+                // four cells share come from registers. Each fine residual is fine_residual's
+                // arithmetic (taps in the Laplacian's order); the even lane of a pair gathers its
+                // neighbour's four residuals by shuffle and sums the eight children in Box([0,1]^3)
+                // order.
                 const int nc = n / 2;
                 const int y = row % nc, z = row / nc;
                 const long long Sy = sx, Sz = (long long)sx * (n + 2);
                 float* out = it.out + (long long)row * nc;
-                for (int x = lane; x < nc; x += 32) {
-                    float acc = 0.f;
+                const float* b0 = it.in + grown_index<float>(n, sx, 0, 2 * y, 2 * z);   // fine (0, 2y, 2z)
+                const float* r0 = it.rhs + (long long)n * (2 * y + (long long)n * (2 * z));
+                for (int fx0 = 0; fx0 < n; fx0 += 32) {   // uniform over the warp (shuffles below)
+                    const int fx = fx0 + lane;
+                    float res[2][2] = {{0.f, 0.f}, {0.f, 0.f}};   // [dy][dz]
+                    if (fx < n) {
+                        const float* q = b0 + fx;
+                        float c[2][2];
 #pragma unroll
-                    for (int k = 0; k < 8; k++) {
-                        const int fx = 2 * x + (k & 1), fy = 2 * y + ((k >> 1) & 1), fz = 2 * z + (k >> 2);
-                        const int fi = fx + n * (fy + n * fz);
-                        const float r = fine_residual<float>(it.in, grown_index<float>(n, sx, fx, fy, fz), Sy, Sz,
-                                                             it.rhs[fi], it.alpha, it.k.helm, it.c, it.beta);
-                        acc = dadd(acc, dmul(0.125f, r));
+                        for (int dy = 0; dy < 2; dy++)
+#pragma unroll
+                            for (int dz = 0; dz < 2; dz++) c[dy][dz] = q[dy * Sy + dz * Sz];
+#pragma unroll
+                        for (int dy = 0; dy < 2; dy++)
+#pragma unroll
+                            for (int dz = 0; dz < 2; dz++) {
+                                const float* p = q + dy * Sy + dz * Sz;
+                                // 0, +x, -x, +y, -y, +z, -z
+                                const float t[7] = {c[dy][dz], p[1], p[-1], dy == 0 ? c[1][dz] : p[Sy],
+                                                    dy == 1 ? c[0][dz] : p[-Sy], dz == 0 ? c[dy][1] : p[Sz],
+                                                    dz == 1 ? c[dy][0] : p[-Sz]};
+                                const float rho = r0[fx + dy * n + (long long)dz * n * n];
+                                if (!it.k.helm) {
+                                    float v = dadd(0.f, rho);
+#pragma unroll
+                                    for (int j = 0; j < 7; j++) v = dadd(v, dmul(it.c.c[j], t[j]));
+                                    res[dy][dz] = v;
+                                } else {
+                                    float lp = 0.f;
+#pragma unroll
+                                    for (int j = 0; j < 7; j++) lp = dadd(lp, dmul(it.c.c[j], t[j]));
+                                    res[dy][dz] = dsub(rho, dsub(dmul(it.alpha, t[0]), dmul(it.beta, lp)));
+                                }
+                            }
                     }
-                    out[x] = acc;
+                    float odd[2][2];
+#pragma unroll
+                    for (int dy = 0; dy < 2; dy++)
+#pragma unroll
+                        for (int dz = 0; dz < 2; dz++) odd[dy][dz] = __shfl_down_sync(0xffffffffu, res[dy][dz], 1);
+                    if (fx < n && (fx & 1) == 0) {
+                        float acc = 0.f;
+#pragma unroll
+                        for (int k = 0; k < 8; k++) {
+                            const int dx = k & 1, dy = (k >> 1) & 1, dz = k >> 2;
+                            acc = dadd(acc, dmul(0.125f, dx ? odd[dy][dz] : res[dy][dz]));
+                        }
+                        out[fx / 2] = acc;
+                    }
                 }
             } else {
                 const int y = row % n, z = row / n;

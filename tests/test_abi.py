@@ -108,7 +108,7 @@ def test_multigrid_parameter_rules():
         assert lp(ctypes.byref(P(n=16, levels=2, nu1=4, nu2=4, nu_bottom=10).c)) == 1 * 10 + 1
         assert L.pb_mg_coarse_edge(-1) == -1
     finally:
-        L.pb_mg_coarse_edge(16)
+        L.pb_mg_coarse_edge(8)
 
 
 def test_serve_host_rules():

@@ -150,7 +150,7 @@ def test_coarse_levels_as_one_kernel_bitwise(pb, port, edge, lev):
         it, hist, phi = _gpu_solve(pb, N, lev, pb.MG_FP64, max_iter=8, alpha=alpha, rhs=rhs, bottom=1)
         it2, hist2, phi2 = _gpu_solve(pb, N, lev, pb.MG_FP64, max_iter=8)
     finally:
-        L.pb_mg_coarse_edge(16)
+        L.pb_mg_coarse_edge(8)
     p1 = np.zeros(N ** 3)
     n1, h1 = port.mg_cs(N, lev, 4, 4, 10, 2.0 / 3.0, 1.0, alpha.reshape(-1).copy(), 8, 1e-10,
                         rhs.reshape(-1).copy(), p1, bottom=1)

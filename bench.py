@@ -41,7 +41,9 @@ NU_BOTTOM = 10
 OMEGA = 2.0 / 3.0
 TOL = 1e-10
 MAX_ITER = 100
-CYCLES_PER_SOLVE = 16   # V(4,4) cycles this workload takes to 1e-10 (FP64, bitwise equal on CPU and GPU)
+# V(4,4) cycles the GPU solver takes on this workload; the reference arm uses it only when it ran too
+# few cycles for a solve of its own to converge (the two residual histories are bitwise identical)
+GPU_CYCLES_PER_SOLVE = 16
 STENCIL_BYTES = 8 * (258 ** 3 + 256 ** 3)          # algorithmic bytes of dst |= L(src), 256^3
 RELAX_BYTES = 24 * 256 ** 3                        # read phi, read rho, write phi_new
 SERVE_MAX_ACTIVE = 128                             # serving: solves in one batched cycle at most
@@ -126,46 +128,74 @@ class Clocks:
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_reference_rate(iters_per_solve, procs=None, reps=1):
-    """Reference CPU path (oracle/_ref) on host cores: each process times `reps` V-cycles plus the
-    residual norm of the 256^3 solve; the rate scales by the GPU's cycle count (same arithmetic,
-    same count). Independent processes, one solve each, as the reference solver is single-threaded."""
-    import multiprocessing as mp
-    from oracle.oracle import Ref
-    ncpu = os.cpu_count() or 1
-    if procs is None:
-        procs = max(1, min(16, ncpu // 2))
-    if Ref.available():
-        ctx = mp.get_context("spawn")
-        with ctx.Pool(procs) as pool:
-            times = pool.map(_ref_cycle_time, [reps] * procs)
-        t_cycle = float(np.mean(times)) / reps
-        rate = procs / (t_cycle * iters_per_solve)
-        return {"value": rate, "unit": "solves/s", "cores": procs, "kind": "reference",
-                "sample": "%d V(%d,%d) cycle(s) + residual norm of the 256^3 solve in each of %d processes "
-                          "(reference LevelBoxData/Stencil code, box 64, 1 thread each), scaled by %d cycles per "
-                          "solve; mean cycle %.2f s" % (reps, NU1, NU2, procs, iters_per_solve, t_cycle)}
-    # the C restatement with OpenMP threads
-    from oracle.oracle import Port
-    from proto_b200 import workloads as W
-    P = Port()
-    rho = W.poisson_rho(N, seed=1).reshape(-1).copy()
-    phi = np.zeros(N ** 3)
-    t0 = time.perf_counter()
-    n, _ = P.mg_cs(N, LEVELS, NU1, NU2, NU_BOTTOM, OMEGA, 1.0, None, reps, 0.0, rho, phi)
-    t = (time.perf_counter() - t0) / max(n, 1)
-    return {"value": 1.0 / (t * iters_per_solve), "unit": "solves/s", "cores": P.num_threads(), "kind": "port",
-            "sample": "%d V-cycle(s) of the 256^3 solve with the C restatement (OpenMP), scaled by %d cycles" %
-                      (reps, iters_per_solve)}
+def _host_procs(per_proc_gb=1.6, cap=32):
+    """Independent single-threaded reference processes the host can run at once: one per CPU this
+    process may use, bounded by available memory (about 1.6 GB per 256^3 reference solve)."""
+    try:
+        ncpu = len(os.sched_getaffinity(0))
+    except AttributeError:
+        ncpu = os.cpu_count() or 1
+    procs = max(1, min(cap, ncpu))
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    avail_gb = int(line.split()[1]) / 2 ** 20
+                    procs = max(1, min(procs, int(avail_gb * 0.8 / per_proc_gb)))
+    except OSError:
+        pass
+    return procs, ncpu
 
 
-def _ref_cycle_time(reps):
+def _ref_cycles_worker(ncycles):
     sys.path.insert(0, ROOT)
     from oracle.oracle import Ref
     from proto_b200 import workloads as W
-    R = Ref()
     rho = W.poisson_rho(N, seed=1).reshape(-1).copy()
-    return R.mg_cs_time_cycles(N, 64, LEVELS, NU1, NU2, NU_BOTTOM, OMEGA, rho, reps)
+    first, done, t0, t_end = Ref().mg_cs_cycles(N, 64, LEVELS, NU1, NU2, NU_BOTTOM, OMEGA, TOL, rho, ncycles)
+    return first, done, t0, [float(t) for t in t_end]
+
+
+def cpu_reference_cycles(warmup, steps, gpu_cycles=None, procs=None):
+    """The reference's own CPU solver (oracle/_ref: its LevelBoxData / Stencil / AvgDown /
+    InterpStencil code, boxes of 64) on the host cores. `procs` independent single-threaded
+    processes (the reference solver has no threading of its own) each run warmup + steps real
+    V(4,4) cycles of the 256^3 solve, each cycle followed by the residual norm, from u = 0, starting a
+    new solve whenever one converges. A step is one cycle in every process; the timed region is a
+    process's last `steps` cycles, and the slowest process's region counts. Solves/s = procs * steps
+    / (T * cycles per solve), the cycle count being the one the reference needed to converge, or, if
+    no solve converged within the cycles run, the GPU solver's count for the same problem (the two
+    residual histories are bitwise identical)."""
+    import multiprocessing as mp
+    from oracle.oracle import Ref
+    if not Ref.available():
+        raise RuntimeError("oracle/_ref/libproto_ref.so is not built")
+    nproc, ncpu = _host_procs()
+    if procs:
+        nproc = procs
+    ncyc = warmup + steps
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(nproc) as pool:
+        res = pool.map(_ref_cycles_worker, [ncyc] * nproc)
+    spans = []
+    for first, done, t0, t_end in res:
+        t_a = t_end[warmup - 1] if warmup >= 1 else t0
+        spans.append(t_end[ncyc - 1] - t_a)
+    T = max(spans)
+    firsts = [r[0] for r in res if r[0] > 0]
+    if firsts:
+        cps, src = firsts[0], "reference (converged within the run)"
+    else:
+        if not gpu_cycles:
+            raise RuntimeError("no reference solve converged within %d cycles" % ncyc)
+        cps, src = gpu_cycles, "GPU solver, same problem (bitwise-identical residual history)"
+    rate = nproc * steps / (T * cps)
+    return {"value": rate, "unit": "solves/s", "cores": nproc, "host_cpus": ncpu, "kind": "reference",
+            "timed_s": T, "ms_per_cycle_step": 1000.0 * T / steps, "cycles_per_solve": cps,
+            "cycles_per_solve_from": src, "solves_completed": int(sum(r[1] for r in res)),
+            "sample": "%d processes x (%d warm-up + %d timed) real V(%d,%d) cycles + residual norm of the 256^3 "
+                      "solve (reference code, boxes of 64, 1 thread each); %.2f s per cycle" %
+                      (nproc, warmup, steps, NU1, NU2, T / steps)}
 
 
 def profile_kernels(pb, torch):
@@ -304,7 +334,6 @@ def run_fas(pb, torch, sizes=(64, 128, 256), reps=3, cpu=True):
     st = torch.cuda.current_stream()
     out = {"workload": "FAS V(6,6) 4th-order flux-form Laplace, periodic, coarsest 4^3, 8 sine modes (seed 1), "
                        "tol 1e-10"}
-    iters64 = None
     for n in sizes:
         levels = int(round(math.log2(n))) - 1
         force = torch.from_numpy(-W.poisson_rho(n, seed=1).reshape(-1)).cuda()
@@ -321,11 +350,9 @@ def run_fas(pb, torch, sizes=(64, 128, 256), reps=3, cpu=True):
         ms = sorted(e0.elapsed_time(e1) for e0, e1 in ev)[reps // 2]
         out["n%d" % n] = {"levels": levels, "iters": it, "ms_per_solve": ms, "solves_per_s": 1000.0 / ms,
                           "final_rel_residual": hist[-1] / hist[0]}
-        if n == 64:
-            iters64 = it
         del mg
     pb.device_check()
-    if cpu and iters64:
+    if cpu:
         try:
             from oracle.oracle import Ref
             if Ref.available():
@@ -333,12 +360,12 @@ def run_fas(pb, torch, sizes=(64, 128, 256), reps=3, cpu=True):
                 f = -W.poisson_rho(64, seed=1).reshape(-1).copy()
                 p = np.zeros(64 ** 3)
                 t0 = time.perf_counter()
-                R.mg_fas(64, 16, 5, 1, 0.0, f, p)
+                it_ref, _ = R.mg_fas(64, 16, 5, 20, 1e-10, f, p)
                 t = time.perf_counter() - t0
-                out["cpu_baseline_64"] = {"value": 1.0 / (t * iters64), "unit": "solves/s", "cores": 1,
-                                          "kind": "reference",
-                                          "sample": "1 FAS cycle + 2 residual norms at 64^3 (boxes of 16) with the "
-                                                    "reference's LevelMultigridSolver, scaled by %d cycles" % iters64}
+                out["cpu_baseline_64"] = {"value": 1.0 / t, "unit": "solves/s", "cores": 1, "kind": "reference",
+                                          "iters": it_ref,
+                                          "sample": "one whole FAS solve at 64^3 (boxes of 16, %d cycles to 1e-10) with "
+                                                    "the reference's LevelMultigridSolver, one thread" % it_ref}
         except Exception as e:   # the baseline never hides the GPU result
             out["cpu_baseline_64"] = {"error": str(e)}
     return out
@@ -392,16 +419,22 @@ def run_serving(pb, count):
 
 
 def run_reference(args, rank, world):
+    """The reference's own CPU path, unmodified (oracle/_ref), on this host's cores, for the same
+    workload and metric: every step is one real V(4,4) cycle (+ residual norm) of the 256^3 solve in
+    each of the independent reference processes (cpu_reference_cycles). Rank 0 alone runs it."""
     if rank != 0:
         return
-    iters = CYCLES_PER_SOLVE
     t0 = time.perf_counter()
-    cb = cpu_reference_rate(iters)
+    cb = cpu_reference_cycles(args.warmup, args.steps, gpu_cycles=GPU_CYCLES_PER_SOLVE,
+                              procs=args.ref_procs or None)
     wall = time.perf_counter() - t0
     line = {"impl": "reference", "metric": "MG solves/s", "value": cb["value"], "unit": "solves/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1000.0 / cb["value"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic", "config": workload_config(), "cpu_baseline": cb,
+            "ms_per_step": cb["ms_per_cycle_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload_config(),
+            "step": "one V(%d,%d) cycle + residual norm in each of %d reference processes; solves/s = processes x "
+                    "steps / (timed s x %d cycles per solve)" % (NU1, NU2, cb["cores"], cb["cycles_per_solve"]),
+            "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "wall_s": wall}
     print(json.dumps(line), flush=True)
@@ -427,6 +460,8 @@ def main():
     ap.add_argument("--profile-fas", action="store_true",
                     help="FAS solves at 256^3 only (for kernel captures)")
     ap.add_argument("--serve-requests", type=int, default=2000)
+    ap.add_argument("--ref-procs", type=int, default=0,
+                    help="reference arm: independent reference processes (0 = one per usable host CPU)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -660,11 +695,12 @@ def main():
             line["amr_level"] = amr
         if serving is not None:
             line["serving"] = serving
-        if iters != CYCLES_PER_SOLVE:
-            line["note"] = "cycles per solve %d differ from the %d the reference arm scales by" % (iters, CYCLES_PER_SOLVE)
+        if iters != GPU_CYCLES_PER_SOLVE:
+            line["note"] = "cycles per solve %d differ from the %d the reference arm assumes when it runs too few " \
+                           "cycles to converge" % (iters, GPU_CYCLES_PER_SOLVE)
         if world == 1 and not args.no_cpu_baseline:
             try:
-                line["cpu_baseline"] = cpu_reference_rate(iters)
+                line["cpu_baseline"] = cpu_reference_cycles(1, 2, gpu_cycles=iters)
             except Exception as e:  # the baseline never hides the GPU result
                 line["cpu_baseline"] = {"error": str(e)}
         try:

@@ -42,6 +42,12 @@ const char* pb_status_string(int status);
 int pb_last_cuda_error(void);
 /* Reads (and clears) the device-side error flag of the current device; synchronises the stream. */
 int pb_device_check(void* stream);
+/* Test hook for the failure path of every pipelined kernel (no counterpart in the reference, which
+ * aborts): runs the bounded mbarrier wait those kernels use on a barrier that never completes,
+ * with a limit of `tries` polls (1 .. 2^24). *expired = 1 when the wait gave up; the device error
+ * flag is then set and the next pb_device_check returns PB_ERR_DEVICE. No copy is in flight and
+ * the context stays usable. Synchronises the stream. */
+int pb_debug_wait_expiry(unsigned int tries, int* expired, void* stream);
 /* Library version string and the compute capability it was built for ("sm_100a"). */
 const char* pb_version(void);
 
@@ -256,7 +262,9 @@ int pb_fas_solve(pb_fas* m, const double* force, double* phi, int max_iter, doub
  * the device (an upload stream of its own; hierarchies come from a stream-ordered pool of the
  * engine). An admitted solve takes a free slot in the same step when no requests are queued (light
  * load), else in the first step after its upload has landed (uploads overlap the running cycles).
- * Solves are retired when their max-norm residual drops below tol times the first one. Per solve
+ * Solves are retired when their max-norm residual drops below tol times the first one, as failed
+ * after max_cycles cycles, and as failed at once when a residual is not finite (a NaN or infinite
+ * right-hand side, or a diverging solve), without disturbing the other solves. Per solve
  * the arithmetic is pb_mg's PB_MG_MIXED solver's (constant alpha, levels = every
  * halving, bottom = nu_bottom sweeps), so each result is the same alone and in any mix.
  * An edge must halve down to <= 16 (n = m * 2^k with m <= 16). */

@@ -12,6 +12,8 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+# the reference checkout's mount point in the build container (read only); PROTO_REFERENCE_ROOT
+# points the recipe elsewhere. Where neither exists the reference-built library is skipped.
 REF_ROOT = os.environ.get("PROTO_REFERENCE_ROOT", "/root/reference")
 
 

@@ -204,6 +204,19 @@ class Ref:
                                               _c_int(nu2), _c_int(nu_bottom), _c_dbl(omega), _p(rhs),
                                               _c_int(reps))
 
+    def mg_cs_cycles(self, N, box_size, levels, nu1, nu2, nu_bottom, omega, tol, rhs, ncycles):
+        """Runs ncycles real V-cycles (+ norms) of the Poisson solve, restarting from zero after each
+        converged solve. Returns (cycles of the first solve, solves completed, start time, end time of
+        every cycle); times are steady-clock seconds."""
+        rhs = _f64(rhs)
+        t_end = np.zeros(ncycles)
+        t0 = _c_dbl(0.0)
+        done = _c_int(0)
+        first = self.lib.ref_mg_cs_cycles(_c_int(N), _c_int(box_size), _c_int(levels), _c_int(nu1), _c_int(nu2),
+                                          _c_int(nu_bottom), _c_dbl(omega), _c_dbl(tol), _p(rhs), _c_int(ncycles),
+                                          ctypes.byref(t0), _p(t_end), ctypes.byref(done))
+        return first, done.value, t0.value, t_end
+
     def level13_steps(self, widths, ghost, h, dt, steps, data):
         arrs = [_i3(w) for w in widths]
         counts = _i3([len(w) for w in widths])

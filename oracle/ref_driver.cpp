@@ -522,6 +522,52 @@ double ref_mg_cs_time_cycles(int N, int boxSize, int levels, int nu1, int nu2, i
     return std::chrono::duration<double>(t1 - t0).count();
 }
 
+// Runs ncycles V-cycles of ref_mg_cs's Poisson solver from phi = 0, each followed by the residual
+// norm, exactly as a solve does; when a solve reaches res < tol*res0 the next cycle starts a new
+// solve from phi = 0 (its initial norm counted in that cycle). *t_start is the steady-clock time
+// (seconds) before the first norm, t_end[k] the time at which cycle k ended. Returns the number of
+// cycles the first solve took to converge (0 if none converged within ncycles).
+int ref_mg_cs_cycles(int N, int boxSize, int levels, int nu1, int nu2, int nuBottom, double omega,
+                     double tol, const double* rhs, int ncycles, double* t_start, double* t_end,
+                     int* solves_done)
+{
+    auto now = []() {
+        return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+    };
+    Box domain = Box::Cube(N);
+    Array<bool,DIM> per; per.fill(true);
+    double dx = 1.0/N;
+    ProblemDomain pd(domain, per);
+    DisjointBoxLayout layout(pd, Point::Ones(boxSize));
+    CSParams p{nu1, nu2, nuBottom, omega, 1.0};
+    RefCS mg(layout, dx, levels, p, false);
+    LevelBoxData<double> R(layout, Point::Zeros());
+    LevelBoxData<double> P(layout, Point::Ones());
+    R.setToZero(); P.setToZero();
+    load_level(R, domain, rhs);
+    *t_start = now();
+    double r0 = mg.resnorm(P, R);
+    int first = 0, done = 0, inSolve = 0;
+    for (int k = 0; k < ncycles; k++) {
+        if (inSolve < 0) {          // previous solve converged: start the next one from zero
+            P.setToZero();
+            r0 = mg.resnorm(P, R);
+            inSolve = 0;
+        }
+        mg.vCycle(P, R);
+        double r = mg.resnorm(P, R);
+        inSolve++;
+        if (r < tol*r0) {
+            if (done == 0) first = inSolve;
+            done++;
+            inSolve = -1;
+        }
+        t_end[k] = now();
+    }
+    *solves_done = done;
+    return first;
+}
+
 // ---- AMR-level stepping on uneven patches (per-patch BoxData, ghost fill by BoxData::copyTo) ----
 // Patches tile a periodic domain as a tensor product of per-axis widths. For every step:
 // periodic ghost fill, Lu = L13(u, 1/h^2) (13-point: sum_d Derivative(2,d,4)), u += dt*Lu.

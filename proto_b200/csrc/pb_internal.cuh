@@ -173,14 +173,20 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
         : "memory");
     return ok != 0;
 }
-// Bounded wait: returns false (and flags DEV_WAIT_TIMEOUT) if the phase never completes.
+// Bounded wait: returns false (and flags DEV_WAIT_TIMEOUT) if the phase has not completed after
+// `tries` polls. Every pipelined kernel waits through mbar_wait (kMaxWaitTries polls, about a
+// second); pb_debug_wait_expiry runs the same code with a small limit so a test can make it expire.
 constexpr uint32_t kMaxWaitTries = 1u << 24;
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
+__device__ __forceinline__ bool mbar_wait_limited(uint64_t* bar, uint32_t parity, uint32_t tries)
 {
-    for (uint32_t i = 0; i < kMaxWaitTries; i++)
+    for (uint32_t i = 0; i < tries; i++)
         if (mbar_try_wait(bar, parity)) return true;
     flag_error(DEV_WAIT_TIMEOUT);
     return false;
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
+{
+    return mbar_wait_limited(bar, parity, kMaxWaitTries);
 }
 __device__ __forceinline__ void tma_load_3d(void* smem_dst, const CUtensorMap* map, uint64_t* bar, int x, int y,
                                             int z)

@@ -102,7 +102,11 @@ __global__ void __launch_bounds__(kThreads) k_reduce_chunks(int op, const double
     }
 }
 
-// Device address of g_scratch per device ordinal, resolved once with that device current.
+// Device address of g_scratch per device ordinal, resolved once with that device current. The cache
+// lives as long as the process's CUDA context on that device: after cudaDeviceReset the module may be
+// loaded again at another address, so a caller that resets a device must not call this entry point
+// on it again in the same process. Two host threads that race on a device's first call both store
+// the same address, which is harmless.
 static unsigned char* g_addr[64] = {nullptr};
 
 static int scratch_address(unsigned char** out)

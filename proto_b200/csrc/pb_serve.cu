@@ -924,7 +924,10 @@ int pb_serve_step(pb_serve* sv, int* active, int* waiting)
             }
             s.cycles++;
             s.r = sv->h_norms[i];
-            if (s.r < sv->p.tol * s.r0) e = retire(sv, s, PB_SERVE_DONE);
+            // a residual that is not finite (a NaN or infinite right-hand side, or a diverging
+            // solve) ends the solve at once as failed; its neighbours in the batch are unaffected
+            if (!std::isfinite(s.r0) || !std::isfinite(s.r)) e = retire(sv, s, PB_SERVE_FAILED);
+            else if (s.r < sv->p.tol * s.r0) e = retire(sv, s, PB_SERVE_DONE);
             else if (s.cycles >= sv->p.max_cycles) e = retire(sv, s, PB_SERVE_FAILED);
             if (e != PB_OK) return e;
         }

@@ -14,6 +14,9 @@
 // The per-cell arithmetic is the single-solve solver's (same helpers, same order), so a solve's
 // result does not depend on what else is in the batch.
 #pragma once
+#include <cfloat>
+#include <math_constants.h>
+
 #include "pb_mg_kernels.cuh"
 
 namespace pb {
@@ -291,6 +294,8 @@ __global__ void __launch_bounds__(kSvUnit, 3) k_sv_ring(const SvItem* __restrict
         for (int r = 0; r < YC; r++) oyo[r] = ey[r] == 1 ? n * wsx : (ey[r] == 2 ? -n * wsx : 0);
         const long long ozn = (long long)n * wSz;
         double m = 0.0;
+        bool bad = false;     // K1: a residual that is not finite (the norm itself skips NaN, as
+                              // Reduction<Abs> does); the solve's norm is then reported as +inf
         // v at q (a valid cell) and at its periodic images (the stores store_with_images makes)
         auto put = [&](Wt* q, int oy, long long oz, Wt v) {
             *q = v;
@@ -334,6 +339,7 @@ __global__ void __launch_bounds__(kSvUnit, 3) k_sv_ring(const SvItem* __restrict
                     al = __double2float_rn(alpha64);
                 }
                 m = upd_abs(m, res);
+                bad = bad || !(fabs(res) <= DBL_MAX);
                 const float r32 = __double2float_rn(res);
                 out32[ii] = r32;
                 put(q, oy, oz, relax_value(k, 0.f, 0.f, r32, al));
@@ -407,6 +413,7 @@ __global__ void __launch_bounds__(kSvUnit, 3) k_sv_ring(const SvItem* __restrict
         cp_async_wait<0>();
         __syncthreads();              // the ring is free for the next unit
         if constexpr (OP == SV_K1) {
+            if (__any_sync(0xffffffffu, bad)) m = CUDART_INF;
             for (int o = 16; o > 0; o >>= 1) {
                 const double w = __shfl_down_sync(0xffffffffu, m, o);
                 m = (m < w) ? w : m;

@@ -23,6 +23,22 @@ namespace pb {
 
 PB_DEFINE_ERROR_READER(read_error_stencil)
 
+// The bounded wait of the pipelined kernels, made to expire on purpose: one thread waits on an
+// mbarrier whose phase never completes (nothing arrives and no copy is in flight), gives up after
+// `tries` polls through the same mbar_wait_limited every kernel uses, and records whether the wait
+// reported the timeout; the wait also sets the device error flag that pb_device_check reads.
+static __device__ int g_wait_expired = 0;
+static __global__ void k_wait_expiry(uint32_t tries)
+{
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) g_wait_expired = mbar_wait_limited(&bar, 0, tries) ? 0 : 1;
+}
+
 static thread_local int t_last_cuda = 0;
 void set_cuda_error(cudaError_t e) { t_last_cuda = (int)e; }
 
@@ -327,6 +343,17 @@ const char* pb_status_string(int s)
 int pb_last_cuda_error(void) { return t_last_cuda; }
 
 const char* pb_version(void) { return "proto_b200 1.0 sm_100a"; }
+
+int pb_debug_wait_expiry(unsigned int tries, int* expired, void* stream)
+{
+    if (!expired || tries == 0 || tries > kMaxWaitTries) return PB_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    k_wait_expiry<<<1, 32, 0, st>>>(tries);
+    PB_LAUNCH_CHECK();
+    PB_CUDA(cudaStreamSynchronize(st));
+    PB_CUDA(cudaMemcpyFromSymbol(expired, g_wait_expired, sizeof(int)));
+    return PB_OK;
+}
 
 int pb_device_check(void* stream)
 {

@@ -125,3 +125,11 @@ def test_serve_host_rules():
     assert L.pb_serve_create(ctypes.byref(bad), ctypes.byref(h)) == -1
     bad = pb.pb_serve_params(0, 4, 4, 4, 10, 2.0 / 3.0, 1e-8, 100)         # no budget
     assert L.pb_serve_create(ctypes.byref(bad), ctypes.byref(h)) == -1
+
+
+def test_wait_expiry_hook_validates_arguments():
+    L = pb.lib()
+    e = ctypes.c_int()
+    assert L.pb_debug_wait_expiry(ctypes.c_uint(0), ctypes.byref(e), None) == -1
+    assert L.pb_debug_wait_expiry(ctypes.c_uint(1000), None, None) == -1
+    assert L.pb_debug_wait_expiry(ctypes.c_uint((1 << 24) + 1), ctypes.byref(e), None) == -1

@@ -118,3 +118,27 @@ def test_error_against_fp64_oracle(pb, port):
         port.mg_cs(n, halvings(n), 4, 4, 10, 2.0 / 3.0, 1.0, alpha, 100, 1e-8, rhs.copy(), ref)
         err = np.max(np.abs(o - ref)) / np.max(np.abs(ref))
         assert err < 1e-6, (n, helm, err)
+
+
+def test_failed_requests_leave_the_others_unchanged(pb):
+    """Failure paths of the engine, made on the host: a right-hand side holding a NaN fails at its
+    first residual pass (the norm reports a non-finite residual); a zero right-hand side never meets
+    res < tol * res0 (res0 = 0) and fails after max_cycles. Every other solve in the same batch
+    completes with bitwise the result it has alone."""
+    reqs = requests()
+    n = 32
+    nan_rhs = reqs[0][3].copy()
+    nan_rhs[n ** 3 // 2 + 7] = np.nan
+    zero_rhs = np.zeros(n ** 3)
+    mix = reqs[:3] + [(n, 0, 0.0, nan_rhs)] + reqs[3:] + [(n, 1, 0.5, zero_rhs)]
+    outs, stats, _ = serve(pb, mix, max_cycles=40)
+    nan_state, nan_cycles, _ = stats[3]
+    assert nan_state == pb.SERVE_FAILED and nan_cycles == 1
+    zero_state, zero_cycles, _ = stats[-1]
+    assert zero_state == pb.SERVE_FAILED and zero_cycles == 40
+    good = [i for i in range(len(mix)) if i not in (3, len(mix) - 1)]
+    alone, astats, _ = serve(pb, [mix[i] for i in good], max_cycles=40)
+    for k, i in enumerate(good):
+        assert stats[i][0] == pb.SERVE_DONE and astats[k][0] == pb.SERVE_DONE
+        assert stats[i][1] == astats[k][1]
+        assert np.array_equal(outs[i], alone[k])

@@ -237,6 +237,16 @@ int pb_mg_launches_per_cycle(const pb_mg_params* p);
  * 0 turns this off. Default 8 (measured faster than 16 for large solves). Applies to solvers
  * created and cycles captured afterwards. */
 int pb_mg_coarse_edge(int edge);
+/* Process-wide: levels of edge >= 'edge' (of the edges the two-sweep kernel is built for: 128, 256,
+ * 384) run each pair of consecutive Jacobi sweeps as one pass over the level (the intermediate
+ * sweep stays on chip; same arithmetic, bitwise the same results); 0 turns this off. Default 128.
+ * Applies to cycles captured afterwards. */
+int pb_mg_relax2_min_edge(int edge);
+/* Process-wide launch-shape knobs of the two-sweep pass: planes per CTA (0 = chosen from the
+ * occupancy so whole waves fill the GPU), cells per thread along x (0 = the default per edge, 1 or
+ * 2) and output rows per thread group (0 = the default, 2 or 4; a CTA takes two groups). For
+ * tuning and tests; results do not depend on them. */
+int pb_mg_relax2_shape(int zc, int cells_per_thread, int rows_per_group);
 
 /* ---- FAS multigrid with the 4th-order flux-form Laplacian (reference: LevelMultigridSolver<
  * BoxOp_Laplace>, include/utils/implem/Proto_LevelMultigridSolverImplem.H:85-433, operator

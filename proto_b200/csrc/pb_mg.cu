@@ -20,11 +20,13 @@
 // FMA, so the FP64 solver reproduces the reference CPU path's residual history bit for bit.
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <type_traits>
 #include <vector>
 
 #include "pb_internal.cuh"
 #include "pb_mg_kernels.cuh"
+#include "pb_relax2.cuh"
 #include "pb_stencil_impl.cuh"
 
 namespace pb {
@@ -193,6 +195,133 @@ static int launch_relax(pb_mg* mg, MGLevel<T>& L, bool first, cudaStream_t st)
     return PB_OK;
 }
 
+// ---- two sweeps per pass (k_relax2) ----------------------------------------------------------------
+// Levels of edge >= g_relax2_min_edge whose edge the kernel is built for (128, 256, 384) run each
+// pair of consecutive sweeps as one k_relax2 pass; 0 turns this off (every sweep a launch). The
+// results are bitwise the same either way.
+static int g_relax2_min_edge = 128;
+static int g_relax2_zc = 0;   // z chunk override (0: the occupancy heuristic)
+static int g_relax2_pv = 0;   // cells per thread override (0: the default per edge)
+static int g_relax2_rg = 0;   // output rows per group override (0: the default per edge)
+
+// shared memory of a k_relax2 CTA with nst stages (the launcher's layout)
+static size_t relax2_smem(int n, int esize, bool helm, int nst, int rg = 2)
+{
+    int nb, bw;
+    relax2_segments(esize == 8 ? grown_pitch<double>(n) : grown_pitch<float>(n), esize, &nb, &bw);
+    const size_t tile0 = (size_t)(2 * rg + 4) * nb * bw, tilea = (size_t)(2 * rg + 2) * n;
+    return nst * (tile0 + (helm ? 2 : 1) * tilea) * esize + 2 * tilea * esize + 16 * (size_t)nst;
+}
+// the pass needs at least three stages (two planes in use and one in flight)
+static bool relax2_edge(int n, int esize, bool helm)
+{
+    return g_relax2_min_edge > 0 && n >= g_relax2_min_edge && (n == 128 || n == 256 || n == 384) &&
+           relax2_smem(n, esize, helm, 3, g_relax2_rg == 4 ? 4 : 2) <= 220 * 1024 && tma_available();
+}
+template <typename T>
+static bool relax2_ok(const pb_mg* mg, const MGLevel<T>& L)
+{
+    return relax2_edge(L.n, (int)sizeof(T), is_helm(mg));
+}
+
+template <typename T, int NXT, int PV, int RG, bool HELM, bool NORM>
+static int launch_relax2_t(pb_mg* mg, MGLevel<T>& L, double* result, cudaStream_t st)
+{
+    using SH = Relax2Shape<NXT, PV, RG>;
+    Relax2Args<T> a;
+    memset(&a, 0, sizeof(a));
+    a.out = L.phi[1 - L.cur];
+    a.k = relax_coef(mg, L);
+    a.c = lap7_coefs<T>(HELM ? L.hsqinv : mg->p.omega / 6.0);
+    a.c2 = lap7_coefs<T>(L.hsqinv);
+    a.beta = (T)mg->p.beta;
+    a.result = result;
+    relax2_segments(L.sx, (int)sizeof(T), &a.nb, &a.bw);
+    // tile boxes (all rows of an x segment) and row boxes (the tiles that wrap in y)
+    CUtensorMap map, map1, rmap, rmap1, amap, amap1;
+    const int es = (int)sizeof(T), bwr = SH::N / (SH::N > 256 ? 2 : 1);
+    int e = encode_tmap_3d(&map, L.phi[L.cur], es, L.sx, L.n + 2, L.n + 2, a.bw, SH::ROWS, 1);
+    if (e == PB_OK) e = encode_tmap_3d(&map1, L.phi[L.cur], es, L.sx, L.n + 2, L.n + 2, a.bw, 1, 1);
+    if (e == PB_OK) e = encode_tmap_3d(&rmap, L.rhs, es, L.n, L.n, L.n, bwr, SH::B1ROWS, 1);
+    if (e == PB_OK) e = encode_tmap_3d(&rmap1, L.rhs, es, L.n, L.n, L.n, bwr, 1, 1);
+    if (e == PB_OK && HELM) e = encode_tmap_3d(&amap, L.alpha, es, L.n, L.n, L.n, bwr, SH::B1ROWS, 1);
+    if (e == PB_OK && HELM) e = encode_tmap_3d(&amap1, L.alpha, es, L.n, L.n, L.n, bwr, 1, 1);
+    if (e != PB_OK) return e;
+    if (!HELM) {
+        amap = rmap;
+        amap1 = rmap1;
+    }
+    const int per_sm = relax2_min_blocks(SH::THREADS);
+    int nst = 6;
+    while (nst > 3 && (size_t)per_sm * (relax2_smem(SH::N, (int)sizeof(T), HELM, nst, RG) + 1024) > 227 * 1024) nst--;
+    a.nst = nst;
+    const size_t smem = relax2_smem(SH::N, (int)sizeof(T), HELM, nst, RG);
+    if (smem > 220 * 1024) return PB_ERR_UNSUPPORTED;
+    auto kern = k_relax2<T, NXT, PV, RG, HELM, NORM>;
+    static bool attr = false;
+    static int occ = 0;
+    static size_t occ_smem = 0;
+    if (!attr) {
+        PB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+        attr = true;
+    }
+    if (occ_smem != smem) {
+        PB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, SH::THREADS, smem));
+        if (occ < 1) occ = 1;
+        occ_smem = smem;
+    }
+    // z chunk: whole waves of the resident CTAs against the 3 planes each chunk adds (2 of phi0 and
+    // one of phi1 beyond its own)
+    const int tiles = SH::N / SH::TY;
+    const double slots = (double)cached_sm_count() * occ;
+    double best = -1.0;
+    int zc = SH::N;
+    for (int c = 8; c <= SH::N; c += 2) {
+        const long long blocks = (long long)tiles * ((SH::N + c - 1) / c);
+        const double waves = blocks / slots;
+        const double eff = (waves / std::ceil(waves)) * c / (double)(c + 3);
+        if (eff > best + 1e-9) {
+            best = eff;
+            zc = c;
+        }
+    }
+    // 384^3: chunks of 32 planes measured 1.5x faster than the wave heuristic's choice
+    if (SH::N == 384) zc = 32;
+    a.zc = g_relax2_zc > 0 ? std::min(g_relax2_zc, SH::N) : zc;
+    dim3 grid(tiles, (SH::N + a.zc - 1) / a.zc);
+    kern<<<grid, SH::THREADS, smem, st>>>(map, map1, rmap, rmap1, amap, amap1, a);
+    PB_LAUNCH_CHECK();
+    L.cur = 1 - L.cur;
+    return PB_OK;
+}
+
+template <typename T, bool HELM, bool NORM>
+static int launch_relax2_form(pb_mg* mg, MGLevel<T>& L, double* result, cudaStream_t st)
+{
+    // defaults (measured on B200): two cells per thread at 128, one at 256, two at 384
+    const bool tall = g_relax2_rg == 4;
+    const bool two = g_relax2_pv == 2 || (g_relax2_pv == 0 && L.n == 128);
+    switch (L.n) {
+    case 128: return two ? launch_relax2_t<T, 64, 2, 2, HELM, NORM>(mg, L, result, st)
+                         : launch_relax2_t<T, 128, 1, 2, HELM, NORM>(mg, L, result, st);
+    case 256: return two ? launch_relax2_t<T, 128, 2, 2, HELM, NORM>(mg, L, result, st)
+                         : (tall ? launch_relax2_t<T, 256, 1, 4, HELM, NORM>(mg, L, result, st)
+                                 : launch_relax2_t<T, 256, 1, 2, HELM, NORM>(mg, L, result, st));
+    case 384: return tall ? launch_relax2_t<T, 192, 2, 4, HELM, NORM>(mg, L, result, st)
+                          : launch_relax2_t<T, 192, 2, 2, HELM, NORM>(mg, L, result, st);
+    default: return PB_ERR_UNSUPPORTED;
+    }
+}
+
+// Two sweeps of level L in one pass (NORM: also the max-norm residual of the state it starts from,
+// into result). The caller checks relax2_ok.
+template <typename T, bool NORM>
+static int launch_relax2(pb_mg* mg, MGLevel<T>& L, double* result, cudaStream_t st)
+{
+    return is_helm(mg) ? launch_relax2_form<T, true, NORM>(mg, L, result, st)
+                       : launch_relax2_form<T, false, NORM>(mg, L, result, st);
+}
+
 // last FP32 post-sweep of the finest level fused with u64 += e
 static int launch_relax_update(pb_mg* mg, MGLevel<float>& L, cudaStream_t st)
 {
@@ -230,9 +359,23 @@ static int launch_resnorm(pb_mg* mg, MGLevel<double>& L, cudaStream_t st)
 // which goes to the other buffer (L.cur is left on the state measured)
 static bool fuse_norm(const pb_mg* mg) { return !is_mixed(mg) && mg->p.nu1 >= 1 && mg->p.levels >= 1; }
 
+// sweeps the fused norm pass performs: two (k_relax2 with the norm) where that kernel takes the
+// finest level and the cycle smooths at least twice before restricting, else one
+static int norm_sweeps_for(const pb_mg_params& p)
+{
+    return (p.nu1 >= 2 && relax2_edge(p.n, 8, p.form == PB_MG_HELMHOLTZ)) ? 2 : 1;
+}
+static int norm_sweeps(const pb_mg* mg) { return norm_sweeps_for(mg->p); }
+
 static int launch_relax_norm(pb_mg* mg, MGLevel<double>& L, cudaStream_t st)
 {
     PB_CUDA(cudaMemsetAsync(mg->d_res, 0, sizeof(double), st));
+    if (norm_sweeps(mg) == 2) {
+        const int cur = L.cur;
+        int e = launch_relax2<double, true>(mg, L, mg->d_res, st);
+        L.cur = cur;   // left on the state measured, like the one-sweep pass
+        return e;
+    }
     EpiRelaxNorm<double> epi;
     epi.out = L.phi[1 - L.cur];
     epi.k = relax_coef(mg, L);
@@ -273,8 +416,19 @@ static int launch_res64(pb_mg* mg, cudaStream_t st)
 template <typename T>
 static int relax_sweeps(pb_mg* mg, MGLevel<T>& L, int k, bool zero_start, cudaStream_t st)
 {
-    for (int s = 0; s < k; s++) {
-        int e = launch_relax(mg, L, zero_start && s == 0, st);
+    int s = 0;
+    if (zero_start && k > 0) {
+        int e = launch_relax(mg, L, true, st);
+        if (e != PB_OK) return e;
+        s = 1;
+    }
+    if (relax2_ok(mg, L))
+        for (; s + 2 <= k; s += 2) {
+            int e = launch_relax2<T, false>(mg, L, nullptr, st);
+            if (e != PB_OK) return e;
+        }
+    for (; s < k; s++) {
+        int e = launch_relax(mg, L, false, st);
         if (e != PB_OK) return e;
     }
     if (zero_start && k == 0) PB_CUDA(cudaMemsetAsync(L.phi[L.cur], 0, sizeof(T) * L.grown_elems(), st));
@@ -341,9 +495,9 @@ static int launch_coarse_cycle(pb_mg* mg, std::vector<MGLevel<T>>& lv, int top, 
     return PB_OK;
 }
 
-// V-cycle on level l of hierarchy lv. pre_done: the first pre-smoothing sweep already ran (the
-// mixed-precision residual pass does it); fuse_update: the last post-smoothing sweep adds its
-// result to the FP64 solution instead of storing it.
+// V-cycle on level l of hierarchy lv. pre_done: the first pre-smoothing sweep(s) already ran (the
+// mixed-precision residual pass does one, the FP64 norm pass one or two); fuse_update: the last
+// post-smoothing sweep adds its result to the FP64 solution instead of storing it.
 template <typename T>
 static int vcycle(pb_mg* mg, std::vector<MGLevel<T>>& lv, int l, bool zero_start, int pre_done, bool fuse_update,
                   cudaStream_t st)
@@ -420,8 +574,8 @@ static int cycle_and_norm(pb_mg* mg, cudaStream_t st)
     } else if (fuse_norm(mg)) {
         const int top = (int)mg->lv.size() - 1;
         MGLevel<double>& T = mg->lv[top];
-        T.cur = 1 - T.cur;   // the previous fused pass left this cycle's first sweep in the other buffer
-        if ((e = vcycle(mg, mg->lv, top, false, 1, false, st)) != PB_OK) return e;
+        T.cur = 1 - T.cur;   // the previous fused pass left this cycle's first sweeps in the other buffer
+        if ((e = vcycle(mg, mg->lv, top, false, norm_sweeps(mg), false, st)) != PB_OK) return e;
         if ((e = launch_relax_norm(mg, T, st)) != PB_OK) return e;
     } else {
         const int top = (int)mg->lv.size() - 1;
@@ -684,16 +838,48 @@ int pb_mg_relax(pb_mg* mg, int sweeps, void* stream)
 int pb_mg_launches_per_cycle(const pb_mg_params* p)
 {
     if (params_ok(p) != PB_OK) return -1;
-    // levels top..1: nu1 + nu2 sweeps, one restriction, one prolongation; the bottom solve; one norm
-    // (mixed: the first pre-sweep and the last post-sweep fuse into the residual and update passes,
-    // and the residual pass replaces the norm; FP64 with nu1 >= 1: the norm rides on the next
-    // cycle's first sweep). Levels at or below the fused edge: one launch.
-    const int per = p->nu1 + p->nu2 + 2;
-    const int mixed = (p->precision == PB_MG_MIXED || (p->nu1 >= 1 && p->levels >= 1)) ? 1 : 0;
-    const int ft = fused_top(*p);
-    if (ft >= 0) return (p->levels - ft) * per - mixed + 1 + 1;
-    const int bottom = p->bottom == PB_MG_BOTTOM_DIRECT ? 1 : p->nu_bottom;
-    return p->levels * per - mixed + bottom + 1;
+    // mirrors cycle_and_norm / vcycle / relax_sweeps, counting kernel launches (memsets excluded)
+    const pb_mg_params& q = *p;
+    const int ft = fused_top(q);
+    const int es = q.precision == PB_MG_MIXED ? 4 : 8;
+    const bool helm = q.form == PB_MG_HELMHOLTZ;
+    auto sweeps = [&](int n, int k, bool zero_start) {
+        int s = 0, c = 0;
+        if (zero_start && k > 0) s = c = 1;
+        if (relax2_edge(n, es, helm))
+            for (; s + 2 <= k; s += 2) c++;
+        return c + (k - s);
+    };
+    std::function<int(int, bool, int, bool)> cyc = [&](int l, bool zero_start, int pre_done, bool fuse_update) {
+        const int n = q.n >> (q.levels - l);
+        if (zero_start && l == ft) return 1;
+        if (l > 0) {
+            int c = sweeps(n, q.nu1 - pre_done, zero_start && !pre_done) + 1 + cyc(l - 1, true, 0, false) + 1;
+            c += fuse_update ? sweeps(n, q.nu2 - 1, false) + 1 : sweeps(n, q.nu2, false);
+            return c;
+        }
+        return q.bottom == PB_MG_BOTTOM_DIRECT ? 1 : sweeps(n, q.nu_bottom, zero_start);
+    };
+    if (q.precision == PB_MG_MIXED) return cyc(q.levels, false, 1, true) + 1;
+    if (q.nu1 >= 1 && q.levels >= 1) return cyc(q.levels, false, norm_sweeps_for(q), false) + 1;
+    return cyc(q.levels, false, 0, false) + 1;
+}
+
+int pb_mg_relax2_min_edge(int edge)
+{
+    if (edge < 0) return PB_ERR_ARG;
+    g_relax2_min_edge = edge;
+    return PB_OK;
+}
+
+int pb_mg_relax2_shape(int zc, int cells_per_thread, int rows_per_group)
+{
+    if (zc < 0 || cells_per_thread < 0 || cells_per_thread > 2) return PB_ERR_ARG;
+    if (rows_per_group != 0 && rows_per_group != 2 && rows_per_group != 4) return PB_ERR_ARG;
+    g_relax2_zc = zc;
+    g_relax2_pv = cells_per_thread;
+    g_relax2_rg = rows_per_group;
+    return PB_OK;
 }
 
 int pb_mg_coarse_edge(int edge)

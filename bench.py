@@ -45,7 +45,7 @@ MAX_ITER = 100
 # few cycles for a solve of its own to converge (the two residual histories are bitwise identical)
 GPU_CYCLES_PER_SOLVE = 16
 STENCIL_BYTES = 8 * (258 ** 3 + 256 ** 3)          # algorithmic bytes of dst |= L(src), 256^3
-RELAX_BYTES = 24 * 256 ** 3                        # read phi, read rho, write phi_new
+RELAX_BYTES = 24 * 256 ** 3                        # read phi, read rho, write phi_new (one or two sweeps)
 SERVE_MAX_ACTIVE = 128                             # serving: solves in one batched cycle at most
 
 
@@ -391,30 +391,50 @@ def profile_serving(pb, torch, count=16, n=96, steps=2):
 
 def run_serving(pb, count):
     """Request stream of periodic Poisson/Helmholtz solves (Poisson arrivals at 200/s, seed 4; edge
-    log-uniform in [32, 192] rounded to 16; alpha ~ U[0, 1]; 4-mode right-hand sides; tolerance
-    1e-8). Served by the batching engine (mixed precision, in-flight solves advanced together) and
-    by plain FP64 multigrid one request at a time, both open loop at the arrival rate and saturated
-    (every request available at once). Host buffers are pinned for both."""
-    import numpy as np
+    log-uniform in [32, 192] rounded to 16; alpha ~ U[0, 1]; a 4-mode right-hand side per request).
+    Three arms, each with pinned host buffers and the copies inside the measured time: the batching
+    engine (mixed precision, in-flight solves advanced together), plain mixed-precision multigrid
+    one request at a time, and plain FP64 multigrid one request at a time; so served / mixed-single
+    is what batching gains and mixed-single / FP64 what precision gains. At tolerance 1e-8 (the
+    configuration's) and 1e-10 (the precision target), saturated (every request available at once);
+    at 1e-8 also open loop at the arrival rate for latency. Every served result is compared with
+    the FP64 solver's solution of the same request."""
     from proto_b200 import serving as S
     trace = S.make_trace(count=count)
-    pool = S.rhs_pool([r["n"] for r in trace])
-    eng = pb.Serve(150 << 30, max_active=SERVE_MAX_ACTIVE, tol=1e-8)
-    ring = S._Ring([r["n"] for r in trace], SERVE_MAX_ACTIVE // 4)
-    # warm-up (untimed): the engine serves the whole trace once, as a running server would have, so
-    # its cache holds the hierarchies this traffic needs; the FP64 solvers see every (edge, form)
-    S.serve_trace(pb, trace, pool, realtime=False, engine=eng, ring=ring)
-    S.fp64_trace(pb, trace[:100], pool, realtime=False)
+    t0 = time.perf_counter()
+    data = S.TraceData(trace)
     out = {"workload": "%d requests, Poisson arrivals 200/s (seed 4), edge log-uniform [32,192] step 16, "
-                       "Poisson/Helmholtz 50/50, alpha~U[0,1], 4 sine modes, tol 1e-8" % count,
-           "hbm_budget_gb": 150, "max_active": SERVE_MAX_ACTIVE}
-    for mode, rt in (("saturated", False), ("arrival_rate", True)):
-        a, ka = S.serve_trace(pb, trace, pool, realtime=rt, keep=20, engine=eng, ring=ring)
-        b, kb = S.fp64_trace(pb, trace, pool, realtime=rt, keep=20)
-        err = max(float(np.max(np.abs(ka[i] - kb[i])) / np.max(np.abs(kb[i]))) for i in ka)
-        out[mode] = {"served_mixed": a, "fp64_one_at_a_time": b,
-                     "solves_per_s_ratio": a["solves_per_s"] / b["solves_per_s"],
-                     "max_rel_diff_vs_fp64_first20": err}
+                       "Poisson/Helmholtz 50/50, alpha~U[0,1], one 4-sine-mode right-hand side per request" % count,
+           "hbm_budget_gb": 150, "max_active": SERVE_MAX_ACTIVE, "rhs_bytes": data.nbytes,
+           "setup_s": time.perf_counter() - t0}
+    firsts = {}
+    for r in trace:
+        firsts.setdefault((r["n"], r["helm"]), r)
+    for tol, name in ((1e-8, "tol_1e-8"), (1e-10, "tol_1e-10")):
+        eng = pb.Serve(150 << 30, max_active=SERVE_MAX_ACTIVE, tol=tol)
+        fp64 = S.SingleSolvers(pb, trace, tol, pb.MG_FP64)
+        mixed = S.SingleSolvers(pb, trace, tol, pb.MG_MIXED)
+        # warm-up (untimed): the engine serves the trace once, as a running server would have (its
+        # cache holds the hierarchies this traffic needs); every single solver solves once
+        S.serve_trace(pb, trace, data, realtime=False, engine=eng)
+        for r in firsts.values():
+            fp64.solve(r, data.rhs_of(r["i"]))
+            mixed.solve(r, data.rhs_of(r["i"]))
+        served = S.serve_trace(pb, trace, data, realtime=False, engine=eng)
+        err = S.verify(pb, trace, data, fp64)
+        m1 = S.single_trace(pb, trace, data, mixed, realtime=False)
+        f1 = S.single_trace(pb, trace, data, fp64, realtime=False)
+        res = {"saturated": {"served_mixed": served, "mixed_one_at_a_time": m1, "fp64_one_at_a_time": f1,
+                             "served_vs_fp64": served["solves_per_s"] / f1["solves_per_s"],
+                             "batching_gain": served["solves_per_s"] / m1["solves_per_s"],
+                             "precision_gain": m1["solves_per_s"] / f1["solves_per_s"]},
+               "served_rel_err_vs_fp64": err}
+        if tol == 1e-8:
+            a = S.serve_trace(pb, trace, data, realtime=True, engine=eng)
+            b = S.single_trace(pb, trace, data, fp64, realtime=True)
+            res["arrival_rate"] = {"served_mixed": a, "fp64_one_at_a_time": b}
+        out[name] = res
+        del eng, fp64, mixed
     return out
 
 
@@ -592,15 +612,19 @@ def main():
     b.record(stream)
     barrier()
     t_st = a.elapsed_time(b) / 1000.0 / reps
-    for _ in range(3):
-        mg.relax(1)
-    barrier()
-    a.record(stream)
-    for _ in range(reps):
-        mg.relax(1)
-    b.record(stream)
-    barrier()
-    t_rx = a.elapsed_time(b) / 1000.0 / reps
+    def time_relax(m, sweeps):
+        for _ in range(3):
+            m.relax(sweeps)
+        barrier()
+        a.record(stream)
+        for _ in range(reps):
+            m.relax(sweeps)
+        b.record(stream)
+        barrier()
+        return a.elapsed_time(b) / 1000.0 / reps
+
+    t_rx = time_relax(mg, 1)       # one sweep: k_star_tma<Lap7, EpiRelax>
+    t_rx2 = time_relax(mg, 2)      # two sweeps in one pass: k_relax2 (the solve's dominant kernel)
     pb.device_check()
     phi64 = phi.clone()
     mg.solve(rho, phi64.zero_())
@@ -631,15 +655,8 @@ def main():
     t_mx = max_over_ranks(a.elapsed_time(b) / 1000.0)
     lat_m = sorted(x.elapsed_time(y) for x, y in lat_m)
     err_m = float((phim - phi64).abs().max() / phi64.abs().max())
-    for _ in range(3):
-        mgm.relax(1)
-    barrier()
-    a.record(stream)
-    for _ in range(reps):
-        mgm.relax(1)
-    b.record(stream)
-    barrier()
-    t_rx32 = a.elapsed_time(b) / 1000.0 / reps
+    t_rx32 = time_relax(mgm, 1)
+    t_rx32_2 = time_relax(mgm, 2)
     clk = clocks.stop()
     pb.device_check()
     value_m = whole_job_rate(world, args.steps, t_mx)
@@ -648,17 +665,19 @@ def main():
     fas = None if (world > 1 or args.no_fas) else run_fas(pb, torch, cpu=not args.no_cpu_baseline)
     # the serving replay is a one-GPU measurement (replicas add nothing to it)
     serving = None if (args.no_serving or world > 1) else run_serving(pb, args.serve_requests)
+    torch.cuda.synchronize()
     peak, peak_kind = measured_peaks()
     st_gbs = STENCIL_BYTES / t_st / 1e9
     rx_gbs = RELAX_BYTES / t_rx / 1e9
+    rx2_gbs = RELAX_BYTES / t_rx2 / 1e9     # a two-sweep pass moves the bytes of one sweep
 
-    traffic = None
+    traffic = {}
     tp = os.path.join(ROOT, "profiles", "relax_traffic.json")
     if os.path.exists(tp):
         try:
-            traffic = json.load(open(tp)).get("bytes_per_launch_256")
+            traffic = json.load(open(tp))
         except Exception:
-            traffic = None
+            traffic = {}
 
     if rank == 0:
         launches = 3 + iters * mg.launches_per_cycle() + 1
@@ -668,24 +687,6 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": workload_config(), "iters_per_solve": iters, "final_rel_residual": hist[-1] / hist[0],
             "latency_ms": {"p50": lat[len(lat) // 2], "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
-            "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": 8 * N ** 3,
-                    "d2h_bytes_per_step": 8 * N ** 3},
-            "stencil": {"metric": "Stencil::apply 7-point FP64 256^3 GB/s", "value": st_gbs, "unit": "GB/s",
-                        "frac_of_hbm": st_gbs / peak, "us_per_apply": t_st * 1e6,
-                        "gpts_per_s": 256 ** 3 / t_st / 1e9, "algorithmic_bytes": STENCIL_BYTES},
-            "roofline": {"bound": "hbm", "kernel": "k_star_tma<Lap7,EpiRelax> (finest-level Jacobi sweep)",
-                         "achieved": rx_gbs, "peak": peak, "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
-                         "unit": "GB/s", "frac": rx_gbs / peak, "traffic": traffic,
-                         "algorithmic_bytes_per_launch": RELAX_BYTES, "us_per_launch": t_rx * 1e6},
-            "gpu_launches": launches * args.steps,
-            "clocks": clk,
-            "mixed": {"metric": "MG solves/s, FP32 cycles with FP64 residual/correction", "value": value_m,
-                      "unit": "solves/s", "speedup_vs_fp64": value_m / value, "iters_per_solve": itm,
-                      "final_rel_residual": histm[-1] / histm[0], "max_rel_err_vs_fp64_solution": err_m,
-                      "latency_ms": {"p50": lat_m[len(lat_m) // 2],
-                                     "p99": lat_m[min(len(lat_m) - 1, int(0.99 * len(lat_m)))]},
-                      "relax_fp32_us": t_rx32 * 1e6, "relax_fp32_gbs": 12 * 256 ** 3 / t_rx32 / 1e9,
-                      "gpu_launches": (2 + itm * mgm.launches_per_cycle() + 1) * args.steps},
         }
         if precision is not None:
             line["mixed_384"] = precision
@@ -703,10 +704,33 @@ def main():
                 line["cpu_baseline"] = cpu_reference_cycles(1, 2, gpu_cycles=iters)
             except Exception as e:  # the baseline never hides the GPU result
                 line["cpu_baseline"] = {"error": str(e)}
-        try:
-            os.makedirs(os.path.join(ROOT, "profiles"), exist_ok=True)
-        except OSError:
-            pass
+        # the short sections last (a log that keeps only the end of the line keeps them)
+        line["stencil"] = {"metric": "Stencil::apply 7-point FP64 256^3 GB/s", "value": st_gbs, "unit": "GB/s",
+                           "frac_of_hbm": st_gbs / peak, "us_per_apply": t_st * 1e6,
+                           "gpts_per_s": 256 ** 3 / t_st / 1e9, "algorithmic_bytes": STENCIL_BYTES,
+                           "traffic": traffic.get("k_star_tma_apply_f64_256")}
+        line["mixed"] = {"metric": "MG solves/s, FP32 cycles with FP64 residual/correction", "value": value_m,
+                         "unit": "solves/s", "speedup_vs_fp64": value_m / value, "iters_per_solve": itm,
+                         "final_rel_residual": histm[-1] / histm[0], "max_rel_err_vs_fp64_solution": err_m,
+                         "latency_ms": {"p50": lat_m[len(lat_m) // 2],
+                                        "p99": lat_m[min(len(lat_m) - 1, int(0.99 * len(lat_m)))]},
+                         "relax_fp32_us": t_rx32 * 1e6, "relax_fp32_frac": 12 * 256 ** 3 / t_rx32 / 1e9 / peak,
+                         "relax2_fp32_us": t_rx32_2 * 1e6, "relax2_fp32_frac": 12 * 256 ** 3 / t_rx32_2 / 1e9 / peak,
+                         "gpu_launches": (2 + itm * mgm.launches_per_cycle() + 1) * args.steps}
+        line["relax_single_sweep"] = {"kernel": "k_star_tma<Lap7,double,EpiRelax> (one Jacobi sweep, 256^3)",
+                                      "us_per_launch": t_rx * 1e6, "achieved_gbs": rx_gbs, "frac": rx_gbs / peak,
+                                      "algorithmic_bytes_per_launch": RELAX_BYTES,
+                                      "traffic": traffic.get("k_star_tma_relax_f64_256")}
+        line["roofline"] = {"bound": "hbm", "kernel": "k_relax2<double,256> (two finest-level Jacobi sweeps per pass)",
+                            "achieved": rx2_gbs, "peak": peak,
+                            "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)", "unit": "GB/s",
+                            "frac": rx2_gbs / peak, "traffic": traffic.get("k_relax2_f64_256"),
+                            "algorithmic_bytes_per_launch": RELAX_BYTES, "us_per_launch": t_rx2 * 1e6,
+                            "sweeps_per_launch": 2}
+        line["e2e"] = {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": 8 * N ** 3,
+                       "d2h_bytes_per_step": 8 * N ** 3}
+        line["clocks"] = clk
+        line["gpu_launches"] = launches * args.steps
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()

@@ -28,8 +28,8 @@
 // Every phi1 and phi2 value is computed with EpiRelax's arithmetic (taps in the 7-point
 // Laplacian's insertion order, one rounding per operation, relax_value), from the same inputs, so
 // the result is bitwise two launches of the single-sweep kernel. With NORM the pass also takes the
-// max-norm residual of phi0 at every cell it evaluates phi1 on (EpiRelaxNorm's second sum), which
-// covers the whole level.
+// max-norm residual of phi0 (EpiRelaxNorm's second sum) at the cells of its own rows and planes,
+// so at every cell of the level once.
 // Waits are bounded: a stencil thread whose wait expires makes every stencil thread leave at the
 // next barrier (barrier reduction), and the producer drains its copies in flight before the CTA
 // exits.
@@ -277,6 +277,11 @@ __global__ void __launch_bounds__(2 * NXT + 32, relax2_min_blocks(2 * NXT + 32))
             const T* c = cst + ly0 * bw;
             const T* rt = cst + tile0 + br0 * BWR;            // rho(p) of phi1 row 0
             T* b1w = b1 + (t & 1) * tilea + br0 * N;
+            // all rows are computed before any is published: a store between them would keep the
+            // next row's shared-memory loads behind it (the compiler cannot tell the buffers apart),
+            // serialising the rows' independent chains
+            T v1s[J][PV];
+            [[maybe_unused]] const bool own_plane = t >= 1 && t <= nzl;   // p in [zb, zb + nzl)
 #pragma unroll
             for (int j = 0; j < J; j++) {
 #pragma unroll
@@ -299,7 +304,8 @@ __global__ void __launch_bounds__(2 * NXT + 32, relax2_min_blocks(2 * NXT + 32))
                     acc = dadd(acc, dmul(a.c.c[5], tpz));
                     acc = dadd(acc, dmul(a.c.c[6], tmz));
                     const T v1 = rv(acc, tc, rho, al);
-                    if constexpr (NORM) {
+                    // the norm at the tile's own rows and planes only: every cell of the level once
+                    if (NORM && j - JO >= 0 && j - JO < RG && own_plane) {
                         T a2 = HELM ? T(0) : dsub(T(0), rho);
                         a2 = dadd(a2, dmul(a.c2.c[0], tc));
                         a2 = dadd(a2, dmul(a.c2.c[1], tpx));
@@ -311,7 +317,7 @@ __global__ void __launch_bounds__(2 * NXT + 32, relax2_min_blocks(2 * NXT + 32))
                         if constexpr (!HELM) m = upd_abs(m, (double)a2);
                         else m = upd_abs(m, (double)dsub(rho, dsub(dmul(al, tc), dmul(a.beta, a2))));
                     }
-                    b1w[j * N + xs[v]] = v1;
+                    v1s[j][v] = v1;
                     const int r = j - JO;   // output row of phi1 row j (a constant once unrolled)
                     if (r >= 0 && r < RG) p1[PH][r < 0 ? 0 : (r >= RG ? RG - 1 : r)][v] = v1;
                     if (r >= 0 && r < RG) {
@@ -320,6 +326,10 @@ __global__ void __launch_bounds__(2 * NXT + 32, relax2_min_blocks(2 * NXT + 32))
                     }
                 }
             }
+#pragma unroll
+            for (int j = 0; j < J; j++)
+#pragma unroll
+                for (int v = 0; v < PV; v++) b1w[j * N + xs[v]] = v1s[j][v];
             __syncwarp();
             if (lane == 0) mbar_arrive(&empty[sc]);   // centre plane done (its taps and rho)
             // ---- phi2(p-1) on the output rows ----
@@ -328,6 +338,7 @@ __global__ void __launch_bounds__(2 * NXT + 32, relax2_min_blocks(2 * NXT + 32))
                 const T* b1r = b1 + ((t - 1) & 1) * tilea + (br0 + JO) * N;   // output row 0
                 const int ez = edge_code(p - 1, N);
                 const long long ozv = ez == 1 ? (long long)N * Sz : -(long long)N * Sz;
+                T v2s[RG][PV];
 #pragma unroll
                 for (int r = 0; r < RG; r++) {
 #pragma unroll
@@ -348,7 +359,16 @@ __global__ void __launch_bounds__(2 * NXT + 32, relax2_min_blocks(2 * NXT + 32))
                         acc = dadd(acc, dmul(a.c.c[6], tmz));
                         T al = T(0);
                         if constexpr (HELM) al = ao2[r][v];
-                        const T v2 = rv(acc, tc, ro2[r][v], al);
+                        v2s[r][v] = rv(acc, tc, ro2[r][v], al);
+                    }
+                }
+                // stores after every row's value (global stores would otherwise order the next
+                // row's shared-memory loads behind them)
+#pragma unroll
+                for (int r = 0; r < RG; r++) {
+#pragma unroll
+                    for (int v = 0; v < PV; v++) {
+                        const T v2 = v2s[r][v];
                         T* q = orow + r * sx + 32 * v;
                         const int ox = oxv[v], oy = oyr[r];
                         *q = v2;

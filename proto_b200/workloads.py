@@ -38,6 +38,27 @@ def sine_modes_rhs(n, seed=1, modes=8, kmax=8, amplitudes=None):
     return f
 
 
+def sine_modes_rhs_device(n, seed, modes=4, kmax=8, device="cuda"):
+    """sine_modes_rhs evaluated in FP64 on a torch device (the same wave vectors and amplitudes from
+    the same seeded generator; the sums run on the device, so the last bits may differ from the
+    numpy evaluation). Used to make many large right-hand sides quickly."""
+    import torch
+    rng = np.random.default_rng(seed)
+    ks = rng.integers(1, kmax + 1, size=(modes, 3))
+    amps = rng.standard_normal(modes)
+    x = (torch.arange(n, dtype=torch.float64, device=device) + 0.5) / n
+    f = torch.zeros((n, n, n), dtype=torch.float64, device=device)
+    for (kx, ky, kz), a in zip(ks, amps):
+        sx, cx = torch.sin(2 * np.pi * int(kx) * x), torch.cos(2 * np.pi * int(kx) * x)
+        sy, cy = torch.sin(2 * np.pi * int(ky) * x), torch.cos(2 * np.pi * int(ky) * x)
+        sz, cz = torch.sin(2 * np.pi * int(kz) * x), torch.cos(2 * np.pi * int(kz) * x)
+        sxy = sx[None, :] * cy[:, None] + cx[None, :] * sy[:, None]
+        cxy = cx[None, :] * cy[:, None] - sx[None, :] * sy[:, None]
+        f += float(a) * (sxy[None, :, :] * cz[:, None, None] + cxy[None, :, :] * sz[:, None, None])
+    f -= f.mean()
+    return f
+
+
 def poisson_rho(n, seed=1, modes=8):
     """Right-hand side in the reference multigrid's sign convention (L_h phi = rho) for -Lap u = f."""
     return -sine_modes_rhs(n, seed=seed, modes=modes)

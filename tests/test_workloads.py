@@ -69,3 +69,20 @@ def test_amr_level_tiles_the_periodic_domain():
     assert cells == dom[0] * dom[1] * dom[2] == 20959232
     starts = {lo for lo, _ in boxes}
     assert len(starts) == 512
+
+
+def test_one_right_hand_side_per_request():
+    """Every request carries its own seed, and the device evaluation of its right-hand side (run here
+    on the CPU through torch) agrees with the numpy evaluation to rounding."""
+    import torch
+    t = S.make_trace()
+    seeds = [r["seed"] for r in t]
+    assert len(set(seeds)) == len(t)
+    for r in t[:3]:
+        n = 32
+        a = W.sine_modes_rhs(n, seed=r["seed"], modes=4)
+        b = W.sine_modes_rhs_device(n, r["seed"], modes=4, device="cpu").numpy()
+        assert np.max(np.abs(a - b)) <= 1e-12 * np.max(np.abs(a))
+    x = W.sine_modes_rhs_device(32, t[0]["seed"], device="cpu")
+    y = W.sine_modes_rhs_device(32, t[1]["seed"], device="cpu")
+    assert not torch.equal(x, y)

@@ -227,6 +227,12 @@ int pb_mg_set_alpha(pb_mg* mg, const double* alpha, void* stream);
  * solution. hist (host, max_iter+1 doubles, may be NULL) receives the residual norms; *iters the
  * number of V-cycles. Blocks until the solve ends. */
 int pb_mg_solve(pb_mg* mg, const double* rhs, double* phi, int* iters, double* hist, void* stream);
+/* pb_mg_solve with this call's cycle limit and tolerance in place of the parameters' (max_iter >= 0;
+ * 0 only measures the initial residual). The archived LevelMultigrid's vCycle() and resnorm()
+ * (examples/_archived/LevelMultigrid/src/LevelMultigrid.cpp:71-88,133-158) are one cycle and no
+ * cycle of this. hist holds max_iter+1 doubles. Blocks. */
+int pb_mg_solve_n(pb_mg* mg, const double* rhs, double* phi, int max_iter, double tol, int* iters, double* hist,
+                  void* stream);
 /* LevelMultigridSolver's relax on the finest level: 'sweeps' Jacobi sweeps of the solver's current
  * state (the state left by the last pb_mg_solve). Enqueued only; does not synchronise. */
 int pb_mg_relax(pb_mg* mg, int sweeps, void* stream);
@@ -256,6 +262,13 @@ int pb_mg_relax2_shape(int zc, int cells_per_thread, int rows_per_group);
  * lambda = 0.5/(6/h^2) Jacobi, 10 bottom sweeps, FAS coarse force and correction; stops when
  * res < tol*res0 (max norm). Residual history and solution are bitwise the reference's. */
 typedef struct pb_fas pb_fas;
+/* BoxOp<T,1,0>::operator()(output, state, scale) of BoxOp_Laplace on one box (reference:
+ * include/base/implem/Proto_BoxOpImplem.H:130-175 with examples/_common/BoxOp_Laplace.H:22-27):
+ * out = ((0 + sum_d DIV_d(DiffCellToFace(d, Lo, 4)(state) / dx) / dx) * flux_scale) * scale (the
+ * last product only when scale != 1), on 'range' (empty: all of out_box). state (on state_box) must
+ * cover range grown by 2 (PB_ERR_GHOST). Bitwise the reference's operator. Enqueued only. */
+int pb_boxop_laplace_f64(const double* state, pb_box state_box, double* out, pb_box out_box, pb_box range, double dx,
+                         double flux_scale, double scale, void* stream);
 int pb_fas_create(int n, int num_levels, pb_fas** out);
 int pb_fas_destroy(pb_fas* m);
 /* force, phi: device n^3 (x fastest); phi is the initial guess and receives the solution; hist

@@ -101,6 +101,11 @@ class Port:
     def plain_apply(self, n, u, out, h, a, b):
         return self.lib.or_plain_apply(_c_int(n), _p(u), _p(out), _c_dbl(h), _c_dbl(a), _c_dbl(b))
 
+    def boxop_laplace(self, u, s_box, out, o_box, r_box, dx, flux_scale=1.0, scale=1.0):
+        return self.lib.or_boxop_laplace(_p(u), _p(_i3(s_box[0])), _p(_i3(s_box[1])), _p(out), _p(_i3(o_box[0])),
+                                         _p(_i3(o_box[1])), _p(_i3(r_box[0])), _p(_i3(r_box[1])), _c_dbl(dx),
+                                         _c_dbl(flux_scale), _c_dbl(scale))
+
     def periodic_steps(self, L, g, coefs, offs, h, dt, steps, u):
         coefs = _f64(coefs)
         offs = _i3(offs)
@@ -216,6 +221,11 @@ class Ref:
                                           _c_int(nu_bottom), _c_dbl(omega), _c_dbl(tol), _p(rhs), _c_int(ncycles),
                                           ctypes.byref(t0), _p(t_end), ctypes.byref(done))
         return first, done.value, t0.value, t_end
+
+    def boxop_laplace(self, u, s_box, out, o_box, dx, flux_scale=1.0, scale=1.0):
+        """The reference's BoxOp_Laplace::operator()(out, state, scale) on out's box."""
+        return self.lib.ref_boxop_laplace(_p(u), _p(_i3(s_box[0])), _p(_i3(s_box[1])), _p(out), _p(_i3(o_box[0])),
+                                          _p(_i3(o_box[1])), _c_dbl(dx), _c_dbl(flux_scale), _c_dbl(scale))
 
     def level13_steps(self, widths, ghost, h, dt, steps, data):
         arrs = [_i3(w) for w in widths]

@@ -609,6 +609,38 @@ static void fas_coefs(double dx, double* dc)
     dc[5] = (s != 1.0) ? -1.0 * s : -1.0;
 }
 
+/* BoxOp<BoxOp_Laplace>::operator()(out, state, scale) on a box (BoxOp::operator(),
+ * include/base/implem/Proto_BoxOpImplem.H:130-175; flux: examples/_common/BoxOp_Laplace.H:22-27):
+ * divFlux = 0, then per direction divFlux += DIV_d(flux_d, 1/dx) with flux_d |= GRAD_d(state, 1/dx);
+ * out = 0 + divFlux; out *= fluxScale; out *= scale when scale != 1. state on [sLo,sHi], out on
+ * [oLo,oHi], evaluated on range [rLo,rHi]. */
+int or_boxop_laplace(const double* u, const int* sLo, const int* sHi, double* out, const int* oLo, const int* oHi,
+                     const int* rLo, const int* rHi, double dx, double fluxScale, double scale)
+{
+    double dc[6];
+    fas_coefs(dx, dc);
+    long Sx = (long)sHi[0] - sLo[0] + 1, Sxy = Sx * ((long)sHi[1] - sLo[1] + 1);
+    long Ox = (long)oHi[0] - oLo[0] + 1, Oxy = Ox * ((long)oHi[1] - oLo[1] + 1);
+    for (int z = rLo[2]; z <= rHi[2]; z++)
+        for (int y = rLo[1]; y <= rHi[1]; y++)
+            for (int x = rLo[0]; x <= rHi[0]; x++) {
+                long c = (x - sLo[0]) + Sx * (y - sLo[1]) + Sxy * (z - sLo[2]);
+                double div = 0.0;
+                for (int d = 0; d < 3; d++) {
+                    long e = d == 0 ? 1 : (d == 1 ? Sx : Sxy);
+                    double fp = 0.0, fm = 0.0;
+                    for (int k = 0; k < 4; k++) fp = fp + dc[k] * u[c + e + (k - 2) * e];
+                    for (int k = 0; k < 4; k++) fm = fm + dc[k] * u[c + (k - 2) * e];
+                    div = div + dc[4] * fp;
+                    div = div + dc[5] * fm;
+                }
+                double v = (0.0 + div) * fluxScale;
+                if (scale != 1.0) v = v * scale;
+                out[(x - oLo[0]) + Ox * (y - oLo[1]) + Oxy * (z - oLo[2])] = v;
+            }
+    return 0;
+}
+
 typedef struct {
     int N, levels;      /* finest edge; number of levels (finest index levels-1) */
     double** u;         /* per level (n+4)^3 */

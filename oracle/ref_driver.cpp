@@ -11,7 +11,7 @@
 //
 // Reference code exercised (paths relative to the reference project root):
 //   Stencil library + hostApply ........ include/base/implem/Proto_StencilDefs.H, Proto_StencilImplem.H:725-828
-//   InterpStencil::Constant/Linear ..... include/base/implem/Proto_InterpStencilDefs.H:1-35
+//   InterpStencil::Constant/Linear/Quadratic include/base/implem/Proto_InterpStencilDefs.H:1-80
 //   LevelBoxData::exchange ............. include/base/implem/Proto_LevelBoxDataImplem.H:315-329, 900-951
 //   Reduction<T,OP,HOST> ............... include/base/implem/Proto_ReductionImplem.H:62-101
 //   LevelMultigrid (archived, 7-pt CS) . examples/_archived/LevelMultigrid/src/LevelMultigrid.cpp
@@ -330,7 +330,8 @@ int ref_interp_apply(int kind, int ratio, const double* src, const int* srcLo, c
                      double* dst, const int* dstLo, const int* dstHi, int overwrite, double scale)
 {
     InterpStencil<double> I = (kind == 0) ? InterpStencil<double>::Constant(Point::Ones(ratio))
-                                          : InterpStencil<double>::Linear(Point::Ones(ratio));
+                            : (kind == 1) ? InterpStencil<double>::Linear(Point::Ones(ratio))
+                                          : InterpStencil<double>::Quadratic(Point::Ones(ratio));
     BoxData<double,1,HOST> s(src, mkbox(srcLo, srcHi), 1), d(dst, mkbox(dstLo, dstHi), 1);
     if (overwrite) d |= I(s, scale); else d += I(s, scale);
     return 0;
@@ -566,6 +567,25 @@ int ref_mg_cs_cycles(int N, int boxSize, int levels, int nu1, int nu2, int nuBot
     }
     *solves_done = done;
     return first;
+}
+
+// BoxOp_Laplace::operator()(output, state, scale) of the reference on one box (state and output alias
+// caller memory), with the flux scale set through BoxOp::setFluxScale.
+int ref_boxop_laplace(const double* u, const int* sLo, const int* sHi, double* out, const int* oLo, const int* oHi,
+                      double dx, double fluxScale, double scale)
+{
+    Box sb = mkbox(sLo, sHi), ob = mkbox(oLo, oHi);
+    BoxData<double,1,HOST> state(const_cast<double*>(u), sb, 1);
+    BoxData<double,1,HOST> output(out, ob, 1);
+    // the operator is defined on a one-box layout of the output box (it only keeps dx from it)
+    Array<bool,DIM> per; per.fill(false);
+    ProblemDomain pd(ob, per);
+    DisjointBoxLayout layout(pd, ob.sizes());
+    BoxOp_Laplace<double,HOST> op;
+    op.define(layout, *layout.begin(), dx);
+    op.setFluxScale(fluxScale);
+    op(output, state, scale);
+    return 0;
 }
 
 // ---- AMR-level stepping on uneven patches (per-patch BoxData, ghost fill by BoxData::copyTo) ----

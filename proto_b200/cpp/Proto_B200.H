@@ -27,9 +27,17 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/proto_b200.h"
+
+// Point is usable in device code (the forall kernels of Proto_B200_Forall.cuh) when compiled by nvcc.
+#ifdef __CUDACC__
+#define PB_HD __host__ __device__
+#else
+#define PB_HD
+#endif
 
 namespace Proto {
 
@@ -51,34 +59,34 @@ inline void check(int s, const char* where)
 struct Point {
     int v[3] = {0, 0, 0};
     Point() = default;
-    Point(int x, int y, int z) { v[0] = x; v[1] = y; v[2] = z; }
-    int& operator[](int d) { return v[d]; }
-    int operator[](int d) const { return v[d]; }
-    static Point Zeros() { return Point(0, 0, 0); }
-    static Point Ones(int s = 1) { return Point(s, s, s); }
-    static Point Basis(int dir, int s = 1) { Point p; p.v[dir] = s; return p; }
-    static Point X() { return Basis(0); }
-    static Point Y() { return Basis(1); }
-    static Point Z() { return Basis(2); }
-    Point operator+(const Point& o) const { return Point(v[0] + o[0], v[1] + o[1], v[2] + o[2]); }
-    Point operator-(const Point& o) const { return Point(v[0] - o[0], v[1] - o[1], v[2] - o[2]); }
-    Point operator-() const { return Point(-v[0], -v[1], -v[2]); }
-    Point operator*(const Point& o) const { return Point(v[0] * o[0], v[1] * o[1], v[2] * o[2]); }
-    Point operator*(int s) const { return Point(v[0] * s, v[1] * s, v[2] * s); }
-    static int fdiv(int a, int b)
+    PB_HD Point(int x, int y, int z) { v[0] = x; v[1] = y; v[2] = z; }
+    PB_HD int& operator[](int d) { return v[d]; }
+    PB_HD int operator[](int d) const { return v[d]; }
+    PB_HD static Point Zeros() { return Point(0, 0, 0); }
+    PB_HD static Point Ones(int s = 1) { return Point(s, s, s); }
+    PB_HD static Point Basis(int dir, int s = 1) { Point p; p.v[dir] = s; return p; }
+    PB_HD static Point X() { return Basis(0); }
+    PB_HD static Point Y() { return Basis(1); }
+    PB_HD static Point Z() { return Basis(2); }
+    PB_HD Point operator+(const Point& o) const { return Point(v[0] + o[0], v[1] + o[1], v[2] + o[2]); }
+    PB_HD Point operator-(const Point& o) const { return Point(v[0] - o[0], v[1] - o[1], v[2] - o[2]); }
+    PB_HD Point operator-() const { return Point(-v[0], -v[1], -v[2]); }
+    PB_HD Point operator*(const Point& o) const { return Point(v[0] * o[0], v[1] * o[1], v[2] * o[2]); }
+    PB_HD Point operator*(int s) const { return Point(v[0] * s, v[1] * s, v[2] * s); }
+    PB_HD static int fdiv(int a, int b)
     {
         if (a * b >= 0) return a / b;
         if ((-a) % b == 0) return -(-a / b);
         return -(-a / b + 1);
     }
-    Point operator/(const Point& o) const { return Point(fdiv(v[0], o[0]), fdiv(v[1], o[1]), fdiv(v[2], o[2])); }
-    Point operator/(int s) const { return (*this) / Ones(s); }
-    Point operator%(const Point& o) const { return Point(v[0] % o[0], v[1] % o[1], v[2] % o[2]); }
-    bool operator==(const Point& o) const { return v[0] == o[0] && v[1] == o[1] && v[2] == o[2]; }
-    bool operator!=(const Point& o) const { return !(*this == o); }
-    int sumAbs() const { return std::abs(v[0]) + std::abs(v[1]) + std::abs(v[2]); }
-    int min() const { return std::min(v[0], std::min(v[1], v[2])); }
-    int max() const { return std::max(v[0], std::max(v[1], v[2])); }
+    PB_HD Point operator/(const Point& o) const { return Point(fdiv(v[0], o[0]), fdiv(v[1], o[1]), fdiv(v[2], o[2])); }
+    PB_HD Point operator/(int s) const { return (*this) / Ones(s); }
+    PB_HD Point operator%(const Point& o) const { return Point(v[0] % o[0], v[1] % o[1], v[2] % o[2]); }
+    PB_HD bool operator==(const Point& o) const { return v[0] == o[0] && v[1] == o[1] && v[2] == o[2]; }
+    PB_HD bool operator!=(const Point& o) const { return !(*this == o); }
+    PB_HD int sumAbs() const { return (v[0] < 0 ? -v[0] : v[0]) + (v[1] < 0 ? -v[1] : v[1]) + (v[2] < 0 ? -v[2] : v[2]); }
+    PB_HD int min() const { return v[0] < v[1] ? (v[0] < v[2] ? v[0] : v[2]) : (v[1] < v[2] ? v[1] : v[2]); }
+    PB_HD int max() const { return v[0] > v[1] ? (v[0] > v[2] ? v[0] : v[2]) : (v[1] > v[2] ? v[1] : v[2]); }
 };
 
 namespace Side { enum LoHiSide { Lo = 0, Hi = 1 }; }
@@ -627,28 +635,122 @@ void applyFused(const Stencil<T>& L, int epilogue, const BoxData<T, 1, DEVICE>& 
 template <typename T>
 class InterpStencil {
 public:
-    static InterpStencil Constant(int r) { InterpStencil s; s.m_ratio = r; return s; }
+    enum Kind { CONSTANT = 0, LINEAR = 1, QUADRATIC = 2 };
+    InterpStencil() = default;
+    // InterpStencil<T>::Constant / Linear / Quadratic (Proto_InterpStencilDefs.H:1-80): per
+    // direction, one dest-refined 1-D stencil per fine offset s < r
+    static InterpStencil Constant(int r) { return Constant(Point::Ones(r)); }
     static InterpStencil Constant(const Point& r)
     {
-        if (r[0] != r[1] || r[1] != r[2]) throw Error(PB_ERR_UNSUPPORTED, "InterpStencil::Constant anisotropic");
-        return Constant(r[0]);
+        return build(CONSTANT, r, [](int, int, int) { return Stencil<T>(Shift::Zeros(), (T)1.0); });
     }
-    int ratio() const { return m_ratio; }
-    Box range(const Box& src) const { return src.refine(m_ratio); }
+    static InterpStencil Linear(int r) { return Linear(Point::Ones(r)); }
+    static InterpStencil Linear(const Point& r)
+    {
+        return build(LINEAR, r, [](int dir, int shift, int rr) {
+            const double rd = rr, sd = shift;
+            const double p = sd / rd, q = (rd - sd) / rd;
+            return Stencil<T>(Shift::Zeros(), (T)q) + Stencil<T>(Shift::Basis(dir, 1), (T)p);
+        });
+    }
+    static InterpStencil Quadratic(int r) { return Quadratic(Point::Ones(r)); }
+    static InterpStencil Quadratic(const Point& r)
+    {
+        return build(QUADRATIC, r, [](int dir, int shift, int rr) {
+            Stencil<T> S;
+            for (int ii = -1; ii <= 1; ii++) S += Stencil<T>(Shift::Basis(dir, ii), (T)qcoef(shift, rr, ii));
+            return S;
+        });
+    }
+    int ratio() const { return m_ratio[0]; }
+    const Point& ratioPoint() const { return m_ratio; }
+    Kind kind() const { return m_kind; }
+    // InterpStencil::range (Proto_InterpStencilImplem.H:35-53): the bounding box over the shifts
+    Box range(const Box& src) const
+    {
+        Point L, H;
+        for (int d = 0; d < 3; d++)
+            for (size_t s = 0; s < m_interp[d].size(); s++) {
+                Box di = m_interp[d][s].range(src);
+                if (s == 0) { L[d] = di.low()[d]; H[d] = di.high()[d]; }
+                else { L[d] = std::min(di.low()[d], L[d]); H[d] = std::max(di.high()[d], H[d]); }
+            }
+        return Box(L, H);
+    }
     struct Lazy {
         const InterpStencil* op;
         const BoxData<T, 1, DEVICE>* src;
         T scale;
     };
     Lazy operator()(const BoxData<T, 1, DEVICE>& src, T scale = 1) const { return Lazy{this, &src, scale}; }
-    void apply(BoxData<T, 1, DEVICE>& dst, const BoxData<T, 1, DEVICE>& src, bool overwrite, T scale) const
+    // InterpStencil::apply (Proto_InterpStencilImplem.H:83-112): the 1-D stages in x, y, z, then
+    // dst (|= or +=) scale * stage on range(src) & dst (or the given range). Constant with one ratio
+    // takes a single fused kernel, bitwise the staged result.
+    void apply(BoxData<T, 1, DEVICE>& dst, const BoxData<T, 1, DEVICE>& src, bool overwrite, T scale,
+               Box rangeBox = Box()) const
     {
-        check(pb_interp_constant_f64(m_ratio, src.dp(), src.box().c(), dst.dp(), dst.box().c(), overwrite, scale, 0),
-              "InterpStencil::apply");
+        const bool iso = m_ratio[0] == m_ratio[1] && m_ratio[1] == m_ratio[2];
+        if (m_kind == CONSTANT && iso && rangeBox.empty()) {
+            check(pb_interp_constant_f64(m_ratio[0], src.dp(), src.box().c(), dst.dp(), dst.box().c(), overwrite, scale, 0),
+                  "InterpStencil::apply");
+            return;
+        }
+        if (rangeBox.empty()) rangeBox = range(src.box()) & dst.box();
+        BoxData<T, 1, DEVICE> s0 = stage(m_interp[0], src);
+        BoxData<T, 1, DEVICE> s1 = stage(m_interp[1], s0);
+        BoxData<T, 1, DEVICE> s2 = stage(m_interp[2], s1);
+        Stencil<T> S(Shift::Zeros(), scale);
+        S.apply(s2, dst, rangeBox, overwrite, (T)1);
     }
 
 private:
-    int m_ratio = 2;
+    // qcoef of Proto_InterpStencilDefs.H:40-58 (the quadratic weights)
+    static double qcoef(int a_ni, int a_r, int a_side)
+    {
+        double n = a_ni, r = a_r, coef = 0;
+        if (a_side == -1) coef = 1.0 + 3.0 * n + 3.0 * n * n - 3.0 * r - 6.0 * n * r + 2.0 * r * r;
+        else if (a_side == 0) coef = -2.0 - 6.0 * n - 6.0 * n * n + 3.0 * r + 6.0 * n * r + 5.0 * r * r;
+        else if (a_side == 1) coef = -(-1.0 - 3.0 * n - 3.0 * n * n + r * r);
+        coef /= (6.0 * r * r);
+        return coef;
+    }
+    template <class F>
+    static InterpStencil build(Kind kind, const Point& r, F make)
+    {
+        if (r.min() <= 0) throw Error(PB_ERR_ARG, "InterpStencil: non-positive refinement ratio");
+        InterpStencil I;
+        I.m_kind = kind;
+        I.m_ratio = r;
+        for (int d = 0; d < 3; d++)
+            for (int sft = 0; sft < r[d]; sft++) {
+                Stencil<T> S = make(d, sft, r[d]);
+                Point ratio = Point::Ones();
+                ratio[d] = r[d];
+                S.destRatio() = ratio;
+                S.destShift() = Point::Basis(d, sft);
+                I.m_interp[d].push_back(S);
+            }
+        return I;
+    }
+    // InterpStencil1D applied as a LazyStencil into a new BoxData (Proto_InterpStencil1DImplem.H:88-118):
+    // the output covers the bounding box of the shifts' ranges, each shift fills its own cells
+    static BoxData<T, 1, DEVICE> stage(const std::vector<Stencil<T>>& S, const BoxData<T, 1, DEVICE>& src)
+    {
+        Box R;
+        for (size_t s = 0; s < S.size(); s++) {
+            Box r = S[s].range(src.box());
+            R = (s == 0) ? r : ((R & r.low()) & r.high());
+        }
+        BoxData<T, 1, DEVICE> out(R);
+        for (size_t s = 0; s < S.size(); s++) {
+            Box b(src.box().low() - S[s].span().low(), src.box().high() - S[s].span().high());
+            S[s].apply(src, out, b.taperCoarsen(S[s].srcRatio()), true, (T)1);
+        }
+        return out;
+    }
+    Kind m_kind = CONSTANT;
+    Point m_ratio = Point::Ones(2);
+    std::vector<Stencil<T>> m_interp[3];
 };
 template <typename T>
 BoxData<T, 1, DEVICE>& operator|=(BoxData<T, 1, DEVICE>& dst, typename InterpStencil<T>::Lazy&& op)
@@ -758,6 +860,19 @@ private:
 // ---------------------------------------------------------------------------------------------
 class LevelMultigrid {
 public:
+    // the archived solver's signature (examples/_archived/LevelMultigrid/src/LevelMultigrid.H:15):
+    // a periodic cube domain [0, n-1]^3 tiled by any layout, dx = 1/n, numLevels coarsenings; V(6,6),
+    // point Jacobi with weight 1/(4 DIM) (omega = 0.5), 10 bottom sweeps
+    LevelMultigrid(const DisjointBoxLayout& layout, double dx, int numLevels) : LevelMultigrid(cube_edge(layout, dx), numLevels)
+    {
+        m_layout = layout;
+    }
+    void define(const DisjointBoxLayout& layout, double dx, int numLevels) { *this = LevelMultigrid(layout, dx, numLevels); }
+    // one V-cycle on phi for right-hand side rhs (LevelMultigrid::vCycle, LevelMultigrid.cpp:133-158)
+    void vCycle(LevelBoxData<double>& phi, LevelBoxData<double>& rhs) { cycles(phi, rhs, 1); }
+    // max-norm residual of phi (LevelMultigrid::resnorm, LevelMultigrid.cpp:71-88)
+    double resnorm(LevelBoxData<double>& phi, LevelBoxData<double>& rhs) { return cycles(phi, rhs, 0); }
+
     // n: finest edge; numLevels: coarsenings (the archived driver's numLevels argument)
     LevelMultigrid(int n, int numLevels, int nu1 = 2 * 3, int nu2 = 2 * 3, int nuBottom = 10, double omega = 0.5)
     {
@@ -796,8 +911,193 @@ public:
     }
 
 private:
+    static int cube_edge(const DisjointBoxLayout& layout, double dx)
+    {
+        const Box& d = layout.domain().box;
+        const int n = d.size(0);
+        if (d.low() != Point::Zeros() || d.size(1) != n || d.size(2) != n || !layout.domain().periodic[0] ||
+            !layout.domain().periodic[1] || !layout.domain().periodic[2] || dx != 1.0 / n)
+            throw Error(PB_ERR_UNSUPPORTED, "LevelMultigrid: periodic cube [0,n-1]^3 with dx = 1/n expected");
+        return n;
+    }
+    // gathers the valid cells of phi and rhs into the solver's n^3 arrays, runs k cycles (0: the
+    // norm only), scatters phi back and refreshes its ghosts; returns the last residual norm
+    double cycles(LevelBoxData<double>& phi, LevelBoxData<double>& rhs, int k)
+    {
+        const Box dom = m_layout.domain().box;
+        if (!m_full) {
+            m_full = std::make_shared<BoxData<double, 1, DEVICE>>(dom);
+            m_rhs = std::make_shared<BoxData<double, 1, DEVICE>>(dom);
+        }
+        for (size_t i = 0; i < phi.size(); i++) {
+            phi[i].copyTo(*m_full, m_layout[i]);
+            rhs[i].copyTo(*m_rhs, m_layout[i]);
+        }
+        std::vector<double> hist(k + 1);
+        int it = 0;
+        check(pb_mg_solve_n(m_h.get(), m_rhs->dp(), m_full->dp(), k, 0.0, &it, hist.data(), 0), "LevelMultigrid::vCycle");
+        for (size_t i = 0; i < phi.size(); i++) {
+            BoxData<double> p = phi[i];
+            m_full->copyTo(p, m_layout[i]);
+        }
+        phi.exchange();
+        return hist[it];
+    }
     pb_mg_params m_p;
     std::shared_ptr<pb_mg> m_h;
+    DisjointBoxLayout m_layout;
+    std::shared_ptr<BoxData<double, 1, DEVICE>> m_full, m_rhs;
+};
+
+// ---------------------------------------------------------------------------------------------
+// BoxOp_Laplace (examples/_common/BoxOp_Laplace.H through BoxOp::operator(),
+// include/base/implem/Proto_BoxOpImplem.H:130-175): the 4th-order flux-form Laplacian
+//   L(phi) = fluxScale * sum_d DIV_d(DiffCellToFace(d, Lo, 4)(phi) / dx) / dx   (* scale)
+// applied on the device, bitwise the reference's operator. Any class with the same
+// operator()(output, state, scale) can stand in for it in LevelOp (a plugged-in operator).
+// ---------------------------------------------------------------------------------------------
+template <typename T = double, MemType MEM = DEVICE>
+class BoxOp_Laplace {
+    static_assert(std::is_same<T, double>::value && MEM == DEVICE, "BoxOp_Laplace<double, DEVICE>");
+
+public:
+    static constexpr unsigned int numState() { return 1; }
+    static constexpr unsigned int numAux() { return 0; }
+    static constexpr int order() { return 4; }
+    static Point ghost() { return Point::Ones(2); }
+    static Point auxGhost() { return Point::Zeros(); }
+    BoxOp_Laplace() = default;
+    explicit BoxOp_Laplace(double dx) { define(dx); }
+    void define(double dx) { m_dx = dx; }
+    // BoxOp::define(layout, index, dx): the operator keeps dx
+    void define(const DisjointBoxLayout&, size_t, double dx) { define(dx); }
+    double dx() const { return m_dx; }
+    double dxMin() const { return m_dx; }
+    double spectralRadius() const { return (2.0 * 3) / (m_dx * m_dx); }
+    void setFluxScale(T s) { m_fluxScale = s; }
+    T fluxScale() const { return m_fluxScale; }
+    // output |= L(state) on output's box (state must cover it grown by ghost())
+    void operator()(BoxData<T, 1, DEVICE>& output, const BoxData<T, 1, DEVICE>& state, T scale = 1.0) const
+    {
+        check(pb_boxop_laplace_f64(state.dp(), state.box().c(), output.dp(), output.box().c(), Box().c(), m_dx,
+                                   m_fluxScale, scale, 0), "BoxOp_Laplace::operator()");
+    }
+    // out of place on a range box
+    BoxData<T, 1, DEVICE> operator()(const BoxData<T, 1, DEVICE>& state, Box range, T scale = 1.0) const
+    {
+        BoxData<T, 1, DEVICE> out(range);
+        (*this)(out, state, scale);
+        return out;
+    }
+
+private:
+    double m_dx = 1.0;
+    T m_fluxScale = 1.0;
+};
+
+// ---------------------------------------------------------------------------------------------
+// LevelOp<OpType>: the operator of every patch of a level (include/base/Proto_LevelOp.H:25-116):
+// exchange the state's ghost cells, then OpType::operator()(output[i], state[i], scale) per patch.
+// OpType is BoxOp_Laplace or any class with define(dx), operator()(BoxData&, const BoxData&, T)
+// and spectralRadius().
+// ---------------------------------------------------------------------------------------------
+template <template <typename, MemType> class OpType, typename T = double, MemType MEM = DEVICE>
+class LevelOp {
+public:
+    LevelOp() = default;
+    LevelOp(const DisjointBoxLayout& layout, T dx) { define(layout, dx); }
+    void define(const DisjointBoxLayout& layout, T dx)
+    {
+        m_layout = layout;
+        m_ops.assign(layout.size(), OpType<T, MEM>());
+        for (auto& op : m_ops) op.define(dx);
+    }
+    const OpType<T, MEM>& operator[](size_t i) const { return m_ops[i]; }
+    OpType<T, MEM>& operator[](size_t i) { return m_ops[i]; }
+    double spectralRadius() const { return m_ops.empty() ? 0.0 : m_ops[0].spectralRadius(); }
+    const DisjointBoxLayout& layout() const { return m_layout; }
+    void operator()(LevelBoxData<T>& output, LevelBoxData<T>& state, T scale = 1.0) const
+    {
+        state.exchange();
+        for (size_t i = 0; i < m_layout.size(); i++) {
+            BoxData<T> in = state[i];
+            BoxData<T> whole = output[i];
+            apply_valid(m_ops[i], whole, in, m_layout[i], scale);
+        }
+    }
+
+private:
+    // the operator on the valid box of a patch whose output field carries ghost cells: evaluate
+    // into a valid-box temporary and copy it in
+    static void apply_valid(const OpType<T, MEM>& op, BoxData<T>& out_grown, const BoxData<T>& in, const Box& valid,
+                            T scale)
+    {
+        if (out_grown.box() == valid) {
+            op(out_grown, in, scale);
+            return;
+        }
+        BoxData<T> tmp(valid);
+        op(tmp, in, scale);
+        tmp.copyTo(out_grown, valid);
+    }
+    DisjointBoxLayout m_layout;
+    std::vector<OpType<T, MEM>> m_ops;
+};
+
+// ---------------------------------------------------------------------------------------------
+// LevelMultigridSolver<BoxOp_Laplace, double> with the reference's signature
+// (include/utils/Proto_LevelMultigridSolver.H:20-51): FAS V(6,6), lambda = 0.5/spectralRadius,
+// 10 bottom sweeps, stop when res < tol*res0 (max norm). The layout must tile a periodic cube
+// [0, n-1]^3 with dx = 1/n and refinement ratio 2; solve() gathers the level's valid cells, runs
+// the device solver (pb_fas) and scatters the solution back. Bitwise the reference's solver.
+// ---------------------------------------------------------------------------------------------
+template <template <typename, MemType> class OpType, typename T = double, MemType MEM = DEVICE>
+class LevelMultigridSolver {
+    static_assert(std::is_same<OpType<T, MEM>, BoxOp_Laplace<double, DEVICE>>::value,
+                  "the device FAS solver implements BoxOp_Laplace<double>");
+
+public:
+    LevelMultigridSolver(DisjointBoxLayout& layout, Point refRatio, int numLevels, T dx) { define(layout, refRatio, numLevels, dx); }
+    void define(DisjointBoxLayout& layout, Point refRatio, int numLevels, T dx)
+    {
+        const Box& d = layout.domain().box;
+        const int n = d.size(0);
+        if (refRatio != Point::Ones(2) || d.low() != Point::Zeros() || d.size(1) != n || d.size(2) != n ||
+            !layout.domain().periodic[0] || !layout.domain().periodic[1] || !layout.domain().periodic[2] || dx != 1.0 / n)
+            throw Error(PB_ERR_UNSUPPORTED, "LevelMultigridSolver: periodic cube [0,n-1]^3, dx = 1/n, ratio 2 expected");
+        m_layout = layout;
+        pb_fas* h = nullptr;
+        check(pb_fas_create(n, numLevels, &h), "LevelMultigridSolver::define");
+        m_h = std::shared_ptr<pb_fas>(h, [](pb_fas* m) { pb_fas_destroy(m); });
+        m_state = std::make_shared<BoxData<double, 1, DEVICE>>(d);
+        m_force = std::make_shared<BoxData<double, 1, DEVICE>>(d);
+    }
+    // drives L(state) + force to zero from the given state; returns the last residual norm
+    T solve(LevelBoxData<T>& state, LevelBoxData<T>& force, int maxIter, T tolerance)
+    {
+        for (size_t i = 0; i < state.size(); i++) {
+            state[i].copyTo(*m_state, m_layout[i]);
+            force[i].copyTo(*m_force, m_layout[i]);
+        }
+        std::vector<double> hist(maxIter + 1);
+        int it = 0;
+        check(pb_fas_solve(m_h.get(), m_force->dp(), m_state->dp(), maxIter, tolerance, &it, hist.data(), 0),
+              "LevelMultigridSolver::solve");
+        for (size_t i = 0; i < state.size(); i++) {
+            BoxData<T> p = state[i];
+            m_state->copyTo(p, m_layout[i]);
+        }
+        state.exchange();
+        m_hist.assign(hist.begin(), hist.begin() + it + 1);
+        return (T)hist[it];
+    }
+    const std::vector<double>& history() const { return m_hist; }
+
+private:
+    DisjointBoxLayout m_layout;
+    std::shared_ptr<pb_fas> m_h;
+    std::shared_ptr<BoxData<double, 1, DEVICE>> m_state, m_force;
+    std::vector<double> m_hist;
 };
 
 } // namespace Proto

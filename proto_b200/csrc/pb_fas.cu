@@ -535,6 +535,36 @@ static FasCoef fas_coefs(double dx)
     return k;
 }
 
+// BoxOp<BoxOp_Laplace>::operator() on a box: out = ((0 + div) * flux_scale) [* scale], per cell the
+// operations of fas_op with the field's own strides (state on box sb, out on box ob, range rb).
+__global__ void __launch_bounds__(256) k_boxop_laplace(const double* __restrict__ u, Box3 sb, double* out, Box3 ob,
+                                                       Box3 rb, FasCoef k, double flux_scale, double scale,
+                                                       int apply_scale)
+{
+    const long long nx = bsize(rb, 0), ny = bsize(rb, 1), total = bvol(rb);
+    const long long Sx = bsize(sb, 0), Sxy = Sx * bsize(sb, 1);
+    const long long Ox = bsize(ob, 0), Oxy = Ox * bsize(ob, 1);
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+        const int x = rb.lo[0] + (int)(i % nx), y = rb.lo[1] + (int)((i / nx) % ny), z = rb.lo[2] + (int)(i / (nx * ny));
+        const long long c = (x - sb.lo[0]) + Sx * (y - sb.lo[1]) + Sxy * (z - sb.lo[2]);
+        double div = 0.0;
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            const long long e = d == 0 ? 1 : (d == 1 ? Sx : Sxy);
+            double fp = 0.0, fm = 0.0;
+#pragma unroll
+            for (int t = 0; t < 4; t++) fp = dadd(fp, dmul(k.g[t], u[c + e + (t - 2) * e]));
+#pragma unroll
+            for (int t = 0; t < 4; t++) fm = dadd(fm, dmul(k.g[t], u[c + (t - 2) * e]));
+            div = dadd(div, dmul(k.cp, fp));
+            div = dadd(div, dmul(k.c0, fm));
+        }
+        double v = dmul(dadd(0.0, div), flux_scale);
+        if (apply_scale) v = dmul(v, scale);
+        out[(x - ob.lo[0]) + Ox * (y - ob.lo[1]) + Oxy * (z - ob.lo[2])] = v;
+    }
+}
+
 } // namespace pb
 
 struct pb_fas {
@@ -667,6 +697,28 @@ static void fas_free(pb_fas* m)
 }
 
 extern "C" {
+
+int pb_boxop_laplace_f64(const double* state, pb_box state_box, double* out, pb_box out_box, pb_box range, double dx,
+                         double flux_scale, double scale, void* stream)
+{
+    if (!state || !out || !(dx > 0)) return PB_ERR_ARG;
+    const Box3 sb = to_box(state_box), ob = to_box(out_box);
+    Box3 rb = to_box(range);
+    if (bempty(sb) || bempty(ob)) return PB_ERR_BOX;
+    if (bempty(rb)) rb = ob;
+    if (!contains_box(ob, rb)) return PB_ERR_BOX;
+    Box3 need = rb;
+    for (int d = 0; d < 3; d++) {
+        need.lo[d] -= kFasGhost;      // the face fluxes reach two cells down and two up
+        need.hi[d] += kFasGhost;
+    }
+    if (!contains_box(sb, need)) return PB_ERR_GHOST;
+    const long long total = bvol(rb);
+    k_boxop_laplace<<<grid_for(total, 256), 256, 0, (cudaStream_t)stream>>>(state, sb, out, ob, rb, fas_coefs(dx),
+                                                                            flux_scale, scale, scale != 1.0);
+    PB_LAUNCH_CHECK();
+    return PB_OK;
+}
 
 int pb_fas_create(int n, int num_levels, pb_fas** out)
 {

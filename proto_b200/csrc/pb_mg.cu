@@ -828,6 +828,20 @@ int pb_mg_solve(pb_mg* mg, const double* rhs, double* phi, int* iters, double* h
     return PB_OK;
 }
 
+int pb_mg_solve_n(pb_mg* mg, const double* rhs, double* phi, int max_iter, double tol, int* iters, double* hist,
+                  void* stream)
+{
+    if (!mg || max_iter < 0) return PB_ERR_ARG;
+    const int keep_iter = mg->p.max_iter;
+    const double keep_tol = mg->p.tol;
+    mg->p.max_iter = max_iter;   // the captured cycles do not depend on either
+    mg->p.tol = tol;
+    const int e = pb_mg_solve(mg, rhs, phi, iters, hist, stream);
+    mg->p.max_iter = keep_iter;
+    mg->p.tol = keep_tol;
+    return e;
+}
+
 int pb_mg_relax(pb_mg* mg, int sweeps, void* stream)
 {
     if (!mg || sweeps < 0) return PB_ERR_ARG;

@@ -113,14 +113,19 @@ def main():
     for k, (kind, r, sb, db, overwrite, scale, seed) in enumerate([
             (0, 2, ((-1, -2, 0), (5, 6, 7)), ((-3, -4, -1), (12, 13, 15)), False, 1.0, 51),
             (0, 2, ((-1, -2, 0), (5, 6, 7)), ((-3, -4, -1), (12, 13, 15)), True, 0.3, 52),
-            (0, 4, ((0, 0, 0), (3, 3, 3)), ((0, 0, 0), (15, 15, 15)), False, 1.0, 53)]):
+            (0, 4, ((0, 0, 0), (3, 3, 3)), ((0, 0, 0), (15, 15, 15)), False, 1.0, 53),
+            (1, 2, ((-1, -2, 0), (5, 6, 7)), ((-3, -4, -1), (12, 13, 15)), False, 1.0, 54),
+            (1, 2, ((-1, -2, 0), (5, 6, 7)), ((-3, -4, -1), (12, 13, 15)), True, 0.3, 55),
+            (1, 4, ((0, 0, 0), (3, 3, 3)), ((0, 0, 0), (15, 15, 15)), False, 1.0, 56),
+            (2, 2, ((-1, -2, 0), (5, 6, 7)), ((-3, -4, -1), (12, 13, 15)), False, 1.0, 57),
+            (2, 3, ((0, 0, 0), (4, 4, 4)), ((0, 0, 0), (14, 14, 14)), True, 2.0, 58)]):
         rng = np.random.default_rng(seed)
         src = rng.uniform(-1, 1, box_vol(sb))
         dst = rng.uniform(-1, 1, box_vol(db))
         R.interp_apply(kind, r, src, sb, dst, db, overwrite, scale)
         arrays["interp_%d" % k] = dst
-        meta["interp"].append({"ratio": r, "src": sb, "dst": db, "overwrite": overwrite, "scale": scale,
-                               "seed": seed})
+        meta["interp"].append({"kind": kind, "ratio": r, "src": sb, "dst": db, "overwrite": overwrite,
+                               "scale": scale, "seed": seed})
     # multigrid residual histories (inputs: the sine-mode right-hand side, seed 1)
     cases = {
         "archived_32": dict(kind="archived", N=32, box=16, numLevels=5, maxIter=20, tol=1e-10),

@@ -94,7 +94,9 @@ def test_multigrid_parameter_rules():
     lp = L.pb_mg_launches_per_cycle
     try:
         # one launch per step: (nu1 + nu2 + 2) per level above the coarsest, the bottom, the norm;
-        # with nu1 >= 1 the FP64 norm rides on the next cycle's first sweep
+        # with nu1 >= 1 the FP64 norm rides on the next cycle's first sweep (two-sweep passes off;
+        # where a GPU runs them, they are counted in test_gpu_relax2.py)
+        assert L.pb_mg_relax2_min_edge(0) == 0
         assert L.pb_mg_coarse_edge(0) == 0
         assert lp(ctypes.byref(P(n=256, levels=6, nu1=4, nu2=4, nu_bottom=10).c)) == 6 * 10 + 10
         assert lp(ctypes.byref(P(n=256, levels=6, nu1=0, nu2=4, nu_bottom=10).c)) == 6 * 6 + 10 + 1
@@ -109,6 +111,7 @@ def test_multigrid_parameter_rules():
         assert L.pb_mg_coarse_edge(-1) == -1
     finally:
         L.pb_mg_coarse_edge(8)
+        L.pb_mg_relax2_min_edge(128)
 
 
 def test_serve_host_rules():

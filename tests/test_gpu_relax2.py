@@ -89,3 +89,17 @@ def test_tall_tiles_bitwise(pb, N, levels, precision):
     a = _solve(pb, N, levels, precision, None, max_iter=2, rg=4, bottom=1)
     b = _solve(pb, N, levels, precision, None, max_iter=2, relax2=0, bottom=1)
     assert a[1] == b[1] and np.array_equal(a[2], b[2])
+
+
+def test_launch_count_with_pairs(pb):
+    """pb_mg_launches_per_cycle counts a two-sweep pass as one launch: 256^3 V(4,4) over 6 levels with
+    the coarse levels (edge <= 8) as one kernel: 256 and 128 take pairs (256: the norm pass does the
+    first two sweeps, then one pair before and two after the coarse correction; 128: a sweep from
+    zero, a pair, a single sweep, two pairs), 64..16 one launch per sweep."""
+    import ctypes
+    L = pb.lib()
+    p = pb.MGParams(n=256, levels=6, nu1=4, nu2=4, nu_bottom=10)
+    n = L.pb_mg_launches_per_cycle(ctypes.byref(p.c))
+    # 256: 1 pair + restrict + prolong + 2 pairs; 128: first + pair + single + restrict + prolong + 2 pairs;
+    # 64, 32, 16: 4 + 4 sweeps + restrict + prolong; the coarse kernel; the norm pass
+    assert n == (1 + 1 + 1 + 2) + (1 + 1 + 1 + 1 + 1 + 2) + 3 * 10 + 1 + 1

@@ -159,3 +159,21 @@ def test_port_fas_bitwise(golden, port):
     assert n == cfg["iters"]
     assert list(h) == cfg["hist"]
     assert digest(phi) == cfg["phi_sha256"]
+
+
+def test_boxop_laplace_port_matches_reference(port):
+    """The C restatement of BoxOp_Laplace::operator() (flux form, flux scale, scale) against the
+    reference's own operator on an offset box."""
+    from oracle.oracle import Ref
+    if not Ref.available():
+        pytest.skip("reference-built oracle not present")
+    R = Ref()
+    rng = np.random.default_rng(3)
+    sb, ob = ((-2, -1, -3), (13, 12, 10)), ((0, 1, -1), (11, 10, 8))
+    u = rng.uniform(-1, 1, int(np.prod([sb[1][d] - sb[0][d] + 1 for d in range(3)])))
+    nout = int(np.prod([ob[1][d] - ob[0][d] + 1 for d in range(3)]))
+    for fs, sc in ((1.0, 1.0), (-1.0, 1.0), (-1.0, 0.37)):
+        a, b = np.zeros(nout), np.zeros(nout)
+        port.boxop_laplace(u, sb, a, ob, ob, 1.0 / 16, fs, sc)
+        R.boxop_laplace(u, sb, b, ob, 1.0 / 16, fs, sc)
+        assert np.array_equal(a, b)

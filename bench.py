@@ -276,6 +276,49 @@ def run_amr_level(pb, torch, steps=100, reps=5, cpu=True, tune=True):
     return out
 
 
+def run_sharded_level(pb, torch, dist, rank, world, steps=20, warmup=3):
+    """The uneven AMR level (512 patches, seed 2) sharded over the ranks: each rank owns a Morton
+    run of 512/N patches in its own device level, a step = local ghost exchange + pack of the
+    remote ghost regions + one grouped NCCL send/recv round with the neighbour ranks + unpack +
+    u += dt*L13(u) on the rank's patches. Total work is fixed as N grows (strong scaling); the time
+    is the slowest rank's, on CUDA events between barriers."""
+    from proto_b200 import workloads as W
+    from proto_b200 import sharding as SH
+    boxes, L = W.amr_patches(W.amr_widths(seed=2))
+    domain = ((0, 0, 0), tuple(v - 1 for v in L))
+    sl = SH.ShardedLevel(boxes, 2, domain, (1, 1, 1), rank, world, SH.DistComm())
+    S = pb.Stencil(LAP13_COEFS, LAP13_OFFS)
+    u = torch.rand(sl.slab_elems, dtype=torch.float64, device="cuda") * 2 - 1
+    tmp = torch.zeros_like(u)
+    h = 1.0 / L[0]
+    scale, dt = 1.0 / (h * h), 0.1 * h * h
+    for _ in range(warmup):
+        sl.step(S, u, tmp, scale, dt)
+        u, tmp = tmp, u
+    dist.barrier()
+    torch.cuda.synchronize()
+    st = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(steps):
+        sl.step(S, u, tmp, scale, dt)
+        u, tmp = tmp, u
+    e1.record(st)
+    torch.cuda.synchronize()
+    dist.barrier()
+    t = max_over_ranks_of(e0.elapsed_time(e1) / 1000.0 / steps, dist, "cuda")
+    m = sl.absmax(u)
+    pb.device_check()
+    interior = sum((b[1][0] - b[0][0] + 1) * (b[1][1] - b[0][1] + 1) * (b[1][2] - b[0][2] + 1) for b in boxes)
+    halo = sum(b.numel() for b in sl.sbuf.values())
+    return {"workload": "512 patches, domain %dx%dx%d, 2 ghosts, 13-point 4th-order, u += dt*L(u), sharded over "
+                        "%d ranks (Morton runs), NCCL halo exchange every step" % (L[0], L[1], L[2], world),
+            "scaling": "strong", "ranks": world, "patches_per_rank": len(sl.mine), "us_per_step": t * 1e6,
+            "steps_per_s": 1.0 / t, "gpts_per_s": interior / t / 1e9, "halo_bytes_sent_per_step_rank0": 8 * halo,
+            "peers_rank0": len(sl.sbuf), "absmax_after": m,
+            "gpu_launches_per_step": 3 + (1 if sl.rbuf else 0)}
+
+
 def run_precision(pb, torch, n=384, levels=7, reps=3):
     """Mixed precision at 384^3: the 8-mode Poisson problem (seed 1) and the Helmholtz variant
     alpha u - beta L u = f with alpha ~ U[0.1, 1] per cell (seed 3), beta = 1; V(4,4), omega = 2/3,
@@ -661,6 +704,7 @@ def main():
     pb.device_check()
     value_m = whole_job_rate(world, args.steps, t_mx)
     amr = None if (world > 1 or args.no_amr) else run_amr_level(pb, torch)
+    sharded = None if (world == 1 or args.no_amr) else run_sharded_level(pb, torch, dist, rank, world)
     precision = None if (world > 1 or args.no_precision) else run_precision(pb, torch)
     fas = None if (world > 1 or args.no_fas) else run_fas(pb, torch, cpu=not args.no_cpu_baseline)
     # the serving replay is a one-GPU measurement (replicas add nothing to it)
@@ -694,6 +738,8 @@ def main():
             line["fas"] = fas
         if amr is not None:
             line["amr_level"] = amr
+        if sharded is not None:
+            line["amr_level_sharded"] = sharded
         if serving is not None:
             line["serving"] = serving
         if iters != GPU_CYCLES_PER_SOLVE:

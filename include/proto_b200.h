@@ -161,6 +161,21 @@ int pb_level_destroy(pb_level* lv);
 int pb_level_layout(const pb_level* lv, long long* offsets /* npatch, may be NULL */,
                     long long* slab_elems, int* nitems);
 int pb_level_exchange_f64(const pb_level* lv, double* slab, void* stream);
+/* Halo transfer of a level sharded over several processes (reference: the remote half of
+ * Copier::execute, include/base/implem/Proto_CopierImplem.H:307-460, which packs motion items into
+ * MPI buffers): a plan is a list of regions, each a box of one patch of this (local) level in that
+ * patch's coordinates, inside its grown box, with its element offset in a contiguous buffer
+ * (components as consecutive blocks of the region's volume). Pack copies the regions' cells into the
+ * buffer, unpack copies the buffer into the regions (ghost cells); one launch each. The caller moves
+ * the buffers between processes (NCCL or any transport). */
+typedef struct { int patch; pb_box region; long long offset; } pb_halo_item;
+typedef struct pb_halo_plan pb_halo_plan;
+int pb_halo_plan_create(const pb_level* lv, const pb_halo_item* items, int n, pb_halo_plan** out);
+int pb_halo_plan_destroy(pb_halo_plan* plan);
+/* buffer elements the plan addresses (-1 for NULL) */
+long long pb_halo_plan_elems(const pb_halo_plan* plan);
+int pb_halo_pack_f64(const pb_halo_plan* plan, const double* slab, double* buffer, void* stream);
+int pb_halo_unpack_f64(const pb_halo_plan* plan, double* slab, const double* buffer, void* stream);
 /* Batched stencil step over every patch of a level, one launch: out = u + a*S(u, scale) on each
  * patch's valid box (PB_EPI_EULER), or out = S(u, scale) (epilogue 0). u and out are slabs of the
  * same level. */

@@ -227,6 +227,15 @@ class Ref:
         return self.lib.ref_boxop_laplace(_p(u), _p(_i3(s_box[0])), _p(_i3(s_box[1])), _p(out), _p(_i3(o_box[0])),
                                           _p(_i3(o_box[1])), _c_dbl(dx), _c_dbl(flux_scale), _c_dbl(scale))
 
+    def load_balance(self, points, nranks):
+        """The reference's BoxPartition assignment of patch index points to nranks processes."""
+        pts = np.ascontiguousarray(np.asarray(points, dtype=np.int32).reshape(-1))
+        owner = np.zeros(len(points), dtype=np.int32)
+        rc = self.lib.ref_load_balance(_p(pts), _c_int(len(points)), _c_int(nranks), _p(owner))
+        if rc != 0:
+            raise RuntimeError("ref_load_balance: %d" % rc)
+        return owner.tolist()
+
     def level13_steps(self, widths, ghost, h, dt, steps, data):
         arrs = [_i3(w) for w in widths]
         counts = _i3([len(w) for w in widths])

@@ -652,4 +652,29 @@ int ref_level13_steps(const int* nx, const int* ny, const int* nz, const int* co
     return 0;
 }
 
+// BoxPartition(patchDomain, patches, 0, nranks): Morton::sort, then loadBalance's contiguous
+// segments (include/base/implem/Proto_BoxPartitionImplem.H:35-54,196-222). owner[i] is the process
+// of points[i] (input order). The patch domain is the bounding box of the points, periodic.
+int ref_load_balance(const int* points, int n, int nranks, int* owner)
+{
+    if (n <= 0 || nranks <= 0) return -1;
+    std::vector<Point> pts;
+    Point hi = Point::Zeros();
+    for (int i = 0; i < n; i++) {
+        Point p(points[3*i], points[3*i+1], points[3*i+2]);
+        pts.push_back(p);
+        for (int d = 0; d < 3; d++) if (p[d] > hi[d]) hi[d] = p[d];
+    }
+    ProblemDomain pd(Box(Point::Zeros(), hi), true);
+    BoxPartition part(pd, pts, 0, (unsigned int)nranks);
+    const auto& assigned = part.partition();
+    if ((int)assigned.size() != n) return -2;
+    for (int i = 0; i < n; i++) {
+        owner[i] = -1;
+        for (const auto& a : assigned) if (a.first == pts[i]) { owner[i] = (int)a.second; break; }
+        if (owner[i] < 0) return -3;
+    }
+    return 0;
+}
+
 } // extern "C"

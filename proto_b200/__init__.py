@@ -79,6 +79,8 @@ def lib():
         L.pb_mg_launches_per_cycle.argtypes = [ctypes.POINTER(pb_mg_params)]
         L.pb_serve_device_bytes.restype = _c_ll
         L.pb_serve_request_bytes.restype = _c_ll
+        L.pb_halo_plan_elems.restype = _c_ll
+        L.pb_halo_plan_elems.argtypes = [_vp]
         L.pb_serve_status.argtypes = [_vp, _c_ll, ctypes.POINTER(_c_int), ctypes.POINTER(_c_int),
                                       ctypes.POINTER(_c_dbl)]
         for name in ("pb_stencil_apply_f64", "pb_stencil_apply_f32", "pb_stencil_apply_fused_f64",

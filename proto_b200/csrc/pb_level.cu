@@ -44,6 +44,34 @@ __global__ void __launch_bounds__(256) k_exchange(double* slab, const MotionItem
     }
 }
 
+// Cross-rank halo transfer of a sharded level: one item per region of one local patch (source cells
+// to pack, or ghost cells to fill) and its place in a contiguous buffer; gridDim.y blocks per item
+// (blockIdx.x), consecutive threads on consecutive cells of the region (x fastest), components as
+// blocks of the region's volume.
+struct HaloItem {
+    long long poff, gvol;      // slab offset and grown-box volume of the patch
+    int glo[3], gS[3];         // grown box: low corner, extents
+    int rlo[3], rn[3];         // region (patch coordinates)
+    long long boff;            // buffer offset of the region's first component
+};
+
+__global__ void __launch_bounds__(256) k_halo(double* slab, double* buf, const HaloItem* __restrict__ items, int ncomp,
+                                              int unpack)
+{
+    const HaloItem it = items[blockIdx.x];
+    const long long vol = (long long)it.rn[0] * it.rn[1] * it.rn[2];
+    for (long long i = (long long)blockIdx.y * blockDim.x + threadIdx.x; i < vol; i += (long long)gridDim.y * blockDim.x) {
+        const int x = it.rlo[0] + (int)(i % it.rn[0]);
+        const long long q = i / it.rn[0];
+        const int y = it.rlo[1] + (int)(q % it.rn[1]), z = it.rlo[2] + (int)(q / it.rn[1]);
+        const long long si = it.poff + (x - it.glo[0]) + (long long)it.gS[0] * ((y - it.glo[1]) + (long long)it.gS[1] * (z - it.glo[2]));
+        for (int c = 0; c < ncomp; c++) {
+            if (unpack) slab[si + c * it.gvol] = buf[it.boff + c * vol + i];
+            else buf[it.boff + c * vol + i] = slab[si + c * it.gvol];
+        }
+    }
+}
+
 // One tile = a (tx x ty) block of (x, y) columns of one patch's valid box, each column walked over
 // zd planes by one thread. The tile shape is chosen per patch-size class (the x extent of the
 // valid box) by pb_level_autotune; the default is 16 x 16 columns, 8 planes deep.
@@ -726,7 +754,90 @@ static int launch_level_star(const pb_level* lv, int shape, const double* u, dou
     return PB_OK;
 }
 
+struct pb_halo_plan {
+    int ncomp = 1;
+    int n = 0;
+    int chunks = 1;            // blocks per item: the largest region over 2048 cells, at most 64
+    long long elems = 0;
+    pb::HaloItem* d_items = nullptr;
+};
+
+static int halo_run(const pb_halo_plan* hp, double* slab, double* buf, int unpack, cudaStream_t st)
+{
+    if (!hp || !slab || (!buf && hp->n > 0)) return PB_ERR_ARG;
+    if (hp->n == 0) return PB_OK;
+    k_halo<<<dim3(hp->n, hp->chunks), 256, 0, st>>>(slab, buf, hp->d_items, hp->ncomp, unpack);
+    PB_LAUNCH_CHECK();
+    return PB_OK;
+}
+
 extern "C" {
+
+int pb_halo_plan_create(const pb_level* lv, const pb_halo_item* items, int n, pb_halo_plan** out)
+{
+    if (!lv || !out || n < 0 || (n > 0 && !items)) return PB_ERR_ARG;
+    std::vector<HaloItem> h;
+    long long elems = 0, maxvol = 0;
+    for (int k = 0; k < n; k++) {
+        const int p = items[k].patch;
+        if (p < 0 || p >= (int)lv->patches.size() || items[k].offset < 0) return PB_ERR_ARG;
+        Box3 g = lv->patches[p];
+        for (int d = 0; d < 3; d++) {
+            g.lo[d] -= lv->ghost[d];
+            g.hi[d] += lv->ghost[d];
+        }
+        const Box3 r = to_box(items[k].region);
+        if (bempty(r) || !contains_box(g, r)) return PB_ERR_BOX;
+        HaloItem it{};
+        it.poff = lv->offsets[p];
+        it.gvol = bvol(g);
+        for (int d = 0; d < 3; d++) {
+            it.glo[d] = g.lo[d];
+            it.gS[d] = (int)bsize(g, d);
+            it.rlo[d] = r.lo[d];
+            it.rn[d] = (int)bsize(r, d);
+        }
+        it.boff = items[k].offset;
+        elems = std::max(elems, it.boff + bvol(r) * lv->ncomp);
+        maxvol = std::max(maxvol, bvol(r));
+        h.push_back(it);
+    }
+    pb_halo_plan* hp = new (std::nothrow) pb_halo_plan;
+    if (!hp) return PB_ERR_NOMEM;
+    hp->ncomp = lv->ncomp;
+    hp->n = n;
+    hp->elems = elems;
+    hp->chunks = (int)std::min<long long>(64, std::max<long long>(1, (maxvol + 2047) / 2048));
+    if (n > 0 && (cudaMalloc(&hp->d_items, sizeof(HaloItem) * n) != cudaSuccess ||
+                  cudaMemcpy(hp->d_items, h.data(), sizeof(HaloItem) * n, cudaMemcpyHostToDevice) != cudaSuccess)) {
+        cudaGetLastError();
+        cudaFree(hp->d_items);
+        delete hp;
+        return PB_ERR_CUDA;
+    }
+    *out = hp;
+    return PB_OK;
+}
+
+int pb_halo_plan_destroy(pb_halo_plan* hp)
+{
+    if (!hp) return PB_OK;
+    cudaFree(hp->d_items);
+    delete hp;
+    return PB_OK;
+}
+
+long long pb_halo_plan_elems(const pb_halo_plan* hp) { return hp ? hp->elems : -1; }
+
+int pb_halo_pack_f64(const pb_halo_plan* hp, const double* slab, double* buffer, void* stream)
+{
+    return halo_run(hp, const_cast<double*>(slab), buffer, 0, (cudaStream_t)stream);
+}
+
+int pb_halo_unpack_f64(const pb_halo_plan* hp, double* slab, const double* buffer, void* stream)
+{
+    return halo_run(hp, slab, const_cast<double*>(buffer), 1, (cudaStream_t)stream);
+}
 
 int pb_level_create(const pb_box* patches, int npatch, const int ghost[3], pb_box domain, const int periodic[3],
                     int ncomp, pb_level** out)

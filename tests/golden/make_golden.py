@@ -66,6 +66,10 @@ BOX_CASES = [((-5, -4, -3), (6, 7, 9), (2, 2, 2)), ((-7, 0, 3), (-1, 5, 5), (2, 
              ((1, -9, -8), (15, -2, 8), (4, 4, 2)), ((0, 0, 0), (63, 63, 63), (2, 2, 2))]
 
 
+PARTITION_CASES = [((2, 2, 2), 2), ((2, 2, 2), 3), ((4, 4, 4), 5), ((3, 5, 2), 4), ((8, 8, 8), 7), ((1, 1, 7), 3),
+                   ((6, 3, 4), 8)]
+
+
 def digest(a):
     return hashlib.sha256(np.ascontiguousarray(a, dtype="<f8").tobytes()).hexdigest()
 
@@ -182,6 +186,13 @@ def main():
     for lo, hi, r in BOX_CASES:
         meta["box"].append({"lo": lo, "hi": hi, "ratio": r, "coarsen": R.box_op(0, lo, hi, r),
                             "taper": R.box_op(1, lo, hi, r), "refine": R.box_op(2, lo, hi, r)})
+    # BoxPartition: process of each patch index point (points listed in a seeded shuffled order)
+    meta["partition"] = []
+    prng = np.random.default_rng(12)
+    for shape, nranks in PARTITION_CASES:
+        pts = [(x, y, z) for z in range(shape[2]) for y in range(shape[1]) for x in range(shape[0])]
+        pts = [pts[k] for k in prng.permutation(len(pts))]
+        meta["partition"].append({"points": pts, "nranks": nranks, "owner": R.load_balance(pts, nranks)})
     np.savez_compressed(os.path.join(OUT, "golden_arrays.npz"), **arrays)
 
     def conv(o):

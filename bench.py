@@ -214,6 +214,22 @@ def profile_kernels(pb, torch):
     pb.device_check()
 
 
+def profile_solve(pb, torch, precision):
+    """Two solves of the bench's 256^3 problem (the second one is the one a launch list reads)."""
+    from proto_b200 import workloads as W
+    prec = pb.MG_MIXED if precision == "mixed" else 0
+    mg = pb.Multigrid(pb.MGParams(n=N, levels=LEVELS, nu1=NU1, nu2=NU2, nu_bottom=NU_BOTTOM, omega=OMEGA,
+                                  max_iter=MAX_ITER, tol=TOL, precision=prec))
+    rho = torch.from_numpy(W.poisson_rho(N, seed=1).reshape(-1).copy()).cuda()
+    phi = torch.zeros(N ** 3, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        phi.zero_()
+        it, _ = mg.solve(rho, phi)
+    torch.cuda.synchronize()
+    pb.device_check()
+    print(json.dumps({"cycles": it, "launches_per_solve": 3 + it * mg.launches_per_cycle() + 1}))
+
+
 LAP13_OFFS = [(1, 0, 0), (0, 0, 0), (-1, 0, 0), (2, 0, 0), (-2, 0, 0), (0, 1, 0), (0, -1, 0), (0, 2, 0), (0, -2, 0),
               (0, 0, 1), (0, 0, -1), (0, 0, 2), (0, 0, -2)]
 LAP13_COEFS = [4.0 / 3, -7.5, 4.0 / 3, -1.0 / 12, -1.0 / 12] + [4.0 / 3, 4.0 / 3, -1.0 / 12, -1.0 / 12] * 2
@@ -516,6 +532,8 @@ def main():
     ap.add_argument("--no-amr", action="store_true", help="skip the AMR-level section (and its tile autotuning)")
     ap.add_argument("--profile-kernels", action="store_true",
                     help="run one 256^3 FP64 sweep, one FP32 sweep and one Stencil::apply, then exit (for ncu)")
+    ap.add_argument("--profile-solve", choices=["f64", "mixed"], default=None,
+                    help="two 256^3 solves only (for launch lists)")
     ap.add_argument("--profile-level", action="store_true",
                     help="run the AMR-level setup and 2 graph steps with default tiles, then exit (for ncu)")
     ap.add_argument("--profile-serving", action="store_true",
@@ -539,6 +557,8 @@ def main():
     torch.cuda.set_device(local)
     if args.profile_kernels:
         return profile_kernels(pb, torch)
+    if args.profile_solve:
+        return profile_solve(pb, torch, args.profile_solve)
     if args.profile_level:
         return run_amr_level(pb, torch, steps=2, reps=1, cpu=False, tune=False)
     if args.profile_serving:

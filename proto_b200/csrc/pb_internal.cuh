@@ -107,6 +107,12 @@ __device__ __forceinline__ float dmul(float a, float b) { return __fmul_rn(a, b)
 __device__ __forceinline__ float dadd(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ float dsub(float a, float b) { return __fsub_rn(a, b); }
 __device__ __forceinline__ float ddiv(float a, float b) { return __fdiv_rn(a, b); }
+// the quotient of a Jacobi update: FP64 keeps the correctly rounded division (the reference's
+// arithmetic, bit for bit); FP32 (mixed-precision cycles, whose error the FP64 residual and
+// correction remove) takes the reciprocal-multiply form (within 2 ulp), two instructions instead
+// of the correctly rounded division's sequence
+__device__ __forceinline__ double squot(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ float squot(float a, float b) { return __fdividef(a, b); }
 
 // Reduction<T,Abs>::update (Proto_ReductionImplem.H:87): NaN inputs leave the value unchanged.
 __device__ __forceinline__ double upd_abs(double v1, double v2)

@@ -212,11 +212,26 @@ static size_t relax2_smem(int n, int esize, bool helm, int nst, int rg = 2)
     const size_t tile0 = (size_t)(2 * rg + 4) * nb * bw, tilea = (size_t)(2 * rg + 2) * n;
     return nst * (tile0 + (helm ? 2 : 1) * tilea) * esize + 2 * tilea * esize + 16 * (size_t)nst;
 }
+// cells per thread: one at 128 and 256, two at 384 (a group of 192 threads is whole warps)
+static int relax2_cells(int n)
+{
+    if (g_relax2_pv) return g_relax2_pv;
+    return n == 384 ? 2 : 1;
+}
+// output rows per group: four (tiles of 8 rows) where three ring stages of them fit in the shared
+// memory of the CTAs the kernel is built to keep resident per SM, else two (measured on B200: tiles
+// of 8 rows where they fit take 6-16 % less time than tiles of 4)
+static int relax2_rows(int n, int esize, bool helm)
+{
+    if (g_relax2_rg) return g_relax2_rg;
+    const int per_sm = relax2_min_blocks(2 * (n / relax2_cells(n)) + 32);
+    return (size_t)per_sm * (relax2_smem(n, esize, helm, 3, 4) + 1024) <= 227 * 1024 ? 4 : 2;
+}
 // the pass needs at least three stages (two planes in use and one in flight)
 static bool relax2_edge(int n, int esize, bool helm)
 {
     return g_relax2_min_edge > 0 && n >= g_relax2_min_edge && (n == 128 || n == 256 || n == 384) &&
-           relax2_smem(n, esize, helm, 3, g_relax2_rg == 4 ? 4 : 2) <= 220 * 1024 && tma_available();
+           relax2_smem(n, esize, helm, 3, relax2_rows(n, esize, helm)) <= 220 * 1024 && tma_available();
 }
 template <typename T>
 static bool relax2_ok(const pb_mg* mg, const MGLevel<T>& L)
@@ -237,18 +252,23 @@ static int launch_relax2_t(pb_mg* mg, MGLevel<T>& L, double* result, cudaStream_
     a.beta = (T)mg->p.beta;
     a.result = result;
     relax2_segments(L.sx, (int)sizeof(T), &a.nb, &a.bw);
-    // tile boxes (all rows of an x segment) and row boxes (the tiles that wrap in y)
-    CUtensorMap map, map1, rmap, rmap1, amap, amap1;
+    // tile boxes (all rows of an x segment), and for the two tiles that wrap in y the boxes of all
+    // rows but one plus single-row boxes
+    CUtensorMap map, mapE, map1, rmap, rmapE, rmap1, amap, amapE, amap1;
     const int es = (int)sizeof(T), bwr = SH::N / (SH::N > 256 ? 2 : 1);
     int e = encode_tmap_3d(&map, L.phi[L.cur], es, L.sx, L.n + 2, L.n + 2, a.bw, SH::ROWS, 1);
+    if (e == PB_OK) e = encode_tmap_3d(&mapE, L.phi[L.cur], es, L.sx, L.n + 2, L.n + 2, a.bw, SH::ROWS - 1, 1);
     if (e == PB_OK) e = encode_tmap_3d(&map1, L.phi[L.cur], es, L.sx, L.n + 2, L.n + 2, a.bw, 1, 1);
     if (e == PB_OK) e = encode_tmap_3d(&rmap, L.rhs, es, L.n, L.n, L.n, bwr, SH::B1ROWS, 1);
+    if (e == PB_OK) e = encode_tmap_3d(&rmapE, L.rhs, es, L.n, L.n, L.n, bwr, SH::B1ROWS - 1, 1);
     if (e == PB_OK) e = encode_tmap_3d(&rmap1, L.rhs, es, L.n, L.n, L.n, bwr, 1, 1);
     if (e == PB_OK && HELM) e = encode_tmap_3d(&amap, L.alpha, es, L.n, L.n, L.n, bwr, SH::B1ROWS, 1);
+    if (e == PB_OK && HELM) e = encode_tmap_3d(&amapE, L.alpha, es, L.n, L.n, L.n, bwr, SH::B1ROWS - 1, 1);
     if (e == PB_OK && HELM) e = encode_tmap_3d(&amap1, L.alpha, es, L.n, L.n, L.n, bwr, 1, 1);
     if (e != PB_OK) return e;
     if (!HELM) {
         amap = rmap;
+        amapE = rmapE;
         amap1 = rmap1;
     }
     const int per_sm = relax2_min_blocks(SH::THREADS);
@@ -289,7 +309,7 @@ static int launch_relax2_t(pb_mg* mg, MGLevel<T>& L, double* result, cudaStream_
     if (SH::N == 384) zc = 32;
     a.zc = g_relax2_zc > 0 ? std::min(g_relax2_zc, SH::N) : zc;
     dim3 grid(tiles, (SH::N + a.zc - 1) / a.zc);
-    kern<<<grid, SH::THREADS, smem, st>>>(map, map1, rmap, rmap1, amap, amap1, a);
+    kern<<<grid, SH::THREADS, smem, st>>>(map, mapE, map1, rmap, rmapE, rmap1, amap, amapE, amap1, a);
     PB_LAUNCH_CHECK();
     L.cur = 1 - L.cur;
     return PB_OK;
@@ -298,15 +318,19 @@ static int launch_relax2_t(pb_mg* mg, MGLevel<T>& L, double* result, cudaStream_
 template <typename T, bool HELM, bool NORM>
 static int launch_relax2_form(pb_mg* mg, MGLevel<T>& L, double* result, cudaStream_t st)
 {
-    // defaults (measured on B200): two cells per thread at 128, one at 256, two at 384
-    const bool tall = g_relax2_rg == 4;
-    const bool two = g_relax2_pv == 2 || (g_relax2_pv == 0 && L.n == 128);
+    const bool tall = relax2_rows(L.n, (int)sizeof(T), HELM) == 4;
+    const bool two = relax2_cells(L.n) == 2;
     switch (L.n) {
-    case 128: return two ? launch_relax2_t<T, 64, 2, 2, HELM, NORM>(mg, L, result, st)
-                         : launch_relax2_t<T, 128, 1, 2, HELM, NORM>(mg, L, result, st);
-    case 256: return two ? launch_relax2_t<T, 128, 2, 2, HELM, NORM>(mg, L, result, st)
-                         : (tall ? launch_relax2_t<T, 256, 1, 4, HELM, NORM>(mg, L, result, st)
-                                 : launch_relax2_t<T, 256, 1, 2, HELM, NORM>(mg, L, result, st));
+    case 128:
+        if (two) return tall ? launch_relax2_t<T, 64, 2, 4, HELM, NORM>(mg, L, result, st)
+                             : launch_relax2_t<T, 64, 2, 2, HELM, NORM>(mg, L, result, st);
+        return tall ? launch_relax2_t<T, 128, 1, 4, HELM, NORM>(mg, L, result, st)
+                    : launch_relax2_t<T, 128, 1, 2, HELM, NORM>(mg, L, result, st);
+    case 256:
+        if (two) return tall ? launch_relax2_t<T, 128, 2, 4, HELM, NORM>(mg, L, result, st)
+                             : launch_relax2_t<T, 128, 2, 2, HELM, NORM>(mg, L, result, st);
+        return tall ? launch_relax2_t<T, 256, 1, 4, HELM, NORM>(mg, L, result, st)
+                    : launch_relax2_t<T, 256, 1, 2, HELM, NORM>(mg, L, result, st);
     case 384: return tall ? launch_relax2_t<T, 192, 2, 4, HELM, NORM>(mg, L, result, st)
                           : launch_relax2_t<T, 192, 2, 2, HELM, NORM>(mg, L, result, st);
     default: return PB_ERR_UNSUPPORTED;

@@ -166,7 +166,7 @@ __device__ __forceinline__ T relax_value(const RelaxCoef<T>& k, T acc, T c, T rh
 {
     if (!k.helm) return dadd(c, dadd(acc, dmul(k.neg_lambda, rho)));
     const T r = dsub(rho, dsub(dmul(al, c), dmul(k.beta, acc)));
-    return dadd(c, ddiv(dmul(k.omega, r), dadd(al, k.diagB)));
+    return dadd(c, squot(dmul(k.omega, r), dadd(al, k.diagB)));
 }
 
 // relax epilogue: auxiliary field 0 = rho, 1 = alpha (Helmholtz)

@@ -95,10 +95,11 @@ __host__ __device__ constexpr int relax2_min_blocks(int threads)
 
 template <typename T, int NXT, int PV, int RG, bool HELM, bool NORM>
 __global__ void __launch_bounds__(2 * NXT + 32, relax2_min_blocks(2 * NXT + 32))
-    k_relax2(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CUtensorMap tmap1,
-             const __grid_constant__ CUtensorMap rmap, const __grid_constant__ CUtensorMap rmap1,
-             const __grid_constant__ CUtensorMap amap, const __grid_constant__ CUtensorMap amap1,
-             const Relax2Args<T> a)
+    k_relax2(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CUtensorMap tmapE,
+             const __grid_constant__ CUtensorMap tmap1, const __grid_constant__ CUtensorMap rmap,
+             const __grid_constant__ CUtensorMap rmapE, const __grid_constant__ CUtensorMap rmap1,
+             const __grid_constant__ CUtensorMap amap, const __grid_constant__ CUtensorMap amapE,
+             const __grid_constant__ CUtensorMap amap1, const Relax2Args<T> a)
 {
     using SH = Relax2Shape<NXT, PV, RG>;
     constexpr int N = SH::N, TY = SH::TY, J = RG + 1, NA = HELM ? 2 : 1;
@@ -131,11 +132,20 @@ __global__ void __launch_bounds__(2 * NXT + 32, relax2_min_blocks(2 * NXT + 32))
     if (warp == SH::NCW) {
         // ---- producer: plane kp (= zb-2+kp, wrapped) into stage kp % nst: the phi0 tile (rows
         // y0-2 .. y0+TY+1) and the rho (and alpha) tile (rows y0-1 .. y0+TY). Inside the domain the
-        // rows of a tile are contiguous, so each x segment is one box of all its rows; the first
-        // and last row tiles wrap in y and take one box per row. Shared memory holds each segment
+        // rows of a tile are contiguous, so each x segment is one box of all its rows. The first
+        // and last row tiles wrap in y by one row: each segment is one box of the other rows (one
+        // row shorter) and one single-row box of the wrapped row. Shared memory holds each segment
         // as a dense [rows][width] block either way. ----
         if (lane == 0) {
             const bool inner = y0 >= 1 && y0 + TY <= N - 1;
+            const bool top = y0 == 0;                    // else the last tile (y0 + TY == N)
+            const int row_bytes0 = a.bw * (int)sizeof(T), row_bytesr = BWR * (int)sizeof(T);
+            // first tile: wrapped row first, then the rest from grown row 0 (phi0) / row 0 (rho);
+            // last tile: the rest from grown row N-TY-1 / row N-TY-1, then the wrapped row
+            const int e0_dst = top ? 1 : 0, e0_y = top ? 0 : N - TY - 1, w0_dst = top ? 0 : SH::ROWS - 1,
+                      w0_y = top ? N - 1 : 2;
+            const int er_dst = top ? 1 : 0, er_y = top ? 0 : N - TY - 1, wr_dst = top ? 0 : SH::B1ROWS - 1,
+                      wr_y = top ? N - 1 : 0;
             int issued = 0;
             for (int kp = 0; kp < nplanes; kp++) {
                 const int s = kp % nst;
@@ -155,20 +165,20 @@ __global__ void __launch_bounds__(2 * NXT + 32, relax2_min_blocks(2 * NXT + 32))
                         if constexpr (HELM) tma_load_3d(d + tilea * (int)sizeof(T), &amap, &full[s], xb * BWR, y0 - 1, wz);
                     }
                 } else {
-                    for (int ly = 0; ly < SH::ROWS; ly++) {
-                        const int gy = r2_grown(y0 - 2 + ly, N);
-                        for (int xb = 0; xb < a.nb; xb++)
-                            tma_load_3d(st + (xb * SH::ROWS + ly) * a.bw * (int)sizeof(T), &tmap1, &full[s], xb * a.bw, gy,
-                                        gz);
+                    for (int xb = 0; xb < a.nb; xb++) {
+                        unsigned char* d = st + xb * SH::ROWS * row_bytes0;
+                        tma_load_3d(d + e0_dst * row_bytes0, &tmapE, &full[s], xb * a.bw, e0_y, gz);
+                        tma_load_3d(d + w0_dst * row_bytes0, &tmap1, &full[s], xb * a.bw, w0_y, gz);
                     }
-                    for (int r = 0; r < SH::B1ROWS; r++) {
-                        const int wy = r2_wrap(y0 - 1 + r, N);
 #pragma unroll
-                        for (int xb = 0; xb < NBR; xb++) {
-                            unsigned char* d = sr + (xb * SH::B1ROWS + r) * BWR * (int)sizeof(T);
-                            tma_load_3d(d, &rmap1, &full[s], xb * BWR, wy, wz);
-                            if constexpr (HELM)
-                                tma_load_3d(d + tilea * (int)sizeof(T), &amap1, &full[s], xb * BWR, wy, wz);
+                    for (int xb = 0; xb < NBR; xb++) {
+                        unsigned char* d = sr + xb * SH::B1ROWS * row_bytesr;
+                        tma_load_3d(d + er_dst * row_bytesr, &rmapE, &full[s], xb * BWR, er_y, wz);
+                        tma_load_3d(d + wr_dst * row_bytesr, &rmap1, &full[s], xb * BWR, wr_y, wz);
+                        if constexpr (HELM) {
+                            unsigned char* da = d + tilea * (int)sizeof(T);
+                            tma_load_3d(da + er_dst * row_bytesr, &amapE, &full[s], xb * BWR, er_y, wz);
+                            tma_load_3d(da + wr_dst * row_bytesr, &amap1, &full[s], xb * BWR, wr_y, wz);
                         }
                     }
                 }
@@ -227,7 +237,7 @@ __global__ void __launch_bounds__(2 * NXT + 32, relax2_min_blocks(2 * NXT + 32))
             if constexpr (!HELM) return dadd(c, dadd(acc, dmul(k.neg_lambda, rho)));
             else {
                 const T r = dsub(rho, dsub(dmul(al, c), dmul(k.beta, acc)));
-                return dadd(c, ddiv(dmul(k.omega, r), dadd(al, k.diagB)));
+                return dadd(c, squot(dmul(k.omega, r), dadd(al, k.diagB)));
             }
         };
 

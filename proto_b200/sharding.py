@@ -227,6 +227,7 @@ class _DevicePlan:
             arr[k].offset = off
         h = ctypes.c_void_p()
         _check(L.pb_halo_plan_create(level._h, arr, _c_int(n), ctypes.byref(h)), "pb_halo_plan_create")
+        self._lib = L        # kept for __del__, which may run while the interpreter shuts down
         self._h = h
         self.elems = L.pb_halo_plan_elems(h)
 
@@ -237,9 +238,8 @@ class _DevicePlan:
         _check(lib().pb_halo_unpack_f64(self._h, _ptr(slab), _ptr(buf), _stream(stream)), "pb_halo_unpack_f64")
 
     def __del__(self):
-        from . import _LIB
-        if getattr(self, "_h", None) and _LIB is not None:
-            _LIB.pb_halo_plan_destroy(self._h)
+        if getattr(self, "_h", None) and getattr(self, "_lib", None) is not None:
+            self._lib.pb_halo_plan_destroy(self._h)
             self._h = None
 
 

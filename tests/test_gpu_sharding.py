@@ -7,6 +7,11 @@ import pytest
 
 from proto_b200 import sharding as S
 from proto_b200 import workloads as W
+from tests.util import table
+
+# the 7-point Laplacian in Stencil<T>::Laplacian's insertion order (centre, then +e/-e per axis)
+LAP7 = ([-6.0, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0],
+        [(0, 0, 0), (1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1)])
 
 pytestmark = pytest.mark.gpu
 
@@ -72,10 +77,9 @@ def test_exchange_bitwise_the_oracle(pb, port, world, widths):
     pb.device_check()
 
 
-def _steps(pb, ranks, slabs, nsteps, h):
+def _steps(pb, ranks, slabs, nsteps, h, taps=LAP7):
     import torch
-    c = [-6.0, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0]
-    o = [(0, 0, 0), (-1, 0, 0), (1, 0, 0), (0, -1, 0), (0, 1, 0), (0, 0, -1), (0, 0, 1)]
+    c, o = taps
     st = pb.Stencil(c, o)
     tmps = [torch.zeros_like(s) for s in slabs]
     for _ in range(nsteps):
@@ -110,9 +114,9 @@ def test_steps_bitwise_the_oracle(pb, port, world, widths):
     assert max(m) == float(np.abs(ref).max())
 
 
-def test_full_size_amr_level_on_two_ranks(pb, port):
-    """The 512-patch uneven level over two ranks, 4 Euler steps of the 7-point Laplacian: bitwise
-    the oracle's periodic stepping of the whole domain."""
+def test_full_size_amr_level_on_two_ranks(golden, pb, port):
+    """The 512-patch uneven level over two ranks, 4 Euler steps of the 13-point Laplacian (the
+    reference's StencilLib table): bitwise the oracle's periodic stepping of the whole domain."""
     import torch
     g, nsteps = 2, 4
     boxes, L = W.amr_patches(W.amr_widths(seed=2))
@@ -122,7 +126,8 @@ def test_full_size_amr_level_on_two_ranks(pb, port):
     valid = np.random.default_rng(13).uniform(-1, 1, (L[2], L[1], L[0]))
     slabs = [_fill(torch, r, valid, 0.0) for r in ranks]
     h = 1.0 / L[0]
-    slabs, (c, o) = _steps(pb, ranks, slabs, nsteps, h)
+    c13, o13, _ = table(golden[1], "laplacian13")
+    slabs, (c, o) = _steps(pb, ranks, slabs, nsteps, h, (c13, [tuple(v) for v in np.asarray(o13).reshape(-1, 3)]))
     torch.cuda.synchronize()
     G = np.zeros((L[2] + 2 * g, L[1] + 2 * g, L[0] + 2 * g))
     G[g:-g, g:-g, g:-g] = valid

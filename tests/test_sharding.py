@@ -101,7 +101,8 @@ class HostBackend:
 
 
 def laplacian7():
-    offs = [(0, 0, 0), (-1, 0, 0), (1, 0, 0), (0, -1, 0), (0, 1, 0), (0, 0, -1), (0, 0, 1)]
+    """Stencil<T>::Laplacian's taps in insertion order (centre, then +e/-e per axis)."""
+    offs = [(0, 0, 0), (1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1)]
     return [-6.0, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0], offs
 
 

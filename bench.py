@@ -214,14 +214,17 @@ def profile_kernels(pb, torch):
     pb.device_check()
 
 
-def profile_solve(pb, torch, precision):
-    """Two solves of the bench's 256^3 problem (the second one is the one a launch list reads)."""
+def profile_solve(pb, torch, which):
+    """Two solves (the second one is the one a launch list reads) of the bench's 256^3 problem
+    ("f64", "mixed") or of the 384^3 Poisson configuration ("f64_384", "mixed_384": coarsest 3^3
+    solved exactly)."""
     from proto_b200 import workloads as W
-    prec = pb.MG_MIXED if precision == "mixed" else 0
-    mg = pb.Multigrid(pb.MGParams(n=N, levels=LEVELS, nu1=NU1, nu2=NU2, nu_bottom=NU_BOTTOM, omega=OMEGA,
-                                  max_iter=MAX_ITER, tol=TOL, precision=prec))
-    rho = torch.from_numpy(W.poisson_rho(N, seed=1).reshape(-1).copy()).cuda()
-    phi = torch.zeros(N ** 3, dtype=torch.float64, device="cuda")
+    prec = pb.MG_MIXED if which.startswith("mixed") else 0
+    n, levels, bottom = (384, 7, pb.MG_BOTTOM_DIRECT) if which.endswith("384") else (N, LEVELS, 0)
+    mg = pb.Multigrid(pb.MGParams(n=n, levels=levels, nu1=NU1, nu2=NU2, nu_bottom=NU_BOTTOM, omega=OMEGA,
+                                  max_iter=MAX_ITER, tol=TOL, precision=prec, bottom=bottom))
+    rho = torch.from_numpy(W.poisson_rho(n, seed=1).reshape(-1).copy()).cuda()
+    phi = torch.zeros(n ** 3, dtype=torch.float64, device="cuda")
     for _ in range(2):
         phi.zero_()
         it, _ = mg.solve(rho, phi)
@@ -532,8 +535,8 @@ def main():
     ap.add_argument("--no-amr", action="store_true", help="skip the AMR-level section (and its tile autotuning)")
     ap.add_argument("--profile-kernels", action="store_true",
                     help="run one 256^3 FP64 sweep, one FP32 sweep and one Stencil::apply, then exit (for ncu)")
-    ap.add_argument("--profile-solve", choices=["f64", "mixed"], default=None,
-                    help="two 256^3 solves only (for launch lists)")
+    ap.add_argument("--profile-solve", choices=["f64", "mixed", "f64_384", "mixed_384"], default=None,
+                    help="two solves only (for launch lists)")
     ap.add_argument("--profile-level", action="store_true",
                     help="run the AMR-level setup and 2 graph steps with default tiles, then exit (for ncu)")
     ap.add_argument("--profile-serving", action="store_true",

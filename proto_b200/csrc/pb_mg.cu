@@ -205,11 +205,11 @@ static int g_relax2_pv = 0;   // cells per thread override (0: the default per e
 static int g_relax2_rg = 0;   // output rows per group override (0: the default per edge)
 
 // shared memory of a k_relax2 CTA with nst stages (the launcher's layout)
-static size_t relax2_smem(int n, int esize, bool helm, int nst, int rg = 2)
+static size_t relax2_smem(int n, int esize, bool helm, int nst, int rg = 2, bool zero = false)
 {
     int nb, bw;
     relax2_segments(esize == 8 ? grown_pitch<double>(n) : grown_pitch<float>(n), esize, &nb, &bw);
-    const size_t tile0 = (size_t)(2 * rg + 4) * nb * bw, tilea = (size_t)(2 * rg + 2) * n;
+    const size_t tile0 = zero ? 0 : (size_t)(2 * rg + 4) * nb * bw, tilea = (size_t)(2 * rg + 2) * n;
     return nst * (tile0 + (helm ? 2 : 1) * tilea) * esize + 2 * tilea * esize + 16 * (size_t)nst;
 }
 // cells per thread: one at 128 and 256, two at 384 (a group of 192 threads is whole warps)
@@ -239,13 +239,18 @@ static bool relax2_ok(const pb_mg* mg, const MGLevel<T>& L)
     return relax2_edge(L.n, (int)sizeof(T), is_helm(mg));
 }
 
-template <typename T, int NXT, int PV, int RG, bool HELM, bool NORM>
+template <typename T, int NXT, int PV, int RG, bool HELM, bool NORM, int MODE>
 static int launch_relax2_t(pb_mg* mg, MGLevel<T>& L, double* result, cudaStream_t st)
 {
     using SH = Relax2Shape<NXT, PV, RG>;
+    constexpr bool ZERO = MODE == kRelax2Zero;
     Relax2Args<T> a;
     memset(&a, 0, sizeof(a));
     a.out = L.phi[1 - L.cur];
+    if (MODE == kRelax2Update) {
+        a.u = mg->u64;
+        a.usx = grown_pitch<double>(L.n);
+    }
     a.k = relax_coef(mg, L);
     a.c = lap7_coefs<T>(HELM ? L.hsqinv : mg->p.omega / 6.0);
     a.c2 = lap7_coefs<T>(L.hsqinv);
@@ -273,11 +278,12 @@ static int launch_relax2_t(pb_mg* mg, MGLevel<T>& L, double* result, cudaStream_
     }
     const int per_sm = relax2_min_blocks(SH::THREADS);
     int nst = 6;
-    while (nst > 3 && (size_t)per_sm * (relax2_smem(SH::N, (int)sizeof(T), HELM, nst, RG) + 1024) > 227 * 1024) nst--;
+    while (nst > 3 && (size_t)per_sm * (relax2_smem(SH::N, (int)sizeof(T), HELM, nst, RG, ZERO) + 1024) > 227 * 1024)
+        nst--;
     a.nst = nst;
-    const size_t smem = relax2_smem(SH::N, (int)sizeof(T), HELM, nst, RG);
+    const size_t smem = relax2_smem(SH::N, (int)sizeof(T), HELM, nst, RG, ZERO);
     if (smem > 220 * 1024) return PB_ERR_UNSUPPORTED;
-    auto kern = k_relax2<T, NXT, PV, RG, HELM, NORM>;
+    auto kern = k_relax2<T, NXT, PV, RG, HELM, NORM, MODE>;
     static bool attr = false;
     static int occ = 0;
     static size_t occ_smem = 0;
@@ -311,39 +317,39 @@ static int launch_relax2_t(pb_mg* mg, MGLevel<T>& L, double* result, cudaStream_
     dim3 grid(tiles, (SH::N + a.zc - 1) / a.zc);
     kern<<<grid, SH::THREADS, smem, st>>>(map, mapE, map1, rmap, rmapE, rmap1, amap, amapE, amap1, a);
     PB_LAUNCH_CHECK();
-    L.cur = 1 - L.cur;
+    if (MODE != kRelax2Update) L.cur = 1 - L.cur;
     return PB_OK;
 }
 
-template <typename T, bool HELM, bool NORM>
+template <typename T, bool HELM, bool NORM, int MODE>
 static int launch_relax2_form(pb_mg* mg, MGLevel<T>& L, double* result, cudaStream_t st)
 {
     const bool tall = relax2_rows(L.n, (int)sizeof(T), HELM) == 4;
     const bool two = relax2_cells(L.n) == 2;
     switch (L.n) {
     case 128:
-        if (two) return tall ? launch_relax2_t<T, 64, 2, 4, HELM, NORM>(mg, L, result, st)
-                             : launch_relax2_t<T, 64, 2, 2, HELM, NORM>(mg, L, result, st);
-        return tall ? launch_relax2_t<T, 128, 1, 4, HELM, NORM>(mg, L, result, st)
-                    : launch_relax2_t<T, 128, 1, 2, HELM, NORM>(mg, L, result, st);
+        if (two) return tall ? launch_relax2_t<T, 64, 2, 4, HELM, NORM, MODE>(mg, L, result, st)
+                             : launch_relax2_t<T, 64, 2, 2, HELM, NORM, MODE>(mg, L, result, st);
+        return tall ? launch_relax2_t<T, 128, 1, 4, HELM, NORM, MODE>(mg, L, result, st)
+                    : launch_relax2_t<T, 128, 1, 2, HELM, NORM, MODE>(mg, L, result, st);
     case 256:
-        if (two) return tall ? launch_relax2_t<T, 128, 2, 4, HELM, NORM>(mg, L, result, st)
-                             : launch_relax2_t<T, 128, 2, 2, HELM, NORM>(mg, L, result, st);
-        return tall ? launch_relax2_t<T, 256, 1, 4, HELM, NORM>(mg, L, result, st)
-                    : launch_relax2_t<T, 256, 1, 2, HELM, NORM>(mg, L, result, st);
-    case 384: return tall ? launch_relax2_t<T, 192, 2, 4, HELM, NORM>(mg, L, result, st)
-                          : launch_relax2_t<T, 192, 2, 2, HELM, NORM>(mg, L, result, st);
+        if (two) return tall ? launch_relax2_t<T, 128, 2, 4, HELM, NORM, MODE>(mg, L, result, st)
+                             : launch_relax2_t<T, 128, 2, 2, HELM, NORM, MODE>(mg, L, result, st);
+        return tall ? launch_relax2_t<T, 256, 1, 4, HELM, NORM, MODE>(mg, L, result, st)
+                    : launch_relax2_t<T, 256, 1, 2, HELM, NORM, MODE>(mg, L, result, st);
+    case 384: return tall ? launch_relax2_t<T, 192, 2, 4, HELM, NORM, MODE>(mg, L, result, st)
+                          : launch_relax2_t<T, 192, 2, 2, HELM, NORM, MODE>(mg, L, result, st);
     default: return PB_ERR_UNSUPPORTED;
     }
 }
 
 // Two sweeps of level L in one pass (NORM: also the max-norm residual of the state it starts from,
-// into result). The caller checks relax2_ok.
-template <typename T, bool NORM>
+// into result; MODE: from a zero state, or ending in the FP64 update). The caller checks relax2_ok.
+template <typename T, bool NORM, int MODE = kRelax2Plain>
 static int launch_relax2(pb_mg* mg, MGLevel<T>& L, double* result, cudaStream_t st)
 {
-    return is_helm(mg) ? launch_relax2_form<T, true, NORM>(mg, L, result, st)
-                       : launch_relax2_form<T, false, NORM>(mg, L, result, st);
+    return is_helm(mg) ? launch_relax2_form<T, true, NORM, MODE>(mg, L, result, st)
+                       : launch_relax2_form<T, false, NORM, MODE>(mg, L, result, st);
 }
 
 // last FP32 post-sweep of the finest level fused with u64 += e
@@ -413,12 +419,23 @@ static int launch_relax_norm(pb_mg* mg, MGLevel<double>& L, cudaStream_t st)
 }
 
 // MIXED: FP64 residual of u64 + norm + FP32 right-hand side + first FP32 sweep of the finest level
+// The mixed cycle runs its finest-level sweeps as two-sweep passes (the first pair from zero, the
+// last ending in the FP64 update) where that kernel takes the level and both sweep counts are >= 2;
+// otherwise the residual pass does the first sweep and a fused sweep the update.
+static bool mixed_pairs(const pb_mg_params& p)
+{
+    return p.precision == PB_MG_MIXED && p.nu1 >= 2 && p.nu2 >= 2 &&
+           relax2_edge(p.n, 4, p.form == PB_MG_HELMHOLTZ);
+}
+
+// FP64 residual of the solution: its max-norm into d_res, its FP32 copy as the finest FP32
+// level's right-hand side, and (unless the cycle starts with a pair from zero) the first FP32 sweep.
 static int launch_res64(pb_mg* mg, cudaStream_t st)
 {
     MGLevel<float>& L = mg->lv32.back();
     PB_CUDA(cudaMemsetAsync(mg->d_res, 0, sizeof(double), st));
     EpiRes64 epi;
-    epi.e32 = L.phi[1];
+    epi.e32 = mixed_pairs(mg->p) ? nullptr : L.phi[1];
     epi.rhs32 = L.rhs;
     epi.helm = is_helm(mg);
     epi.beta = mg->p.beta;
@@ -441,7 +458,12 @@ template <typename T>
 static int relax_sweeps(pb_mg* mg, MGLevel<T>& L, int k, bool zero_start, cudaStream_t st)
 {
     int s = 0;
-    if (zero_start && k > 0) {
+    if (zero_start && k >= 2 && relax2_ok(mg, L)) {
+        // the first two sweeps from zero as one pass (no read of the zero state)
+        int e = launch_relax2<T, false, kRelax2Zero>(mg, L, nullptr, st);
+        if (e != PB_OK) return e;
+        s = 2;
+    } else if (zero_start && k > 0) {
         int e = launch_relax(mg, L, true, st);
         if (e != PB_OK) return e;
         s = 1;
@@ -542,8 +564,14 @@ static int vcycle(pb_mg* mg, std::vector<MGLevel<T>>& lv, int l, bool zero_start
         k_prolong<T><<<prolong_grid(L.n), dim3(32, 8), 0, st>>>(L.phi[L.cur], C.phi[C.cur], L.n, L.sx, C.sx);
         PB_LAUNCH_CHECK();
         if (!fuse_update) return relax_sweeps(mg, L, mg->p.nu2, false, st);
-        if ((e = relax_sweeps(mg, L, mg->p.nu2 - 1, false, st)) != PB_OK) return e;
-        if constexpr (std::is_same<T, float>::value) return launch_relax_update(mg, L, st);
+        if constexpr (std::is_same<T, float>::value) {
+            if (mixed_pairs(mg->p)) {
+                if ((e = relax_sweeps(mg, L, mg->p.nu2 - 2, false, st)) != PB_OK) return e;
+                return launch_relax2<float, false, kRelax2Update>(mg, L, nullptr, st);
+            }
+            if ((e = relax_sweeps(mg, L, mg->p.nu2 - 1, false, st)) != PB_OK) return e;
+            return launch_relax_update(mg, L, st);
+        }
         return PB_ERR_ARG;
     }
     if (mg->p.bottom == PB_MG_BOTTOM_DIRECT) {
@@ -592,8 +620,13 @@ static int cycle_and_norm(pb_mg* mg, cudaStream_t st)
     int e;
     if (is_mixed(mg)) {
         const int top = (int)mg->lv32.size() - 1;
-        mg->lv32[top].cur = 1;   // the residual pass left the first sweep in phi[1]
-        if ((e = vcycle(mg, mg->lv32, top, false, 1, true, st)) != PB_OK) return e;
+        if (mixed_pairs(mg->p)) {
+            // the correction starts from zero: its first two sweeps are one pass
+            if ((e = vcycle(mg, mg->lv32, top, true, 0, true, st)) != PB_OK) return e;
+        } else {
+            mg->lv32[top].cur = 1;   // the residual pass left the first sweep in phi[1]
+            if ((e = vcycle(mg, mg->lv32, top, false, 1, true, st)) != PB_OK) return e;
+        }
         if ((e = launch_res64(mg, st)) != PB_OK) return e;
     } else if (fuse_norm(mg)) {
         const int top = (int)mg->lv.size() - 1;
@@ -883,7 +916,12 @@ int pb_mg_launches_per_cycle(const pb_mg_params* p)
     const bool helm = q.form == PB_MG_HELMHOLTZ;
     auto sweeps = [&](int n, int k, bool zero_start) {
         int s = 0, c = 0;
-        if (zero_start && k > 0) s = c = 1;
+        if (zero_start && k >= 2 && relax2_edge(n, es, helm)) {
+            s = 2;
+            c = 1;
+        } else if (zero_start && k > 0) {
+            s = c = 1;
+        }
         if (relax2_edge(n, es, helm))
             for (; s + 2 <= k; s += 2) c++;
         return c + (k - s);
@@ -893,12 +931,12 @@ int pb_mg_launches_per_cycle(const pb_mg_params* p)
         if (zero_start && l == ft) return 1;
         if (l > 0) {
             int c = sweeps(n, q.nu1 - pre_done, zero_start && !pre_done) + 1 + cyc(l - 1, true, 0, false) + 1;
-            c += fuse_update ? sweeps(n, q.nu2 - 1, false) + 1 : sweeps(n, q.nu2, false);
-            return c;
+            if (!fuse_update) return c + sweeps(n, q.nu2, false);
+            return c + (mixed_pairs(q) ? sweeps(n, q.nu2 - 2, false) : sweeps(n, q.nu2 - 1, false)) + 1;
         }
         return q.bottom == PB_MG_BOTTOM_DIRECT ? 1 : sweeps(n, q.nu_bottom, zero_start);
     };
-    if (q.precision == PB_MG_MIXED) return cyc(q.levels, false, 1, true) + 1;
+    if (q.precision == PB_MG_MIXED) return (mixed_pairs(q) ? cyc(q.levels, true, 0, true) : cyc(q.levels, false, 1, true)) + 1;
     if (q.nu1 >= 1 && q.levels >= 1) return cyc(q.levels, false, norm_sweeps_for(q), false) + 1;
     return cyc(q.levels, false, 0, false) + 1;
 }

@@ -297,7 +297,8 @@ struct Res64Row {
     float* r;
 };
 struct EpiRes64 {
-    float* e32;          // grown FP32 level (pitch k.sx)
+    float* e32;          // grown FP32 level (pitch k.sx); null: no first sweep (the cycle starts
+                         // with a two-sweep pass from zero)
     float* rhs32;        // n^3
     int helm;
     double beta;
@@ -310,7 +311,7 @@ struct EpiRes64 {
     __device__ __forceinline__ Row row(int x, int y, int z0, bool active) const
     {
         Row r;
-        r.e = periodic_row(e32, k.n, k.sx, x, y, z0, active);
+        r.e = periodic_row(e32 ? e32 : rhs32, k.n, k.sx, x, y, z0, active);   // rhs32: a valid base, never stored through
         r.r = active ? rhs32 + x + (long long)k.n * (y + (long long)k.n * z0) : rhs32;
         return r;
     }
@@ -334,7 +335,7 @@ struct EpiRes64 {
         m = upd_abs(m, res);
         const float r32 = __double2float_rn(res);
         r.r[(long long)zo * k.n * k.n + pv] = r32;
-        store_row<ZE>(e32, k.n, k.sx, r.e, zo, pv, relax_value(k, 0.f, 0.f, r32, al));
+        if (e32) store_row<ZE>(e32, k.n, k.sx, r.e, zo, pv, relax_value(k, 0.f, 0.f, r32, al));
     }
     __device__ __forceinline__ void end_warp() const { warp_max_atomic(m, result); }
     __device__ __forceinline__ void end_block() const { block_max_atomic(m, result); }

@@ -30,6 +30,11 @@
 // the result is bitwise two launches of the single-sweep kernel. With NORM the pass also takes the
 // max-norm residual of phi0 (EpiRelaxNorm's second sum) at the cells of its own rows and planes,
 // so at every cell of the level once.
+// Modes: kRelax2Plain; kRelax2Zero, the pair that starts a level from zero (phi1 = the sweep of a
+// zero state, from rho and alpha alone, as the first-sweep kernel computes it: no phi0 is read);
+// kRelax2Update (FP32, mixed precision), the pair that ends a cycle: phi2 is not stored but added
+// to the FP64 solution (u += (double)phi2, with u's periodic images), as the fused last-sweep
+// update computes it.
 // Waits are bounded: a stencil thread whose wait expires makes every stencil thread leave at the
 // next barrier (barrier reduction), and the producer drains its copies in flight before the CTA
 // exits.
@@ -38,9 +43,13 @@
 
 namespace pb {
 
+enum Relax2Mode : int { kRelax2Plain = 0, kRelax2Zero = 1, kRelax2Update = 2 };
+
 template <typename T>
 struct Relax2Args {
     T* out;                 // destination level (grown, pitch k.sx)
+    double* u;              // kRelax2Update: FP64 solution (grown, pitch usx)
+    int usx;
     RelaxCoef<T> k;         // n, sx, form and the smoother's scalars
     Coefs<T> c;             // smoother taps: L(., omega/6) (Poisson) | L(., 1/h^2) (Helmholtz)
     Coefs<T> c2;            // NORM: L(., 1/h^2)
@@ -93,7 +102,7 @@ __host__ __device__ constexpr int relax2_min_blocks(int threads)
     return threads <= 160 ? 3 : (threads <= 288 ? 2 : 1);
 }
 
-template <typename T, int NXT, int PV, int RG, bool HELM, bool NORM>
+template <typename T, int NXT, int PV, int RG, bool HELM, bool NORM, int MODE>
 __global__ void __launch_bounds__(2 * NXT + 32, relax2_min_blocks(2 * NXT + 32))
     k_relax2(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CUtensorMap tmapE,
              const __grid_constant__ CUtensorMap tmap1, const __grid_constant__ CUtensorMap rmap,
@@ -103,10 +112,13 @@ __global__ void __launch_bounds__(2 * NXT + 32, relax2_min_blocks(2 * NXT + 32))
 {
     using SH = Relax2Shape<NXT, PV, RG>;
     constexpr int N = SH::N, TY = SH::TY, J = RG + 1, NA = HELM ? 2 : 1;
+    constexpr bool ZERO = MODE == kRelax2Zero, UPD = MODE == kRelax2Update;
     static_assert(NXT % 32 == 0, "groups are whole warps");
+    static_assert(!(NORM && MODE != kRelax2Plain), "the norm rides on plain passes only");
+    static_assert(!UPD || sizeof(T) == 4, "the update pass belongs to mixed precision");
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int nst = a.nst;
-    const int tile0 = SH::ROWS * a.nb * a.bw;                   // phi0 tile (elements)
+    const int tile0 = ZERO ? 0 : SH::ROWS * a.nb * a.bw;        // phi0 tile (elements; none from zero)
     const int tilea = SH::B1ROWS * N;                           // rho / alpha tile (elements)
     const int stage_bytes = (tile0 + NA * tilea) * (int)sizeof(T);   // multiple of 128
     T* b1 = reinterpret_cast<T*>(smem_raw + nst * stage_bytes); // phi1 planes [2][B1ROWS][N]
@@ -156,8 +168,11 @@ __global__ void __launch_bounds__(2 * NXT + 32, relax2_min_blocks(2 * NXT + 32))
                 unsigned char* sr = st + tile0 * (int)sizeof(T);
                 mbar_arrive_expect_tx(&full[s], (uint32_t)stage_bytes);
                 if (inner) {
-                    for (int xb = 0; xb < a.nb; xb++)
-                        tma_load_3d(st + xb * SH::ROWS * a.bw * (int)sizeof(T), &tmap, &full[s], xb * a.bw, y0 - 1, gz);
+                    if constexpr (MODE != kRelax2Zero) {
+                        for (int xb = 0; xb < a.nb; xb++)
+                            tma_load_3d(st + xb * SH::ROWS * a.bw * (int)sizeof(T), &tmap, &full[s], xb * a.bw, y0 - 1,
+                                        gz);
+                    }
 #pragma unroll
                     for (int xb = 0; xb < NBR; xb++) {
                         unsigned char* d = sr + xb * SH::B1ROWS * BWR * (int)sizeof(T);
@@ -165,10 +180,12 @@ __global__ void __launch_bounds__(2 * NXT + 32, relax2_min_blocks(2 * NXT + 32))
                         if constexpr (HELM) tma_load_3d(d + tilea * (int)sizeof(T), &amap, &full[s], xb * BWR, y0 - 1, wz);
                     }
                 } else {
-                    for (int xb = 0; xb < a.nb; xb++) {
-                        unsigned char* d = st + xb * SH::ROWS * row_bytes0;
-                        tma_load_3d(d + e0_dst * row_bytes0, &tmapE, &full[s], xb * a.bw, e0_y, gz);
-                        tma_load_3d(d + w0_dst * row_bytes0, &tmap1, &full[s], xb * a.bw, w0_y, gz);
+                    if constexpr (MODE != kRelax2Zero) {
+                        for (int xb = 0; xb < a.nb; xb++) {
+                            unsigned char* d = st + xb * SH::ROWS * row_bytes0;
+                            tma_load_3d(d + e0_dst * row_bytes0, &tmapE, &full[s], xb * a.bw, e0_y, gz);
+                            tma_load_3d(d + w0_dst * row_bytes0, &tmap1, &full[s], xb * a.bw, w0_y, gz);
+                        }
                     }
 #pragma unroll
                     for (int xb = 0; xb < NBR; xb++) {
@@ -223,6 +240,16 @@ __global__ void __launch_bounds__(2 * NXT + 32, relax2_min_blocks(2 * NXT + 32))
         // plane per phi2 plane; row r, cell v at + r * sx + 32 * v. Periodic image offsets per cell
         // in x and per row in y, and the phi1 plane's x neighbours (wrapped), fixed per thread.
         T* orow = a.out + grown_index<T>(N, sx, xs[0], ys + JO, zb);
+        // kRelax2Update: the FP64 solution's cursor, pitch usx, images per row in y
+        [[maybe_unused]] double* urow = nullptr;
+        [[maybe_unused]] int uyr[MODE == kRelax2Update ? RG : 1] = {};
+        [[maybe_unused]] long long Suz = 0;
+        if constexpr (MODE == kRelax2Update) {
+            urow = a.u + grown_index<double>(N, a.usx, xs[0], ys + JO, zb);
+            Suz = (long long)a.usx * (N + 2);
+#pragma unroll
+            for (int r = 0; r < RG; r++) uyr[r] = image_offset(ys + JO + r, N, a.usx);
+        }
         int oxv[PV], xmv[PV], xpv[PV], oyr[RG];
 #pragma unroll
         for (int v = 0; v < PV; v++) {
@@ -263,7 +290,7 @@ __global__ void __launch_bounds__(2 * NXT + 32, relax2_min_blocks(2 * NXT + 32))
 
         // prologue: phi0 planes zb-2 (kp 0) and zb-1 (kp 1) into window slots 0 and 1
         const bool ok = mbar_wait(&full[0], 0) && mbar_wait(&full[1], 0);
-        if (ok) {
+        if (ok && !ZERO) {
             load_window(std::integral_constant<int, 0>{}, 0);
             load_window(std::integral_constant<int, 1>{}, 1);
         }
@@ -278,8 +305,19 @@ __global__ void __launch_bounds__(2 * NXT + 32, relax2_min_blocks(2 * NXT + 32))
             constexpr int SO = PH, SC = (PH + 1) % 3, SN = (PH + 2) % 3;
             const int p = zb - 1 + t;
             const bool got = mbar_wait(&full[sn], pn);
-            if (got) load_window(std::integral_constant<int, SN>{}, sn);
+            if (got && !ZERO) load_window(std::integral_constant<int, SN>{}, sn);
             if (consumers_any(!got, SH::NC)) return false;
+            // kRelax2Update: the FP64 solution under this step's phi2 outputs (plane p-1), read now so
+            // the loads overlap phi1
+            [[maybe_unused]] double uin[MODE == kRelax2Update ? RG : 1][PV];
+            if constexpr (MODE == kRelax2Update) {
+                if (t >= 2) {
+#pragma unroll
+                    for (int r = 0; r < RG; r++)
+#pragma unroll
+                        for (int v = 0; v < PV; v++) uin[r][v] = urow[r * a.usx + 32 * v];
+                }
+            }
             // ---- phi1(p) on rows j ----
             T rn[RG][PV];
             [[maybe_unused]] T an[HELM ? RG : 1][PV];
@@ -296,24 +334,31 @@ __global__ void __launch_bounds__(2 * NXT + 32, relax2_min_blocks(2 * NXT + 32))
             for (int j = 0; j < J; j++) {
 #pragma unroll
                 for (int v = 0; v < PV; v++) {
-                    const T* q = c + j * bw;
-                    const T tc = w0[SC][j][v];
-                    const T tpx = q[cp[v]], tmx = q[cm[v]];
-                    const T tpy = j + 1 < J ? w0[SC][j + 1][v] : q[bw + cc[v]];
-                    const T tmy = j > 0 ? w0[SC][j - 1][v] : q[cc[v] - bw];
-                    const T tpz = w0[SN][j][v], tmz = w0[SO][j][v];
                     const T rho = rt[j * BWR + cr[v]];
                     T al = T(0);
                     if constexpr (HELM) al = rt[tilea + j * BWR + cr[v]];
-                    T acc = T(0);
-                    acc = dadd(acc, dmul(a.c.c[0], tc));
-                    acc = dadd(acc, dmul(a.c.c[1], tpx));
-                    acc = dadd(acc, dmul(a.c.c[2], tmx));
-                    acc = dadd(acc, dmul(a.c.c[3], tpy));
-                    acc = dadd(acc, dmul(a.c.c[4], tmy));
-                    acc = dadd(acc, dmul(a.c.c[5], tpz));
-                    acc = dadd(acc, dmul(a.c.c[6], tmz));
-                    const T v1 = rv(acc, tc, rho, al);
+                    T v1, tc = T(0), tpx = T(0), tmx = T(0), tpy = T(0), tmy = T(0), tpz = T(0), tmz = T(0);
+                    if constexpr (MODE == kRelax2Zero) {
+                        v1 = rv(T(0), T(0), rho, al);      // the sweep of a zero state
+                    } else {
+                        const T* q = c + j * bw;
+                        tc = w0[SC][j][v];
+                        tpx = q[cp[v]];
+                        tmx = q[cm[v]];
+                        tpy = j + 1 < J ? w0[SC][j + 1][v] : q[bw + cc[v]];
+                        tmy = j > 0 ? w0[SC][j - 1][v] : q[cc[v] - bw];
+                        tpz = w0[SN][j][v];
+                        tmz = w0[SO][j][v];
+                        T acc = T(0);
+                        acc = dadd(acc, dmul(a.c.c[0], tc));
+                        acc = dadd(acc, dmul(a.c.c[1], tpx));
+                        acc = dadd(acc, dmul(a.c.c[2], tmx));
+                        acc = dadd(acc, dmul(a.c.c[3], tpy));
+                        acc = dadd(acc, dmul(a.c.c[4], tmy));
+                        acc = dadd(acc, dmul(a.c.c[5], tpz));
+                        acc = dadd(acc, dmul(a.c.c[6], tmz));
+                        v1 = rv(acc, tc, rho, al);
+                    }
                     // the norm at the tile's own rows and planes only: every cell of the level once
                     if (NORM && j - JO >= 0 && j - JO < RG && own_plane) {
                         T a2 = HELM ? T(0) : dsub(T(0), rho);
@@ -374,6 +419,34 @@ __global__ void __launch_bounds__(2 * NXT + 32, relax2_min_blocks(2 * NXT + 32))
                 }
                 // stores after every row's value (global stores would otherwise order the next
                 // row's shared-memory loads behind them)
+                if constexpr (MODE == kRelax2Update) {
+                    const long long ouz = ez == 1 ? (long long)N * Suz : -(long long)N * Suz;
+#pragma unroll
+                    for (int r = 0; r < RG; r++) {
+#pragma unroll
+                        for (int v = 0; v < PV; v++) {
+                            const double v2 = dadd(uin[r][v], (double)v2s[r][v]);
+                            double* q = urow + r * a.usx + 32 * v;
+                            const int ox = oxv[v], oy = uyr[r];
+                            *q = v2;
+                            if (ox) q[ox] = v2;
+                            if (oy) {
+                                q[oy] = v2;
+                                if (ox) q[oy + ox] = v2;
+                            }
+                            if (ez) {
+                                double* qz = q + ouz;
+                                *qz = v2;
+                                if (ox) qz[ox] = v2;
+                                if (oy) {
+                                    qz[oy] = v2;
+                                    if (ox) qz[oy + ox] = v2;
+                                }
+                            }
+                        }
+                    }
+                    urow += Suz;
+                } else {
 #pragma unroll
                 for (int r = 0; r < RG; r++) {
 #pragma unroll
@@ -399,6 +472,7 @@ __global__ void __launch_bounds__(2 * NXT + 32, relax2_min_blocks(2 * NXT + 32))
                     }
                 }
                 orow += Sz;
+                }
             }
 #pragma unroll
             for (int r = 0; r < RG; r++)

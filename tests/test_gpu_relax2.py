@@ -93,13 +93,22 @@ def test_tall_tiles_bitwise(pb, N, levels, precision):
 
 def test_launch_count_with_pairs(pb):
     """pb_mg_launches_per_cycle counts a two-sweep pass as one launch: 256^3 V(4,4) over 6 levels with
-    the coarse levels (edge <= 8) as one kernel: 256 and 128 take pairs (256: the norm pass does the
-    first two sweeps, then one pair before and two after the coarse correction; 128: a sweep from
-    zero, a pair, a single sweep, two pairs), 64..16 one launch per sweep."""
+    the coarse levels (edge <= 8) as one kernel. FP64: 256 takes pairs (the norm pass does the first
+    two sweeps, then one pair before and two after the coarse correction), 128 too (entered from
+    zero: a pair from zero and a pair, then two pairs), 64..16 one launch per sweep. Mixed: the
+    256^3 correction starts from zero (a pair from zero and a pair) and ends with a pair and the
+    pair that adds it to the FP64 solution; then the FP64 residual pass."""
     import ctypes
     L = pb.lib()
     p = pb.MGParams(n=256, levels=6, nu1=4, nu2=4, nu_bottom=10)
     n = L.pb_mg_launches_per_cycle(ctypes.byref(p.c))
-    # 256: 1 pair + restrict + prolong + 2 pairs; 128: first + pair + single + restrict + prolong + 2 pairs;
-    # 64, 32, 16: 4 + 4 sweeps + restrict + prolong; the coarse kernel; the norm pass
-    assert n == (1 + 1 + 1 + 2) + (1 + 1 + 1 + 1 + 1 + 2) + 3 * 10 + 1 + 1
+    # 64, 32, 16: 4 + 4 sweeps + restrict + prolong; the coarse kernel
+    lower = 3 * 10 + 1
+    # 128: zero pair + pair + restrict + prolong + 2 pairs
+    l128 = 1 + 1 + 1 + 1 + 2
+    # 256: 1 pair + restrict + prolong + 2 pairs; the norm pass
+    assert n == (1 + 1 + 1 + 2) + l128 + lower + 1
+    pm = pb.MGParams(n=256, levels=6, nu1=4, nu2=4, nu_bottom=10, precision=pb.MG_MIXED)
+    nm = L.pb_mg_launches_per_cycle(ctypes.byref(pm.c))
+    # 256: zero pair + pair + restrict + prolong + pair + update pair; the FP64 residual pass
+    assert nm == (1 + 1 + 1 + 1 + 1 + 1) + l128 + lower + 1

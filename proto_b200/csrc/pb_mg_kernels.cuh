@@ -524,29 +524,45 @@ static inline dim3 restrict_z_grid(int nf, int czc)
     return dim3((nf + 31) / 32, (nf / 2 + 7) / 8, (nf / 2 + czc - 1) / czc);
 }
 
-// phi += 1.0 * delta_c(p/2) on the valid box, periodic images included. Block (32, 8) over a
-// 64 x 8 tile of fine cells: each thread takes fine x and x + 32, so every warp access is 32
-// consecutive cells.
+// phi += 1.0 * delta_c(p/2) on the valid box, periodic images included. Block (32, 8): a thread
+// takes the eight fine cells x, x + 32 (every warp access 32 consecutive cells) of the two fine rows
+// and two fine planes over one coarse row and plane, so two coarse loads serve eight cells and the
+// eight fine loads are in flight together before any store.
 template <typename T>
 __global__ void __launch_bounds__(256) k_prolong(T* phi, const T* __restrict__ delta_c, int nf, int sxf, int sxc)
 {
     const int nc = nf / 2;
-    const int y = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
-    if (y >= nf) return;
-    const int ey = edge_code(y, nf), ez = edge_code(z, nf);
-    const T* drow = delta_c + grown_index<T>(nc, sxc, 0, y / 2, z / 2);
-    T* prow = phi + grown_index<T>(nf, sxf, 0, y, z);
+    const int cy = blockIdx.y * 8 + threadIdx.y, cz = blockIdx.z;
+    if (cy >= nc) return;
+    const long long Sy = sxf, Sz = (long long)sxf * (nf + 2);
+    const T* drow = delta_c + grown_index<T>(nc, sxc, 0, cy, cz);
+    T* prow = phi + grown_index<T>(nf, sxf, 0, 2 * cy, 2 * cz);
+    T d[2], v[2][2][2];          // [x half][row][plane]
+    bool in[2];
 #pragma unroll
-    for (int v = 0; v < 2; v++) {
-        const int x = blockIdx.x * 64 + v * 32 + threadIdx.x;
-        if (x < nf) {
-            const T d = __ldg(drow + x / 2);
-            T* q = prow + x;
-            store_with_images(phi, nf, sxf, q, edge_code(x, nf), ey, ez, dadd(*q, dmul(T(1), d)));
-        }
+    for (int h = 0; h < 2; h++) {
+        const int x = blockIdx.x * 64 + h * 32 + threadIdx.x;
+        in[h] = x < nf;
+        d[h] = in[h] ? __ldg(drow + x / 2) : T(0);
+#pragma unroll
+        for (int r = 0; r < 2; r++)
+#pragma unroll
+            for (int pz = 0; pz < 2; pz++) v[h][r][pz] = in[h] ? prow[x + r * Sy + pz * Sz] : T(0);
+    }
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        if (!in[h]) continue;
+        const int x = blockIdx.x * 64 + h * 32 + threadIdx.x;
+        const int ex = edge_code(x, nf);
+#pragma unroll
+        for (int r = 0; r < 2; r++)
+#pragma unroll
+            for (int pz = 0; pz < 2; pz++)
+                store_with_images(phi, nf, sxf, prow + x + r * Sy + pz * Sz, ex, edge_code(2 * cy + r, nf),
+                                  edge_code(2 * cz + pz, nf), dadd(v[h][r][pz], dmul(T(1), d[h])));
     }
 }
-static inline dim3 prolong_grid(int nf) { return dim3((nf + 63) / 64, (nf + 7) / 8, nf); }
+static inline dim3 prolong_grid(int nf) { return dim3((nf + 63) / 64, (nf / 2 + 7) / 8, nf / 2); }
 
 // n^3 <-> grown layout with periodic ghost images
 template <typename T>

@@ -258,7 +258,7 @@ int pb_mg_launches_per_cycle(const pb_mg_params* p);
  * 0 turns this off. Default 8 (measured faster than 16 for large solves). Applies to solvers
  * created and cycles captured afterwards. */
 int pb_mg_coarse_edge(int edge);
-/* Process-wide: levels of edge >= 'edge' (of the edges the two-sweep kernel is built for: 128, 256,
+/* Process-wide: levels of edge >= 'edge' (of the edges the two-sweep kernel is built for: 128, 192, 256,
  * 384) run each pair of consecutive Jacobi sweeps as one pass over the level (the intermediate
  * sweep stays on chip; same arithmetic, bitwise the same results); 0 turns this off. Default 128.
  * Applies to cycles captured afterwards. */

@@ -196,7 +196,7 @@ static int launch_relax(pb_mg* mg, MGLevel<T>& L, bool first, cudaStream_t st)
 }
 
 // ---- two sweeps per pass (k_relax2) ----------------------------------------------------------------
-// Levels of edge >= g_relax2_min_edge whose edge the kernel is built for (128, 256, 384) run each
+// Levels of edge >= g_relax2_min_edge whose edge the kernel is built for (128, 192, 256, 384) run each
 // pair of consecutive sweeps as one k_relax2 pass; 0 turns this off (every sweep a launch). The
 // results are bitwise the same either way.
 static int g_relax2_min_edge = 128;
@@ -230,7 +230,7 @@ static int relax2_rows(int n, int esize, bool helm)
 // the pass needs at least three stages (two planes in use and one in flight)
 static bool relax2_edge(int n, int esize, bool helm)
 {
-    return g_relax2_min_edge > 0 && n >= g_relax2_min_edge && (n == 128 || n == 256 || n == 384) &&
+    return g_relax2_min_edge > 0 && n >= g_relax2_min_edge && (n == 128 || n == 192 || n == 256 || n == 384) &&
            relax2_smem(n, esize, helm, 3, relax2_rows(n, esize, helm)) <= 220 * 1024 && tma_available();
 }
 template <typename T>
@@ -337,6 +337,8 @@ static int launch_relax2_form(pb_mg* mg, MGLevel<T>& L, double* result, cudaStre
                              : launch_relax2_t<T, 128, 2, 2, HELM, NORM, MODE>(mg, L, result, st);
         return tall ? launch_relax2_t<T, 256, 1, 4, HELM, NORM, MODE>(mg, L, result, st)
                     : launch_relax2_t<T, 256, 1, 2, HELM, NORM, MODE>(mg, L, result, st);
+    case 192: return tall ? launch_relax2_t<T, 192, 1, 4, HELM, NORM, MODE>(mg, L, result, st)
+                          : launch_relax2_t<T, 192, 1, 2, HELM, NORM, MODE>(mg, L, result, st);
     case 384: return tall ? launch_relax2_t<T, 192, 2, 4, HELM, NORM, MODE>(mg, L, result, st)
                           : launch_relax2_t<T, 192, 2, 2, HELM, NORM, MODE>(mg, L, result, st);
     default: return PB_ERR_UNSUPPORTED;

@@ -1,7 +1,7 @@
 """Two Jacobi sweeps per pass (k_relax2): the multigrid solves that use it are bitwise the ones that
 run every sweep as its own launch, and bitwise the C restatement's, for FP64 and mixed precision,
-Poisson and Helmholtz, on the edges the kernel is built for (128 and 256 with one cell per thread,
-384 with two), with the fused residual norm, and with small z chunks (many chunk seams)."""
+Poisson and Helmholtz, on the edges the kernel is built for (128, 192 and 256 with one cell per
+thread, 384 with two), with the fused residual norm, and with small z chunks (many chunk seams)."""
 import numpy as np
 import pytest
 
@@ -31,7 +31,7 @@ def _solve(pb, N, levels, precision, alpha=None, max_iter=3, relax2=128, zc=0, b
         L.pb_mg_relax2_shape(0, 0, 0)
 
 
-@pytest.mark.parametrize("N,levels", [(128, 5), (256, 6)])
+@pytest.mark.parametrize("N,levels", [(128, 5), (192, 6), (256, 6)])
 @pytest.mark.parametrize("form", ["poisson", "helmholtz"])
 def test_fp64_pairs_bitwise_single_sweeps_and_port(pb, port, N, levels, form):
     alpha = W.helmholtz_alpha(N, seed=3) if form == "helmholtz" else None

@@ -324,7 +324,9 @@ static int launch_relax2_t(pb_mg* mg, MGLevel<T>& L, double* result, cudaStream_
 template <typename T, bool HELM, bool NORM, int MODE>
 static int launch_relax2_form(pb_mg* mg, MGLevel<T>& L, double* result, cudaStream_t st)
 {
-    const bool tall = relax2_rows(L.n, (int)sizeof(T), HELM) == 4;
+    // the pass that also takes the residual norm keeps tiles of 4 rows: its second tap sum makes
+    // tiles of 8 rows spill (measured at 256^3: 132 us against 150 us)
+    const bool tall = (g_relax2_rg || !NORM) && relax2_rows(L.n, (int)sizeof(T), HELM) == 4;
     const bool two = relax2_cells(L.n) == 2;
     switch (L.n) {
     case 128:

@@ -454,6 +454,17 @@ def profile_serving(pb, torch, count=16, n=96, steps=2):
     pb.device_check()
 
 
+def profile_serving_mix(pb, torch, count=150):
+    """The first `count` requests of the serving trace, all available at once, through one engine
+    (for launch lists of the batched phases on the real mix of edges and forms)."""
+    from proto_b200 import serving as S
+    trace = S.make_trace(count=count)
+    data = S.TraceData(trace)
+    S.serve_trace(pb, trace, data, realtime=False, max_active=128, tol=1e-8)
+    torch.cuda.synchronize()
+    pb.device_check()
+
+
 def run_serving(pb, count):
     """Request stream of periodic Poisson/Helmholtz solves (Poisson arrivals at 200/s, seed 4; edge
     log-uniform in [32, 192] rounded to 16; alpha ~ U[0, 1]; a 4-mode right-hand side per request).
@@ -542,6 +553,8 @@ def main():
                     help="two solves only (for launch lists)")
     ap.add_argument("--profile-level", action="store_true",
                     help="run the AMR-level setup and 2 graph steps with default tiles, then exit (for ncu)")
+    ap.add_argument("--profile-serving-mix", action="store_true",
+                    help="the first 150 requests of the serving trace through one engine, then exit")
     ap.add_argument("--profile-serving", action="store_true",
                     help="16 in-flight 96^3 Helmholtz solves, 2 V-cycles (small case for kernel captures)")
     ap.add_argument("--profile-fas", action="store_true",
@@ -569,6 +582,8 @@ def main():
         return run_amr_level(pb, torch, steps=2, reps=1, cpu=False, tune=False)
     if args.profile_serving:
         return profile_serving(pb, torch)
+    if args.profile_serving_mix:
+        return profile_serving_mix(pb, torch)
     if args.profile_fas:
         return run_fas(pb, torch, sizes=(256,), reps=1, cpu=False)
     dist = None

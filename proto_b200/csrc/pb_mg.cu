@@ -545,6 +545,41 @@ static int launch_coarse_cycle(pb_mg* mg, std::vector<MGLevel<T>>& lv, int top, 
     return PB_OK;
 }
 
+// Restriction of level L's residual into C's right-hand side: FP64 levels of edge >=
+// g_restrict_star_edge through the TMA-staged star kernel (where it takes that path: 52 against
+// 80 us at 256^3), else the z-marching kernel (also for FP32 levels, where it measured faster: 182
+// against 222 us at 384^3).
+static int g_restrict_star_edge = 128;
+
+template <typename T>
+static int launch_restrict(pb_mg* mg, MGLevel<T>& L, MGLevel<T>& C, cudaStream_t st)
+{
+    const double s = is_helm(mg) ? L.hsqinv : -L.hsqinv;
+    if (std::is_same<T, double>::value && g_restrict_star_edge > 0 && L.n >= g_restrict_star_edge && L.n % 2 == 0) {
+        EpiRestrict<T> epi;
+        epi.rhs_c = C.rhs;
+        epi.nc = C.n;
+        epi.helm = is_helm(mg);
+        epi.beta = (T)mg->p.beta;
+        epi.sum = T(0);
+        StarTune tune = default_star_tune();
+        tune.mode = StarTune::TMA;
+        tune.ty = 8;
+        tune.yb = 2;
+        tune.xv = 2;
+        tune.zc = 0;     // the chunk heuristic only picks even chunks; an even edge keeps every start even
+        if (launch_star<ShapeLap7>(L.phi[L.cur], grown_box(L), valid_box(L), lap7_coefs<T>(s), epi, st, tune,
+                                   level_aux(mg, L.rhs, L.alpha, L), 2) == PB_OK)
+            return PB_OK;
+        cudaGetLastError();
+    }
+    const int czc = restrict_z_chunk(L.n, cached_sm_count());
+    k_resid_restrict_z<T><<<restrict_z_grid(L.n, czc), dim3(32, 8), 0, st>>>(
+        L.phi[L.cur], L.rhs, L.alpha, C.rhs, L.n, L.sx, is_helm(mg), lap7_coefs<T>(s), (T)mg->p.beta, czc);
+    PB_LAUNCH_CHECK();
+    return PB_OK;
+}
+
 // V-cycle on level l of hierarchy lv. pre_done: the first pre-smoothing sweep(s) already ran (the
 // mixed-precision residual pass does one, the FP64 norm pass one or two); fuse_update: the last
 // post-smoothing sweep adds its result to the FP64 solution instead of storing it.
@@ -559,11 +594,7 @@ static int vcycle(pb_mg* mg, std::vector<MGLevel<T>>& lv, int l, bool zero_start
     if (l > 0) {
         MGLevel<T>& C = lv[l - 1];
         if ((e = relax_sweeps(mg, L, mg->p.nu1 - pre_done, zero_start && !pre_done, st)) != PB_OK) return e;
-        const double s = is_helm(mg) ? L.hsqinv : -L.hsqinv;
-        const int czc = restrict_z_chunk(L.n, cached_sm_count());
-        k_resid_restrict_z<T><<<restrict_z_grid(L.n, czc), dim3(32, 8), 0, st>>>(
-            L.phi[L.cur], L.rhs, L.alpha, C.rhs, L.n, L.sx, is_helm(mg), lap7_coefs<T>(s), (T)mg->p.beta, czc);
-        PB_LAUNCH_CHECK();
+        if ((e = launch_restrict(mg, L, C, st)) != PB_OK) return e;
         if ((e = vcycle(mg, lv, l - 1, true, 0, false, st)) != PB_OK) return e;
         k_prolong<T><<<prolong_grid(L.n), dim3(32, 8), 0, st>>>(L.phi[L.cur], C.phi[C.cur], L.n, L.sx, C.sx);
         PB_LAUNCH_CHECK();

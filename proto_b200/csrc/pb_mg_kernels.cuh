@@ -426,6 +426,57 @@ __global__ void __launch_bounds__(256) k_resid_restrict(const T* __restrict__ ph
 }
 static inline dim3 restrict_grid(int nf) { return dim3((nf / 2 + 31) / 32, (nf / 2 + 7) / 8, nf / 2); }
 
+// The same coarse right-hand side through the TMA-staged star kernel (k_star_tma with two x points
+// in each of two rows per thread, chunks of an even number of planes starting on an even plane):
+// a thread's four points of a plane are the children (dx, dy) of one coarse cell and two
+// consecutive planes its dz = 0, 1, so the kernel hands the eight fine residuals of a coarse cell to
+// the same thread in Box([0,1]^3) order (x fastest). Each residual is fine_residual's arithmetic
+// (the star kernel sums the taps in the Laplacian's order from init's start value) and the eight
+// are summed as 1/8 each in that order, as k_resid_restrict does.
+template <typename T>
+struct EpiRestrict {
+    T* rhs_c;            // coarse right-hand side (nc^3)
+    int nc;
+    int helm;
+    T beta;
+    T sum;               // running sum of the thread's current coarse cell
+    struct Row {
+        T* out;          // the coarse cell under this point at the chunk's first coarse plane
+        int dy;          // child row (y & 1)
+        bool act;
+        __device__ __forceinline__ bool active() const { return act; }
+    };
+    static constexpr bool kZEdge = false;
+    static constexpr int kAux = 2;
+    __device__ __forceinline__ Row row(int x, int y, int z0, bool active) const
+    {
+        Row w;
+        w.dy = y & 1;
+        w.act = active;
+        w.out = active ? rhs_c + (x >> 1) + (long long)nc * ((y >> 1) + (long long)nc * (z0 >> 1)) : rhs_c;
+        return w;
+    }
+    __device__ __forceinline__ bool z_edge(int) const { return false; }
+    __device__ __forceinline__ T init(const Row& r, int, int, const AuxCtx& ax) const
+    {
+        if (helm || !r.act) return T(0);
+        return dadd(T(0), ax.get<T>(0));
+    }
+    template <bool ZE>
+    __device__ __forceinline__ void finish(const Row& r, int zo, int v, T acc, T c, const AuxCtx& ax)
+    {
+        const int child = v + 2 * r.dy + 4 * (zo & 1);
+        if (child == 0) sum = T(0);
+        if (!r.act) return;
+        T res = acc;
+        if (helm) res = dsub(ax.get<T>(0), dsub(dmul(ax.get<T>(1), c), dmul(beta, acc)));
+        sum = dadd(sum, dmul(T(1.0 / 8), res));
+        if (child == 7) r.out[(long long)(zo >> 1) * nc * nc] = sum;
+    }
+    __device__ __forceinline__ void end_warp() const {}
+    __device__ __forceinline__ void end_block() const {}
+};
+
 // The same coarse right-hand side, marching in z. Block (32, 8): lane = fine x (32 consecutive
 // fine cells, coalesced), threadIdx.y = coarse row cy (fine rows 2cy, 2cy+1); the block walks
 // coarse planes [cz0, cz0 + czc). Each fine row keeps phi at the fine planes 2cz-1 .. 2cz+2 in a

@@ -16,8 +16,9 @@ restriction/prolongation pair stalls at depth (reference CPU path: 0.48, 0.72, 0
   mixed_384: FP64 vs mixed at 384^3, Poisson and Helmholtz with a per-cell alpha (exact coarsest solve)
   fas   : the reference's FAS LevelMultigridSolver (4th-order flux-form Laplacian) at 64^3..256^3
   amr_level: 100 steps of exchange + 13-point Euler update over a 512-patch uneven level
-  serving: a stream of Poisson/Helmholtz requests (edges 32..192) served by the batching engine vs
-          plain FP64 multigrid one request at a time (saturated and at the 200/s arrival rate)
+  serving: a stream of Poisson/Helmholtz requests (edges 32..192) served by the batching engine
+          (mixed precision and FP64) vs plain multigrid one request at a time (saturated and at the
+          200/s arrival rate)
 
 Multi-GPU (torchrun): every rank solves its own grid (replicas; no data-path collective), value is
 the whole-job rate. --impl reference times the reference's own CPU code (oracle/_ref) on host cores.
@@ -468,13 +469,14 @@ def profile_serving_mix(pb, torch, count=150):
 def run_serving(pb, count):
     """Request stream of periodic Poisson/Helmholtz solves (Poisson arrivals at 200/s, seed 4; edge
     log-uniform in [32, 192] rounded to 16; alpha ~ U[0, 1]; a 4-mode right-hand side per request).
-    Three arms, each with pinned host buffers and the copies inside the measured time: the batching
-    engine (mixed precision, in-flight solves advanced together), plain mixed-precision multigrid
-    one request at a time, and plain FP64 multigrid one request at a time; so served / mixed-single
-    is what batching gains and mixed-single / FP64 what precision gains. At tolerance 1e-8 (the
-    configuration's) and 1e-10 (the precision target), saturated (every request available at once);
-    at 1e-8 also open loop at the arrival rate for latency. Every served result is compared with
-    the FP64 solver's solution of the same request."""
+    Four arms, each with pinned host buffers and the copies inside the measured time: the batching
+    engine in mixed precision and in FP64 (in-flight solves advanced together), plain mixed-precision
+    multigrid one request at a time, and plain FP64 multigrid one request at a time; so the two
+    served arms give what precision gains under batching, and each served arm against its
+    one-at-a-time arm what batching gains. At tolerance 1e-8 (the configuration's) and 1e-10 (the
+    precision target), saturated (every request available at once); at 1e-8 also open loop at the
+    arrival rate for latency. Every served result is compared with the FP64 solver's solution of the
+    same request (the FP64 engine's bitwise)."""
     from proto_b200 import serving as S
     trace = S.make_trace(count=count)
     t0 = time.perf_counter()
@@ -488,29 +490,37 @@ def run_serving(pb, count):
         firsts.setdefault((r["n"], r["helm"]), r)
     for tol, name in ((1e-8, "tol_1e-8"), (1e-10, "tol_1e-10")):
         eng = pb.Serve(150 << 30, max_active=SERVE_MAX_ACTIVE, tol=tol)
+        eng64 = pb.Serve(150 << 30, max_active=SERVE_MAX_ACTIVE, tol=tol, precision=pb.MG_FP64)
         fp64 = S.SingleSolvers(pb, trace, tol, pb.MG_FP64)
         mixed = S.SingleSolvers(pb, trace, tol, pb.MG_MIXED)
-        # warm-up (untimed): the engine serves the trace once, as a running server would have (its
+        # warm-up (untimed): each engine serves the trace once, as a running server would have (its
         # cache holds the hierarchies this traffic needs); every single solver solves once
         S.serve_trace(pb, trace, data, realtime=False, engine=eng)
+        S.serve_trace(pb, trace, data, realtime=False, engine=eng64)
         for r in firsts.values():
             fp64.solve(r, data.rhs_of(r["i"]))
             mixed.solve(r, data.rhs_of(r["i"]))
+        served64 = S.serve_trace(pb, trace, data, realtime=False, engine=eng64)
+        err64 = S.verify(pb, trace, data, fp64)
         served = S.serve_trace(pb, trace, data, realtime=False, engine=eng)
         err = S.verify(pb, trace, data, fp64)
         m1 = S.single_trace(pb, trace, data, mixed, realtime=False)
         f1 = S.single_trace(pb, trace, data, fp64, realtime=False)
-        res = {"saturated": {"served_mixed": served, "mixed_one_at_a_time": m1, "fp64_one_at_a_time": f1,
-                             "served_vs_fp64": served["solves_per_s"] / f1["solves_per_s"],
-                             "batching_gain": served["solves_per_s"] / m1["solves_per_s"],
-                             "precision_gain": m1["solves_per_s"] / f1["solves_per_s"]},
-               "served_rel_err_vs_fp64": err}
+        sps = lambda a: a["solves_per_s"]
+        res = {"saturated": {"served_mixed": served, "served_fp64_batched": served64, "mixed_one_at_a_time": m1,
+                             "fp64_one_at_a_time": f1,
+                             "served_vs_fp64": sps(served) / sps(f1),
+                             "precision_gain_batched": sps(served) / sps(served64),
+                             "batching_gain_fp64": sps(served64) / sps(f1),
+                             "batching_gain": sps(served) / sps(m1),
+                             "precision_gain": sps(m1) / sps(f1)},
+               "served_rel_err_vs_fp64": err, "served_fp64_rel_err_vs_fp64": err64}
         if tol == 1e-8:
             a = S.serve_trace(pb, trace, data, realtime=True, engine=eng)
             b = S.single_trace(pb, trace, data, fp64, realtime=True)
             res["arrival_rate"] = {"served_mixed": a, "fp64_one_at_a_time": b}
         out[name] = res
-        del eng, fp64, mixed
+        del eng, eng64, fp64, mixed
     return out
 
 

@@ -293,9 +293,10 @@ int pb_fas_solve(pb_fas* m, const double* force, double* phi, int max_iter, doub
 
 /* ---- Serving engine (no counterpart in the reference, which solves one grid at a time) ----------
  * Periodic Poisson/Helmholtz solves of different edges, solved together: each admitted solve keeps
- * its hierarchy on the device; one pb_serve_step runs one mixed-precision V-cycle (FP32 cycle,
- * FP64 residual, correction and norm) for every in-flight solve, each cycle phase one launch for
- * all of them, the whole step one CUDA graph. Solves are admitted between steps while the HBM
+ * its hierarchy on the device; one pb_serve_step runs one V-cycle for every in-flight solve, each
+ * cycle phase one launch for all of them, the whole step one CUDA graph. The engine's precision is
+ * PB_MG_MIXED (FP32 cycle, FP64 residual, correction and norm) or PB_MG_FP64 (every level FP64,
+ * the reference's arithmetic; nu1 + nu2 must be even). Solves are admitted between steps while the HBM
  * budget allows, up to max(2, max_active / 4) at a time with their right-hand side on its way to
  * the device (an upload stream of its own; hierarchies come from a stream-ordered pool of the
  * engine). An admitted solve takes a free slot in the same step when no requests are queued (light
@@ -303,7 +304,7 @@ int pb_fas_solve(pb_fas* m, const double* force, double* phi, int max_iter, doub
  * Solves are retired when their max-norm residual drops below tol times the first one, as failed
  * after max_cycles cycles, and as failed at once when a residual is not finite (a NaN or infinite
  * right-hand side, or a diverging solve), without disturbing the other solves. Per solve
- * the arithmetic is pb_mg's PB_MG_MIXED solver's (constant alpha, levels = every
+ * the arithmetic is pb_mg's solver's of the same precision (constant alpha, levels = every
  * halving, bottom = nu_bottom sweeps), so each result is the same alone and in any mix.
  * An edge must halve down to <= 16 (n = m * 2^k with m <= 16). */
 enum { PB_SERVE_WAITING = 0, PB_SERVE_ACTIVE = 1, PB_SERVE_DONE = 2, PB_SERVE_FAILED = 3 };
@@ -314,6 +315,7 @@ typedef struct {
     double omega;
     double tol;             /* relative max-norm residual                                          */
     int max_cycles;         /* a solve still above tol after this many cycles is retired as failed */
+    int precision;          /* PB_MG_MIXED / PB_MG_FP64                                            */
 } pb_serve_params;
 typedef struct {
     int n;                  /* edge                                                                */
@@ -344,8 +346,10 @@ int pb_serve_status(const pb_serve* sv, long long ticket, int* state, int* cycle
 int pb_serve_timing(const pb_serve* sv, double* seconds5, long long* steps);
 /* Bytes of hierarchies held (in use and cached for reuse). */
 long long pb_serve_device_bytes(const pb_serve* sv);
-/* Bytes one solve of edge n holds (-1 if n is not servable). */
+/* Bytes one solve of edge n holds in a mixed-precision engine (-1 if n is not servable). */
 long long pb_serve_request_bytes(int n);
+/* The same for an engine of the given precision (PB_MG_MIXED / PB_MG_FP64). */
+long long pb_serve_hierarchy_bytes(int n, int precision);
 
 #ifdef __cplusplus
 }

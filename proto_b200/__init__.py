@@ -46,7 +46,8 @@ class pb_mg_params(ctypes.Structure):
 
 class pb_serve_params(ctypes.Structure):
     _fields_ = [("hbm_budget", _c_ll), ("max_active", _c_int), ("nu1", _c_int), ("nu2", _c_int),
-                ("nu_bottom", _c_int), ("omega", _c_dbl), ("tol", _c_dbl), ("max_cycles", _c_int)]
+                ("nu_bottom", _c_int), ("omega", _c_dbl), ("tol", _c_dbl), ("max_cycles", _c_int),
+                ("precision", _c_int)]
 
 
 class pb_serve_request(ctypes.Structure):
@@ -79,6 +80,7 @@ def lib():
         L.pb_mg_launches_per_cycle.argtypes = [ctypes.POINTER(pb_mg_params)]
         L.pb_serve_device_bytes.restype = _c_ll
         L.pb_serve_request_bytes.restype = _c_ll
+        L.pb_serve_hierarchy_bytes.restype = _c_ll
         L.pb_halo_plan_elems.restype = _c_ll
         L.pb_halo_plan_elems.argtypes = [_vp]
         L.pb_serve_status.argtypes = [_vp, _c_ll, ctypes.POINTER(_c_int), ctypes.POINTER(_c_int),
@@ -380,16 +382,17 @@ class Serve:
     the engine keeps references until the request completes."""
 
     def __init__(self, hbm_budget, max_active=64, nu1=4, nu2=4, nu_bottom=10, omega=2.0 / 3.0, tol=1e-8,
-                 max_cycles=100):
-        self.params = pb_serve_params(int(hbm_budget), max_active, nu1, nu2, nu_bottom, omega, tol, max_cycles)
+                 max_cycles=100, precision=MG_MIXED):
+        self.params = pb_serve_params(int(hbm_budget), max_active, nu1, nu2, nu_bottom, omega, tol, max_cycles,
+                                      precision)
         h = _vp()
         _check(lib().pb_serve_create(ctypes.byref(self.params), ctypes.byref(h)), "pb_serve_create")
         self._h = h
         self._keep = {}
 
     @staticmethod
-    def request_bytes(n):
-        return lib().pb_serve_request_bytes(_c_int(n))
+    def request_bytes(n, precision=MG_MIXED):
+        return lib().pb_serve_hierarchy_bytes(_c_int(n), _c_int(precision))
 
     def submit(self, n, rhs, out, form=MG_POISSON, alpha=0.0, beta=1.0):
         import numpy as np

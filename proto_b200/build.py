@@ -28,6 +28,34 @@ def headers():
         os.path.join(os.path.dirname(HERE), "include", "proto_b200.h")]
 
 
+def local_deps(path, seen=None):
+    """The files `path` includes by a quoted #include that resolve in csrc/ or include/, recursively."""
+    import re
+    seen = set() if seen is None else seen
+    with open(path) as f:
+        names = re.findall(r'^\s*#\s*include\s+"([^"]+)"', f.read(), re.M)
+    for name in names:
+        for d in (os.path.dirname(path), os.path.join(HERE, "csrc"), os.path.join(os.path.dirname(HERE), "include")):
+            q = os.path.normpath(os.path.join(d, name))
+            if os.path.exists(q):
+                if q not in seen:
+                    seen.add(q)
+                    local_deps(q, seen)
+                break
+    return seen
+
+
+def obj_of(src):
+    return os.path.join(LIB_DIR, "obj", os.path.basename(src) + ".o")
+
+
+def stale(src, obj):
+    if not os.path.exists(obj):
+        return True
+    t = os.path.getmtime(obj)
+    return any(os.path.getmtime(f) > t for f in [src, __file__] + sorted(local_deps(src)))
+
+
 def up_to_date():
     if not os.path.exists(LIB):
         return False
@@ -35,21 +63,31 @@ def up_to_date():
     return all(os.path.getmtime(f) <= t for f in sources() + headers())
 
 
-def build(force=False, verbose=False, ptxas_info=False):
+def build(force=False, verbose=False, ptxas_info=False, jobs=None):
+    """Compiles the sources whose object is older than the source or one of its local includes (all
+    of them with force), in parallel, and links the library."""
+    from concurrent.futures import ThreadPoolExecutor
     if not force and up_to_date():
         return LIB
     os.makedirs(os.path.join(LIB_DIR, "obj"), exist_ok=True)
-    objs = []
-    for src in sources():
-        obj = os.path.join(LIB_DIR, "obj", os.path.basename(src) + ".o")
-        cmd = [NVCC] + ARCH + FLAGS + (["-Xptxas", "-v"] if ptxas_info else []) + ["-c", src, "-o", obj]
-        r = subprocess.run(cmd, capture_output=True, text=True)
+    todo = [s for s in sources() if force or ptxas_info or stale(s, obj_of(s))]
+
+    def compile_one(src):
+        cmd = [NVCC] + ARCH + FLAGS + (["-Xptxas", "-v"] if ptxas_info else []) + ["-c", src, "-o", obj_of(src)]
+        return src, subprocess.run(cmd, capture_output=True, text=True)
+
+    jobs = jobs or max(1, min(len(todo), os.cpu_count() or 1))
+    with ThreadPoolExecutor(max_workers=jobs) as ex:
+        results = list(ex.map(compile_one, todo))
+    failed = []
+    for src, r in results:
         if verbose or r.returncode != 0 or ptxas_info:
             sys.stderr.write(r.stdout + r.stderr)
         if r.returncode != 0:
-            raise RuntimeError("nvcc failed on " + src)
-        objs.append(obj)
-    cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+            failed.append(src)
+    if failed:
+        raise RuntimeError("nvcc failed on " + ", ".join(failed))
+    cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + [obj_of(s) for s in sources()] + ["-lcudart"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)

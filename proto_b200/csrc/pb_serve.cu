@@ -8,9 +8,12 @@
 // read their work lists from device memory). Converged solves are copied out and their slots and
 // memory reused.
 //
-// Per solve the arithmetic is the single-solve mixed-precision solver's (pb_mg with PB_MG_MIXED,
-// a constant alpha field, levels = the number of halvings, coarse levels of edge <= 16 fused), so
-// a result is the same alone and in any mix, and the same as that solver's.
+// Per solve the arithmetic is the single-solve solver's of the engine's precision (pb_mg with
+// PB_MG_MIXED or PB_MG_FP64, a constant alpha field, levels = the number of halvings, coarse levels
+// of edge <= 16 fused), so a result is the same alone and in any mix, and the same as that solver's.
+// The FP64 engine keeps every level in FP64: the top level is the solution itself, and each step
+// ends with the residual norm fused with the first sweep of the next cycle, as the FP64 solver's
+// norm pass; its results are those of the reference's own arithmetic.
 //
 // Reference counterpart: none (the reference runs one solve at a time, LevelMultigridSolver::solve,
 // include/utils/implem/Proto_LevelMultigridSolverImplem.H:85-123).
@@ -35,9 +38,12 @@ struct SvHier {
     int n = 0;
     int nlev = 0;                       // levels, top first
     std::vector<int> edge, sx;          // per level
-    std::vector<float*> phi0, phi1, rhs, alpha;   // alpha: coarse levels only (Helmholtz)
-    double* u64 = nullptr;              // grown, pitch sxd
-    double* f64 = nullptr;              // n^3 (also the staging buffer of the result)
+    // level buffers (FP32 levels of the mixed engine, FP64 levels of the FP64 engine); alpha: coarse
+    // levels only (Helmholtz)
+    std::vector<void*> phi0, phi1, rhs, alpha;
+    double* u64 = nullptr;              // grown, pitch sxd (FP64 engine: the top level's phi[0])
+    double* f64 = nullptr;              // n^3, also the staging buffer of the result (FP64 engine: the
+                                        // top level's rho)
     int sxd = 0;
     size_t bytes = 0;
     void* slab = nullptr;               // one allocation holds every buffer above
@@ -51,6 +57,7 @@ struct SvSolve {
     SvHier* h = nullptr;
     int depth = 0;                      // batched levels (the top one and every edge > 16)
     std::vector<float> alpha_lv;        // per level: the FP32 alpha the single-solve solver has there
+    std::vector<double> alpha_lv64;     // per level: the FP64 alpha (FP64 levels; [0] = the request's)
     int cycles = 0;
     double r0 = 0, r = 0;
     bool fresh = false;                 // admitted, first residual pass pending
@@ -62,6 +69,7 @@ using namespace pb;
 
 struct pb_serve {
     pb_serve_params p{};
+    bool fp64 = false;                  // every level in FP64 (PB_MG_FP64), else FP32 cycles
     int device = 0;
     cudaStream_t st = nullptr;
     long long next_ticket = 1;
@@ -100,10 +108,10 @@ struct pb_serve {
     SvItem* h_items = nullptr;
     long long* h_unit0 = nullptr;
     SvPhaseHeader* h_hdr = nullptr;
-    CoarseArgs<float>* d_cargs = nullptr;
+    void* d_cargs = nullptr;            // CoarseArgs<float> / CoarseArgs<double> per solve
     CoarseOffsets* d_coffs = nullptr;
     int* d_ccount = nullptr;
-    CoarseArgs<float>* h_cargs = nullptr;
+    void* h_cargs = nullptr;
     int* h_ccount = nullptr;
     CoarseOffsets* h_coffs = nullptr;
     double* d_norms = nullptr;          // per slot: residual norm of the step
@@ -146,11 +154,15 @@ void hier_free(SvHier* h, cudaStream_t st)
 }
 
 // Walks the buffers of an n-edge hierarchy in slab order (256-byte aligned offsets): per level the
-// two grown FP32 solutions, rho and (edge <= 16) alpha, then the grown FP64 solution and the FP64
-// right-hand side. place(level, kind, offset, bytes) sees each; the return value is the slab size.
+// two grown solutions, rho and (edge <= 16) alpha, in the level type; then, for FP32 levels, the
+// grown FP64 solution and the FP64 right-hand side. place(level, kind, offset, bytes) sees each;
+// the return value is the slab size.
+int level_pitch(int e, bool fp64) { return fp64 ? grown_pitch<double>(e) : grown_pitch<float>(e); }
+
 template <class F>
-size_t hier_layout(int n, F&& place)
+size_t hier_layout(int n, bool fp64, F&& place)
 {
+    const size_t es = fp64 ? sizeof(double) : sizeof(float);
     size_t off = 0;
     auto put = [&](int l, int kind, size_t b) {
         place(l, kind, off, b);
@@ -158,31 +170,33 @@ size_t hier_layout(int n, F&& place)
     };
     int l = 0;
     for (int e = n;; e /= 2, l++) {
-        const size_t g = sizeof(float) * (size_t)grown_pitch<float>(e) * (e + 2) * (e + 2);
-        const size_t c = sizeof(float) * (size_t)e * e * e;
+        const size_t g = es * (size_t)level_pitch(e, fp64) * (e + 2) * (e + 2);
+        const size_t c = es * (size_t)e * e * e;
         put(l, 0, g);
         put(l, 1, g);
         put(l, 2, c);
         if (e <= kCoarseEdge) put(l, 3, c);
         if (e % 2 != 0 || e == 1) break;
     }
-    put(-1, 4, sizeof(double) * (size_t)grown_pitch<double>(n) * (n + 2) * (n + 2));
-    put(-1, 5, sizeof(double) * (size_t)n * n * n);
+    if (!fp64) {
+        put(-1, 4, sizeof(double) * (size_t)grown_pitch<double>(n) * (n + 2) * (n + 2));
+        put(-1, 5, sizeof(double) * (size_t)n * n * n);
+    }
     return off;
 }
 
-size_t hier_bytes(int n)
+size_t hier_bytes(int n, bool fp64)
 {
-    return hier_layout(n, [](int, int, size_t, size_t) {});
+    return hier_layout(n, fp64, [](int, int, size_t, size_t) {});
 }
 
-// One allocation per hierarchy, ordered on stream st; the FP32 solutions start at zero (their ghost
+// One allocation per hierarchy, ordered on stream st; the level solutions start at zero (their ghost
 // images included), set on st as well.
-SvHier* hier_alloc(int n, cudaMemPool_t pool, cudaStream_t st)
+SvHier* hier_alloc(int n, bool fp64, cudaMemPool_t pool, cudaStream_t st)
 {
     SvHier* h = new SvHier;
     h->n = n;
-    const size_t total = hier_bytes(n);
+    const size_t total = hier_bytes(n, fp64);
     if (cudaMallocFromPoolAsync(&h->slab, total, pool, st) != cudaSuccess) {
         cudaGetLastError();
         delete h;
@@ -190,11 +204,11 @@ SvHier* hier_alloc(int n, cudaMemPool_t pool, cudaStream_t st)
     }
     unsigned char* base = static_cast<unsigned char*>(h->slab);
     bool ok = true;
-    hier_layout(n, [&](int l, int kind, size_t off, size_t b) {
+    hier_layout(n, fp64, [&](int l, int kind, size_t off, size_t b) {
         if (l >= (int)h->edge.size()) {
             const int e = n >> l;
             h->edge.push_back(e);
-            h->sx.push_back(grown_pitch<float>(e));
+            h->sx.push_back(level_pitch(e, fp64));
             h->phi0.push_back(nullptr);
             h->phi1.push_back(nullptr);
             h->rhs.push_back(nullptr);
@@ -202,10 +216,10 @@ SvHier* hier_alloc(int n, cudaMemPool_t pool, cudaStream_t st)
         }
         void* q = base + off;
         switch (kind) {
-        case 0: h->phi0[l] = static_cast<float*>(q); break;
-        case 1: h->phi1[l] = static_cast<float*>(q); break;
-        case 2: h->rhs[l] = static_cast<float*>(q); break;
-        case 3: h->alpha[l] = static_cast<float*>(q); break;
+        case 0: h->phi0[l] = q; break;
+        case 1: h->phi1[l] = q; break;
+        case 2: h->rhs[l] = q; break;
+        case 3: h->alpha[l] = q; break;
         case 4: h->u64 = static_cast<double*>(q); break;
         default: h->f64 = static_cast<double*>(q); break;
         }
@@ -213,6 +227,10 @@ SvHier* hier_alloc(int n, cudaMemPool_t pool, cudaStream_t st)
     });
     h->nlev = (int)h->edge.size();
     h->sxd = grown_pitch<double>(n);
+    if (fp64) {   // the top level is the FP64 solution and its right-hand side
+        h->u64 = static_cast<double*>(h->phi0[0]);
+        h->f64 = static_cast<double*>(h->rhs[0]);
+    }
     h->bytes = total;
     if (!ok) {
         cudaGetLastError();
@@ -245,30 +263,32 @@ int batched_depth(const SvHier* h)
 // Per-level FP32 alpha of a constant field: the top level holds float(alpha), each coarser level the
 // 2^3 average of the one above (eight products 0.125*a summed in order, each rounded to FP32, as
 // the averaging kernel does; for a non-dyadic a the sum is not exactly a).
-std::vector<float> level_alphas(double alpha, int nlev)
+template <typename T>
+std::vector<T> level_alphas(double alpha, int nlev)
 {
-    std::vector<float> v(nlev);
-    v[0] = (float)alpha;
+    std::vector<T> v(nlev);
+    v[0] = (T)alpha;
     for (int l = 1; l < nlev; l++) {
-        float acc = 0.f;
-        for (int k = 0; k < 8; k++) acc = acc + 0.125f * v[l - 1];
+        T acc = T(0);
+        for (int k = 0; k < 8; k++) acc = acc + T(0.125) * v[l - 1];
         v[l] = acc;
     }
     return v;
 }
 
 // Smoother scalars of the level at depth d of an n-edge hierarchy (the single-solve solver's).
-RelaxCoef<float> level_coef(const pb_serve_params& p, const pb_serve_request& q, int n, int e, int sx, int d)
+template <typename T>
+RelaxCoef<T> level_coef(const pb_serve_params& p, const pb_serve_request& q, int n, int e, int sx, int d)
 {
     const double h = (double)(1 << d) / (double)n, hsqinv = 1. / (h * h);
-    RelaxCoef<float> k;
+    RelaxCoef<T> k;
     k.n = e;
     k.sx = sx;
     k.helm = q.form == PB_MG_HELMHOLTZ;
-    k.neg_lambda = (float)(-mg_lambda(p.omega, h));
-    k.beta = (float)q.beta;
-    k.omega = (float)p.omega;
-    k.diagB = (float)(6.0 * q.beta * hsqinv);
+    k.neg_lambda = (T)(-mg_lambda(p.omega, h));
+    k.beta = (T)q.beta;
+    k.omega = (T)p.omega;
+    k.diagB = (T)(6.0 * q.beta * hsqinv);
     return k;
 }
 
@@ -293,6 +313,8 @@ double level_hsqinv(int n, int d)
 //   coarse          : the fused coarse cycle of every solve (one CTA each)
 //   up d = D-1..0   : prolongation from d+1, sweeps (depth 0: nu2-1 then the fused update)
 //   K1              : FP64 residual, norm, FP32 right-hand side and first sweep of the next step
+// The FP64 engine's depth 0 is the solution itself: nu2 sweeps on the way up, and NORM (the residual
+// norm with the first sweep of the next step) in K1's place.
 // Phase slots are laid out in that order; the graph for depth D launches exactly these slots.
 namespace {
 
@@ -303,6 +325,7 @@ struct PhaseSlot {
 
 std::vector<PhaseSlot> phase_plan(const pb_serve_params& p, int D)
 {
+    const bool fp64 = p.precision == PB_MG_FP64;
     std::vector<PhaseSlot> v;
     for (int d = 0; d < D; d++) {
         if (d == 0) {
@@ -316,11 +339,11 @@ std::vector<PhaseSlot> phase_plan(const pb_serve_params& p, int D)
     v.push_back({-1, -1});   // coarse
     for (int d = D - 1; d >= 0; d--) {
         v.push_back({SV_PROLONG, d});
-        const int sweeps = d == 0 ? p.nu2 - 1 : p.nu2;
+        const int sweeps = d == 0 && !fp64 ? p.nu2 - 1 : p.nu2;
         for (int s = 0; s < sweeps; s++) v.push_back({SV_RELAX, d});
-        if (d == 0) v.push_back({SV_UPDATE, 0});
+        if (d == 0 && !fp64) v.push_back({SV_UPDATE, 0});
     }
-    v.push_back({SV_K1, 0});
+    v.push_back({fp64 ? SV_NORM : SV_K1, 0});
     return v;
 }
 
@@ -356,13 +379,106 @@ long long layout_items(std::vector<SvItem>& items, bool staged, long long ctas)
     return total;
 }
 
-bool is_staged(int op) { return op == SV_RELAX || op == SV_UPDATE || op == SV_K1; }
+bool is_staged(int op) { return op == SV_RELAX || op == SV_UPDATE || op == SV_K1 || op == SV_NORM; }
+
+// The fields of an item at depth d of solve s that every phase shares: geometry and smoother scalars
+// (FP32 always: the geometry of the work layout; FP64 for FP64 levels), alpha and beta, the slot and
+// the FP64 top-level buffers.
+SvItem item_base(const pb_serve_params& p, bool fp64, const SvSolve& s, int d)
+{
+    const SvHier& h = *s.h;
+    SvItem it{};
+    it.k = level_coef<float>(p, s.req, h.n, h.edge[d], h.sx[d], d);
+    if (fp64) it.k64 = level_coef<double>(p, s.req, h.n, h.edge[d], h.sx[d], d);
+    it.alpha = s.alpha_lv[d];
+    it.beta = (float)s.req.beta;
+    it.alpha64 = s.alpha_lv64[d];
+    it.beta64 = s.req.beta;
+    it.slot = s.slot;
+    it.sxd = h.sxd;
+    it.u64 = h.u64;
+    it.f64 = h.f64;
+    return it;
+}
+
+// the 7-point coefficients scaled by sc, in the item's level type(s)
+void item_coefs(SvItem& it, bool fp64, double sc)
+{
+    it.c = lap7_coefs<float>(sc);
+    if (fp64) it.c64 = lap7_coefs<double>(sc);
+}
+
+// the FP64 engine's norm pass over the top level: state in phi[0], first sweep into phi[1]
+SvItem norm_item(const pb_serve_params& p, const SvSolve& s)
+{
+    const SvHier& h = *s.h;
+    const bool helm = s.req.form == PB_MG_HELMHOLTZ;
+    SvItem it = item_base(p, true, s, 0);
+    it.in = h.phi0[0];
+    it.out = h.phi1[0];
+    it.rhs = h.rhs[0];
+    const double hs = level_hsqinv(h.n, 0);
+    item_coefs(it, true, helm ? hs : p.omega / 6.0);
+    it.nscale = hs;
+    return it;
+}
 
 } // namespace
+
+template <typename T>
+static int fill_coarse_args(pb_serve* sv, const std::vector<SvSolve*>& act)
+{
+    const pb_serve_params& p = sv->p;
+    const int cap = (int)p.max_active;
+    CoarseArgs<T>* hc = static_cast<CoarseArgs<T>*>(sv->h_cargs);
+    memset(hc, 0, sizeof(CoarseArgs<T>) * cap);
+    memset(sv->h_coffs, 0, sizeof(CoarseOffsets) * cap);
+    int nc = 0;
+    for (size_t a = 0; a < act.size(); a++) {
+        SvSolve& s = *act[a];
+        SvHier& h = *s.h;
+        CoarseArgs<T> ca;
+        memset(&ca, 0, sizeof(ca));
+        const int d0 = s.depth, top = h.nlev - 1 - d0;   // coarse levels: index 0 = coarsest
+        const bool helm = s.req.form == PB_MG_HELMHOLTZ;
+        for (int l = 0; l <= top; l++) {
+            const int d = h.nlev - 1 - l;
+            CoarseLevel<T>& c = ca.lv[l];
+            c.phi[0] = static_cast<T*>(h.phi0[d]);
+            c.phi[1] = static_cast<T*>(h.phi1[d]);
+            c.rhs = static_cast<T*>(h.rhs[d]);
+            c.alpha = static_cast<const T*>(h.alpha[d]);
+            c.k = level_coef<T>(p, s.req, h.n, h.edge[d], h.sx[d], d);
+            const double hs = level_hsqinv(h.n, d);
+            c.crelax = lap7_coefs<T>(helm ? hs : p.omega / 6.0);
+            c.cres = lap7_coefs<T>(helm ? hs : -hs);
+        }
+        ca.top = top;
+        ca.nu1 = p.nu1;
+        ca.nu2 = p.nu2;
+        ca.nu_bottom = p.nu_bottom;
+        ca.direct = 0;
+        ca.ainv = nullptr;
+        ca.beta = (T)s.req.beta;
+        CoarseOffsets off;
+        memset(&off, 0, sizeof(off));
+        const size_t smem = coarse_smem_layout(ca, helm, off.o);
+        ca.in_smem = smem <= sv->coarse_smem ? 1 : 0;
+        hc[nc] = ca;
+        sv->h_coffs[nc] = off;
+        nc++;
+    }
+    PB_CUDA(cudaMemcpyAsync(sv->d_cargs, sv->h_cargs, sizeof(CoarseArgs<T>) * nc, cudaMemcpyHostToDevice, sv->st));
+    PB_CUDA(cudaMemcpyAsync(sv->d_coffs, sv->h_coffs, sizeof(CoarseOffsets) * nc, cudaMemcpyHostToDevice, sv->st));
+    *sv->h_ccount = nc;
+    PB_CUDA(cudaMemcpyAsync(sv->d_ccount, sv->h_ccount, sizeof(int), cudaMemcpyHostToDevice, sv->st));
+    return PB_OK;
+}
 
 static int build_lists(pb_serve* sv)
 {
     const pb_serve_params& p = sv->p;
+    const bool fp64 = sv->fp64;
     int D = 0;
     std::vector<SvSolve*> act;
     for (long long t : sv->slots)
@@ -390,19 +506,10 @@ static int build_lists(pb_serve* sv)
             SvHier& h = *s.h;
             const int d = ps.depth;
             if (d >= s.depth) continue;
-            const int n = h.n, e = h.edge[d], sxl = h.sx[d];
-            SvItem it{};
-            it.k = level_coef(p, s.req, n, e, sxl, d);
+            const int n = h.n, e = h.edge[d];
+            SvItem it = item_base(p, fp64, s, d);
             const bool helm = s.req.form == PB_MG_HELMHOLTZ;
-            it.alpha = s.alpha_lv[d];
-            it.beta = (float)s.req.beta;
-            it.alpha64 = s.req.alpha;
-            it.beta64 = s.req.beta;
-            it.slot = s.slot;
-            it.sxd = h.sxd;
-            it.u64 = h.u64;
-            it.f64 = h.f64;
-            float* ph_[2] = {h.phi0[d], h.phi1[d]};
+            void* ph_[2] = {h.phi0[d], h.phi1[d]};
             int& c = cur[a][d];
             switch (ps.op) {
             case SV_RELAX:
@@ -410,7 +517,7 @@ static int build_lists(pb_serve* sv)
                 it.in = ph_[c];
                 it.out = ph_[1 - c];
                 it.rhs = h.rhs[d];
-                it.c = lap7_coefs<float>(helm ? level_hsqinv(n, d) : p.omega / 6.0);
+                item_coefs(it, fp64, helm ? level_hsqinv(n, d) : p.omega / 6.0);
                 if (ps.op == SV_RELAX) c = 1 - c;
                 break;
             case SV_RELAX_FIRST:
@@ -425,7 +532,7 @@ static int build_lists(pb_serve* sv)
                 it.out = h.rhs[d + 1];
                 it.rhs = h.rhs[d];
                 const double hs = level_hsqinv(n, d);
-                it.c = lap7_coefs<float>(helm ? hs : -hs);
+                item_coefs(it, fp64, helm ? hs : -hs);
                 it.units = (e / 2) * (e / 2);
                 break;
             }
@@ -447,6 +554,11 @@ static int build_lists(pb_serve* sv)
                 c = 1;
                 break;
             }
+            case SV_NORM:
+                // the cycle's sweeps come back to phi[0] (nu1 + nu2 is even)
+                it = norm_item(p, s);
+                c = 1;
+                break;
             }
             items.push_back(it);
         }
@@ -462,18 +574,13 @@ static int build_lists(pb_serve* sv)
         for (size_t a = 0; a < act.size(); a++) {
             SvSolve& s = *act[a];
             if (!s.fresh) continue;
+            if (fp64) {
+                items.push_back(norm_item(p, s));
+                continue;
+            }
             SvHier& h = *s.h;
             const bool helm = s.req.form == PB_MG_HELMHOLTZ;
-            SvItem it{};
-            it.k = level_coef(p, s.req, h.n, h.n, h.sx[0], 0);
-            it.alpha = s.alpha_lv[0];
-            it.beta = (float)s.req.beta;
-            it.alpha64 = s.req.alpha;
-            it.beta64 = s.req.beta;
-            it.slot = s.slot;
-            it.sxd = h.sxd;
-            it.u64 = h.u64;
-            it.f64 = h.f64;
+            SvItem it = item_base(p, false, s, 0);
             it.in = h.phi1[0];
             it.out = h.rhs[0];
             const double hs = level_hsqinv(h.n, 0);
@@ -485,47 +592,6 @@ static int build_lists(pb_serve* sv)
         for (size_t k = 0; k < items.size(); k++) sv->h_unit0[(size_t)ph * cap + k] = items[k].unit0;
         sv->h_hdr[ph] = SvPhaseHeader{(long long)items.size(), total};
     }
-    // coarse-cycle arguments (entry level = depth s.depth)
-    memset(sv->h_cargs, 0, sizeof(CoarseArgs<float>) * cap);
-    memset(sv->h_coffs, 0, sizeof(CoarseOffsets) * cap);
-    int nc = 0;
-    size_t smem_max = 0;
-    for (size_t a = 0; a < act.size(); a++) {
-        SvSolve& s = *act[a];
-        SvHier& h = *s.h;
-        CoarseArgs<float> ca;
-        memset(&ca, 0, sizeof(ca));
-        const int d0 = s.depth, top = h.nlev - 1 - d0;   // coarse levels: index 0 = coarsest
-        const bool helm = s.req.form == PB_MG_HELMHOLTZ;
-        for (int l = 0; l <= top; l++) {
-            const int d = h.nlev - 1 - l;
-            CoarseLevel<float>& c = ca.lv[l];
-            c.phi[0] = h.phi0[d];
-            c.phi[1] = h.phi1[d];
-            c.rhs = h.rhs[d];
-            c.alpha = h.alpha[d];
-            c.k = level_coef(p, s.req, h.n, h.edge[d], h.sx[d], d);
-            const double hs = level_hsqinv(h.n, d);
-            c.crelax = lap7_coefs<float>(helm ? hs : p.omega / 6.0);
-            c.cres = lap7_coefs<float>(helm ? hs : -hs);
-        }
-        ca.top = top;
-        ca.nu1 = p.nu1;
-        ca.nu2 = p.nu2;
-        ca.nu_bottom = p.nu_bottom;
-        ca.direct = 0;
-        ca.ainv = nullptr;
-        ca.beta = (float)s.req.beta;
-        CoarseOffsets off;
-        memset(&off, 0, sizeof(off));
-        const size_t smem = coarse_smem_layout(ca, helm, off.o);
-        ca.in_smem = smem <= sv->coarse_smem ? 1 : 0;
-        smem_max = std::max(smem_max, smem);
-        sv->h_cargs[nc] = ca;
-        sv->h_coffs[nc] = off;
-        nc++;
-    }
-    (void)smem_max;
     // the phases of this depth's plan and the residual-pass slot (the last one)
     const size_t used = plan.size() * cap;
     PB_CUDA(cudaMemcpyAsync(sv->d_items, sv->h_items, sizeof(SvItem) * used, cudaMemcpyHostToDevice, sv->st));
@@ -534,10 +600,9 @@ static int build_lists(pb_serve* sv)
     PB_CUDA(cudaMemcpyAsync(sv->d_items + last, sv->h_items + last, sizeof(SvItem) * cap, cudaMemcpyHostToDevice, sv->st));
     PB_CUDA(cudaMemcpyAsync(sv->d_unit0 + last, sv->h_unit0 + last, sizeof(long long) * cap, cudaMemcpyHostToDevice, sv->st));
     PB_CUDA(cudaMemcpyAsync(sv->d_hdr, sv->h_hdr, sizeof(SvPhaseHeader) * sv->max_phases, cudaMemcpyHostToDevice, sv->st));
-    PB_CUDA(cudaMemcpyAsync(sv->d_cargs, sv->h_cargs, sizeof(CoarseArgs<float>) * nc, cudaMemcpyHostToDevice, sv->st));
-    PB_CUDA(cudaMemcpyAsync(sv->d_coffs, sv->h_coffs, sizeof(CoarseOffsets) * nc, cudaMemcpyHostToDevice, sv->st));
-    *sv->h_ccount = nc;
-    PB_CUDA(cudaMemcpyAsync(sv->d_ccount, sv->h_ccount, sizeof(int), cudaMemcpyHostToDevice, sv->st));
+    // coarse-cycle arguments (entry level = depth s.depth)
+    const int e = fp64 ? fill_coarse_args<double>(sv, act) : fill_coarse_args<float>(sv, act);
+    if (e != PB_OK) return e;
     sv->lists_dirty = false;
     return PB_OK;
 }
@@ -547,14 +612,26 @@ static int launch_phase(pb_serve* sv, int slot, int op, double* norms, cudaStrea
     const SvItem* items = sv->d_items + (size_t)slot * sv->p.max_active;
     const long long* u0 = sv->d_unit0 + (size_t)slot * sv->p.max_active;
     const SvPhaseHeader* hdr = sv->d_hdr + slot;
-    switch (op) {
-    case SV_RELAX: k_sv_ring<SV_RELAX, float><<<sv->ring_grid, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
-    case SV_RELAX_FIRST: k_sv_phase<SV_RELAX_FIRST><<<sv->grid, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
-    case SV_RESTRICT: k_sv_phase<SV_RESTRICT><<<sv->grid, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
-    case SV_PROLONG: k_sv_phase<SV_PROLONG><<<sv->grid, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
-    case SV_K1: k_sv_ring<SV_K1, double><<<sv->ring_grid, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
-    case SV_UPDATE: k_sv_ring<SV_UPDATE, float><<<sv->ring_grid, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
-    default: return PB_ERR_ARG;
+    const int rg = sv->ring_grid, g = sv->grid;
+    if (sv->fp64) {
+        switch (op) {
+        case SV_RELAX: k_sv_ring<SV_RELAX, double><<<rg, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
+        case SV_RELAX_FIRST: k_sv_phase<SV_RELAX_FIRST, double><<<g, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
+        case SV_RESTRICT: k_sv_phase<SV_RESTRICT, double><<<g, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
+        case SV_PROLONG: k_sv_phase<SV_PROLONG, double><<<g, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
+        case SV_NORM: k_sv_ring<SV_NORM, double><<<rg, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
+        default: return PB_ERR_ARG;
+        }
+    } else {
+        switch (op) {
+        case SV_RELAX: k_sv_ring<SV_RELAX, float><<<rg, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
+        case SV_RELAX_FIRST: k_sv_phase<SV_RELAX_FIRST, float><<<g, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
+        case SV_RESTRICT: k_sv_phase<SV_RESTRICT, float><<<g, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
+        case SV_PROLONG: k_sv_phase<SV_PROLONG, float><<<g, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
+        case SV_K1: k_sv_ring<SV_K1, double><<<rg, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
+        case SV_UPDATE: k_sv_ring<SV_UPDATE, float><<<rg, kSvUnit, 0, st>>>(items, u0, hdr, norms); break;
+        default: return PB_ERR_ARG;
+        }
     }
     PB_LAUNCH_CHECK();
     return PB_OK;
@@ -568,12 +645,16 @@ static int enqueue_step(pb_serve* sv, int D, cudaStream_t st)
     for (size_t ph = 0; ph < plan.size(); ph++) {
         const PhaseSlot& ps = plan[ph];
         if (ps.op < 0) {
-            k_coarse_cycle_batch<float><<<sv->p.max_active, kCoarseThreads, sv->coarse_smem, st>>>(sv->d_cargs, sv->d_coffs,
-                                                                                                   sv->d_ccount);
+            if (sv->fp64)
+                k_coarse_cycle_batch<double><<<sv->p.max_active, kCoarseThreads, sv->coarse_smem, st>>>(
+                    static_cast<const CoarseArgs<double>*>(sv->d_cargs), sv->d_coffs, sv->d_ccount);
+            else
+                k_coarse_cycle_batch<float><<<sv->p.max_active, kCoarseThreads, sv->coarse_smem, st>>>(
+                    static_cast<const CoarseArgs<float>*>(sv->d_cargs), sv->d_coffs, sv->d_ccount);
             PB_LAUNCH_CHECK();
             continue;
         }
-        if (ps.op == SV_K1) PB_CUDA(cudaMemsetAsync(sv->d_norms, 0, sizeof(double) * sv->p.max_active, st));
+        if (ps.op == SV_K1 || ps.op == SV_NORM) PB_CUDA(cudaMemsetAsync(sv->d_norms, 0, sizeof(double) * sv->p.max_active, st));
         if ((e = launch_phase(sv, (int)ph, ps.op, sv->d_norms, st)) != PB_OK) return e;
     }
     PB_CUDA(cudaMemcpyAsync(sv->h_norms, sv->d_norms, sizeof(double) * sv->p.max_active, cudaMemcpyDeviceToHost, st));
@@ -610,7 +691,7 @@ static int admit(pb_serve* sv)
             h = it->second;
             sv->cache.erase(it);
         } else {
-            const size_t need = hier_bytes(n);
+            const size_t need = hier_bytes(n, sv->fp64);
             // make room by dropping idle hierarchies of other edges
             while (sv->held + need > (size_t)sv->p.hbm_budget && !sv->cache.empty()) {
                 auto v = sv->cache.begin();
@@ -619,7 +700,7 @@ static int admit(pb_serve* sv)
                 sv->cache.erase(v);
             }
             if (sv->held + need > (size_t)sv->p.hbm_budget) return PB_OK;   // wait for memory
-            h = hier_alloc(n, sv->pool, sv->ust);
+            h = hier_alloc(n, sv->fp64, sv->pool, sv->ust);
             if (!h) return PB_OK;
             sv->held += h->bytes;
         }
@@ -632,7 +713,8 @@ static int admit(pb_serve* sv)
         s.h = h;
         s.state = PB_SERVE_ACTIVE;
         s.depth = batched_depth(h);
-        s.alpha_lv = level_alphas(s.req.alpha, h->nlev);
+        s.alpha_lv = level_alphas<float>(s.req.alpha, h->nlev);
+        s.alpha_lv64 = level_alphas<double>(s.req.alpha, h->nlev);
         // initial guess zero, right-hand side in; constant alpha on the coarse levels
         const size_t n3 = (size_t)n * n * n;
         PB_CUDA(cudaMemsetAsync(h->u64, 0, sizeof(double) * (size_t)h->sxd * (n + 2) * (n + 2), sv->ust));
@@ -641,7 +723,12 @@ static int admit(pb_serve* sv)
             for (int d = 0; d < h->nlev; d++)
                 if (h->alpha[d]) {
                     const long long c = (long long)h->edge[d] * h->edge[d] * h->edge[d];
-                    k_sv_fill<<<grid_for(c, 256), 256, 0, sv->ust>>>(h->alpha[d], c, s.alpha_lv[d]);
+                    if (sv->fp64)
+                        k_sv_fill<double><<<grid_for(c, 256), 256, 0, sv->ust>>>(static_cast<double*>(h->alpha[d]), c,
+                                                                                 s.alpha_lv64[d]);
+                    else
+                        k_sv_fill<float><<<grid_for(c, 256), 256, 0, sv->ust>>>(static_cast<float*>(h->alpha[d]), c,
+                                                                               s.alpha_lv[d]);
                     PB_LAUNCH_CHECK();
                 }
         PB_CUDA(cudaEventRecord(landed, sv->ust));
@@ -740,9 +827,13 @@ int pb_serve_create(const pb_serve_params* p, pb_serve** out)
     if (p->max_active < 1 || p->max_active > kSvMaxSolves || p->nu1 < 1 || p->nu2 < 1 || p->nu_bottom < 0 ||
         p->hbm_budget <= 0 || !(p->tol > 0) || p->max_cycles < 1)
         return PB_ERR_ARG;
+    if (p->precision != PB_MG_MIXED && p->precision != PB_MG_FP64) return PB_ERR_ARG;
+    // FP64: each cycle's sweeps of the top level return to the buffer the norm pass reads
+    if (p->precision == PB_MG_FP64 && (p->nu1 + p->nu2) % 2 != 0) return PB_ERR_ARG;
     pb_serve* sv = new (std::nothrow) pb_serve;
     if (!sv) return PB_ERR_NOMEM;
     sv->p = *p;
+    sv->fp64 = p->precision == PB_MG_FP64;
     cudaGetDevice(&sv->device);
     sv->slots.assign(p->max_active, 0);
     sv->max_phases = phases_for(*p);
@@ -754,13 +845,13 @@ int pb_serve_create(const pb_serve_params* p, pb_serve** out)
               cudaMallocHost(&sv->h_items, sizeof(SvItem) * cap * sv->max_phases) == cudaSuccess &&
               cudaMallocHost(&sv->h_unit0, sizeof(long long) * cap * sv->max_phases) == cudaSuccess &&
               cudaMallocHost(&sv->h_hdr, sizeof(SvPhaseHeader) * sv->max_phases) == cudaSuccess &&
-              cudaMallocHost(&sv->h_cargs, sizeof(CoarseArgs<float>) * cap) == cudaSuccess &&
+              cudaMallocHost(&sv->h_cargs, sizeof(CoarseArgs<double>) * cap) == cudaSuccess &&
               cudaMallocHost(&sv->h_coffs, sizeof(CoarseOffsets) * cap) == cudaSuccess &&
               cudaMallocHost(&sv->h_ccount, sizeof(int)) == cudaSuccess &&
               cudaMalloc(&sv->d_items, sizeof(SvItem) * cap * sv->max_phases) == cudaSuccess &&
               cudaMalloc(&sv->d_unit0, sizeof(long long) * cap * sv->max_phases) == cudaSuccess &&
               cudaMalloc(&sv->d_hdr, sizeof(SvPhaseHeader) * sv->max_phases) == cudaSuccess &&
-              cudaMalloc(&sv->d_cargs, sizeof(CoarseArgs<float>) * cap) == cudaSuccess &&
+              cudaMalloc(&sv->d_cargs, sizeof(CoarseArgs<double>) * cap) == cudaSuccess &&
               cudaMalloc(&sv->d_coffs, sizeof(CoarseOffsets) * cap) == cudaSuccess &&
               cudaMalloc(&sv->d_ccount, sizeof(int)) == cudaSuccess &&
               cudaMalloc(&sv->d_norms, sizeof(double) * cap) == cudaSuccess &&
@@ -772,23 +863,39 @@ int pb_serve_create(const pb_serve_params* p, pb_serve** out)
         // the staged kernels take whole units per CTA: a grid of exactly the resident CTAs spreads
         // the units evenly (a larger one would run in partial waves)
         int o1 = 0, o2 = 0, o3 = 0;
-        ok = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o1, k_sv_ring<SV_RELAX, float>, kSvUnit, 0) == cudaSuccess &&
-             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o2, k_sv_ring<SV_K1, double>, kSvUnit, 0) == cudaSuccess &&
-             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o3, k_sv_ring<SV_UPDATE, float>, kSvUnit, 0) == cudaSuccess;
+        if (sv->fp64) {
+            ok = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o1, k_sv_ring<SV_RELAX, double>, kSvUnit, 0) == cudaSuccess &&
+                 cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o2, k_sv_ring<SV_NORM, double>, kSvUnit, 0) == cudaSuccess;
+            o3 = o1;
+        } else {
+            ok = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o1, k_sv_ring<SV_RELAX, float>, kSvUnit, 0) == cudaSuccess &&
+                 cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o2, k_sv_ring<SV_K1, double>, kSvUnit, 0) == cudaSuccess &&
+                 cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o3, k_sv_ring<SV_UPDATE, float>, kSvUnit, 0) == cudaSuccess;
+        }
         sv->ring_grid = cached_sm_count() * std::max(1, std::min(o1, std::min(o2, o3)));
-        // coarse part: the largest arena (edge 16, Helmholtz) fits in shared memory
-        CoarseArgs<float> ca;
-        memset(&ca, 0, sizeof(ca));
+        // coarse part: the largest arena (edge 16, Helmholtz) in shared memory where it fits (FP32
+        // levels); otherwise the solves whose arena fits use shared memory and the rest global memory
         int l = 0;
         for (int e = kCoarseEdge; e >= 1; e /= 2, l++) {}
-        ca.top = l - 1;
-        for (int i = 0, e = 1; i < l; i++, e *= 2) {
-            ca.lv[i].k.n = e;
-            ca.lv[i].k.sx = grown_pitch<float>(e);
-        }
-        sv->coarse_smem = coarse_smem_layout(ca, 1, nullptr);
-        ok = ok && cudaFuncSetAttribute(k_coarse_cycle_batch<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)sv->coarse_smem) == cudaSuccess;
+        auto arena = [&](auto zero) {
+            using T = decltype(zero);
+            CoarseArgs<T> ca;
+            memset(&ca, 0, sizeof(ca));
+            ca.top = l - 1;
+            for (int i = 0, e = 1; i < l; i++, e *= 2) {
+                ca.lv[i].k.n = e;
+                ca.lv[i].k.sx = grown_pitch<T>(e);
+            }
+            return coarse_smem_layout(ca, 1, nullptr);
+        };
+        // the descriptor table takes a little static shared memory beside the arena
+        sv->coarse_smem = std::min(sv->fp64 ? arena(0.0) : arena(0.f), (size_t)216 * 1024);
+        if (sv->fp64)
+            ok = ok && cudaFuncSetAttribute(k_coarse_cycle_batch<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)sv->coarse_smem) == cudaSuccess;
+        else
+            ok = ok && cudaFuncSetAttribute(k_coarse_cycle_batch<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)sv->coarse_smem) == cudaSuccess;
     }
     if (!ok) {
         cudaGetLastError();
@@ -844,7 +951,7 @@ int pb_serve_submit(pb_serve* sv, const pb_serve_request* q, long long* ticket)
 {
     if (!sv || !q || !q->rhs || !q->out) return PB_ERR_ARG;
     if (!edge_ok(q->n) || (q->form != PB_MG_POISSON && q->form != PB_MG_HELMHOLTZ)) return PB_ERR_ARG;
-    if (hier_bytes(q->n) > (size_t)sv->p.hbm_budget) return PB_ERR_BUDGET;
+    if (hier_bytes(q->n, sv->fp64) > (size_t)sv->p.hbm_budget) return PB_ERR_BUDGET;
     SvSolve s;
     s.ticket = sv->next_ticket++;
     s.req = *q;
@@ -886,7 +993,7 @@ int pb_serve_step(pb_serve* sv, int* active, int* waiting)
             if (t && sv->solves[t].fresh) fresh = true;
         if (fresh) {
             PB_CUDA(cudaMemsetAsync(sv->d_r0, 0, sizeof(double) * sv->p.max_active, sv->st));
-            if ((e = launch_phase(sv, sv->max_phases - 1, SV_K1, sv->d_r0, sv->st)) != PB_OK) return e;
+            if ((e = launch_phase(sv, sv->max_phases - 1, sv->fp64 ? SV_NORM : SV_K1, sv->d_r0, sv->st)) != PB_OK) return e;
             PB_CUDA(cudaMemcpyAsync(sv->h_r0, sv->d_r0, sizeof(double) * sv->p.max_active, cudaMemcpyDeviceToHost, sv->st));
         }
         sv->t_stage[2] += lap(t0);
@@ -981,7 +1088,13 @@ long long pb_serve_device_bytes(const pb_serve* sv)
 
 long long pb_serve_request_bytes(int n)
 {
-    return edge_ok(n) ? (long long)hier_bytes(n) : -1;
+    return edge_ok(n) ? (long long)hier_bytes(n, false) : -1;
+}
+
+long long pb_serve_hierarchy_bytes(int n, int precision)
+{
+    if (precision != PB_MG_MIXED && precision != PB_MG_FP64) return -1;
+    return edge_ok(n) ? (long long)hier_bytes(n, precision == PB_MG_FP64) : -1;
 }
 
 } // extern "C"

@@ -12,7 +12,10 @@
 // kSvRows so a chunk lies in one item. Either way a block finds its item with one binary search
 // over the phase's compact array of first units.
 // The per-cell arithmetic is the single-solve solver's (same helpers, same order), so a solve's
-// result does not depend on what else is in the batch.
+// result does not depend on what else is in the batch. The levels are FP32 in the mixed-precision
+// engine (its FP64 residual pass and update work on the FP64 solution beside them) and FP64 in the
+// FP64 engine, whose cycle is the FP64 solver's (the solution is the top level itself, and the
+// residual norm rides on the first sweep of the next cycle).
 #pragma once
 #include <cfloat>
 #include <math_constants.h>
@@ -26,18 +29,22 @@ constexpr int kSvRows = kSvUnit / 32;   // rows per chunk (one warp each)
 constexpr int kSvMaxSolves = 256;  // solves in flight at most
 
 struct SvItem {
-    float* in;             // relax: source phi; restrict: fine phi; prolong: fine phi (updated in place);
-                           // K1: the level's phi[1] (receives the first sweep)
-    float* out;            // relax: destination phi; restrict: coarse rho; K1: the level's rho
-    const float* rhs;      // this level's rho (n^3)
-    const float* delta;    // prolong: coarse phi
+    // level buffers, of the engine's level type (FP32 levels of the mixed engine, FP64 levels of the
+    // FP64 engine)
+    void* in;              // relax / norm: source phi; restrict: fine phi; prolong: fine phi (updated
+                           // in place); K1: the level's phi[1] (receives the first sweep)
+    void* out;             // relax / norm: destination phi; restrict: coarse rho; K1: the level's rho
+    const void* rhs;       // this level's rho (n^3)
+    const void* delta;     // prolong: coarse phi
     double* u64;           // K1 / update: FP64 solution (grown, pitch sxd)
     const double* f64;     // K1: FP64 right-hand side (n^3)
-    RelaxCoef<float> k;    // n, sx, helm and the smoother's scalars of this level
+    RelaxCoef<float> k;    // n, sx (the level's pitch) and the FP32 smoother's scalars of this level
+    RelaxCoef<double> k64; // FP64 levels: n, sx and the smoother's scalars
     Coefs<float> c;        // relax: L(., omega/6) | L(., 1/h^2); restrict: L(., -1/h^2) | L(., 1/h^2)
-    Coefs<double> c64;     // K1: L(., -1/h^2) | L(., 1/h^2)
-    float alpha, beta;     // Helmholtz scalars
-    double alpha64, beta64;
+    Coefs<double> c64;     // K1: L(., -1/h^2) | L(., 1/h^2); FP64 levels: as c
+    double nscale;         // norm: the residual's Laplacian scale 1/h^2
+    float alpha, beta;     // Helmholtz scalars of the level (FP32 levels)
+    double alpha64, beta64;   // FP64 levels; K1: the top level's
     int sxc;               // prolong: coarse pitch
     int sxd;               // K1 / update: pitch of u64
     int slot;              // solve slot (norms)
@@ -45,6 +52,20 @@ struct SvItem {
     int units;             // rows of this item
     long long unit0;       // first row (multiple of kSvRows)
 };
+
+// the per-level fields of an item in the level type T
+template <typename T> __device__ __forceinline__ const RelaxCoef<T>& sv_k(const SvItem& it);
+template <> __device__ __forceinline__ const RelaxCoef<float>& sv_k<float>(const SvItem& it) { return it.k; }
+template <> __device__ __forceinline__ const RelaxCoef<double>& sv_k<double>(const SvItem& it) { return it.k64; }
+template <typename T> __device__ __forceinline__ const Coefs<T>& sv_c(const SvItem& it);
+template <> __device__ __forceinline__ const Coefs<float>& sv_c<float>(const SvItem& it) { return it.c; }
+template <> __device__ __forceinline__ const Coefs<double>& sv_c<double>(const SvItem& it) { return it.c64; }
+template <typename T> __device__ __forceinline__ T sv_alpha(const SvItem& it);
+template <> __device__ __forceinline__ float sv_alpha<float>(const SvItem& it) { return it.alpha; }
+template <> __device__ __forceinline__ double sv_alpha<double>(const SvItem& it) { return it.alpha64; }
+template <typename T> __device__ __forceinline__ T sv_beta(const SvItem& it);
+template <> __device__ __forceinline__ float sv_beta<float>(const SvItem& it) { return it.beta; }
+template <> __device__ __forceinline__ double sv_beta<double>(const SvItem& it) { return it.beta64; }
 
 struct SvPhaseHeader {
     long long count;       // items
@@ -63,7 +84,9 @@ __device__ __forceinline__ int sv_find(const long long* __restrict__ unit0, int 
     return lo;
 }
 
-enum SvOp { SV_RELAX = 0, SV_RELAX_FIRST = 1, SV_RESTRICT = 2, SV_PROLONG = 3, SV_K1 = 4, SV_UPDATE = 5 };
+// SV_NORM (FP64 engine): the residual max-norm of the solution fused with the next cycle's first
+// sweep, as the FP64 solver's norm pass
+enum SvOp { SV_RELAX = 0, SV_RELAX_FIRST = 1, SV_RESTRICT = 2, SV_PROLONG = 3, SV_K1 = 4, SV_UPDATE = 5, SV_NORM = 6 };
 
 __device__ __forceinline__ void sv_cell(int i, int n, int& x, int& y, int& z)
 {
@@ -72,7 +95,7 @@ __device__ __forceinline__ void sv_cell(int i, int n, int& x, int& y, int& z)
     z = i / (n * n);
 }
 
-template <int OP>
+template <int OP, typename T>
 __global__ void __launch_bounds__(kSvUnit) k_sv_phase(const SvItem* __restrict__ items,
                                                       const long long* __restrict__ unit0,
                                                       const SvPhaseHeader* __restrict__ hdr, double* norms)
@@ -86,7 +109,10 @@ __global__ void __launch_bounds__(kSvUnit) k_sv_phase(const SvItem* __restrict__
         const SvItem& it = items[sv_find(unit0, count, w0)];
         const int row = (int)(w0 - it.unit0) + warp;
         if (row < it.units) {
-            const int n = it.k.n, sx = it.k.sx;
+            const RelaxCoef<T>& kk = sv_k<T>(it);
+            const Coefs<T>& cf = sv_c<T>(it);
+            const T al = sv_alpha<T>(it), be = sv_beta<T>(it);
+            const int n = kk.n, sx = kk.sx;
             if constexpr (OP == SV_RESTRICT) {
                 // a row of coarse cells of the (n/2)^3 level below. Lanes take consecutive fine x of
                 // the two fine rows and two fine planes under the row (coalesced); the taps those
@@ -97,15 +123,15 @@ __global__ void __launch_bounds__(kSvUnit) k_sv_phase(const SvItem* __restrict__
                 const int nc = n / 2;
                 const int y = row % nc, z = row / nc;
                 const long long Sy = sx, Sz = (long long)sx * (n + 2);
-                float* out = it.out + (long long)row * nc;
-                const float* b0 = it.in + grown_index<float>(n, sx, 0, 2 * y, 2 * z);   // fine (0, 2y, 2z)
-                const float* r0 = it.rhs + (long long)n * (2 * y + (long long)n * (2 * z));
+                T* out = static_cast<T*>(it.out) + (long long)row * nc;
+                const T* b0 = static_cast<const T*>(it.in) + grown_index<T>(n, sx, 0, 2 * y, 2 * z);   // fine (0, 2y, 2z)
+                const T* r0 = static_cast<const T*>(it.rhs) + (long long)n * (2 * y + (long long)n * (2 * z));
                 for (int fx0 = 0; fx0 < n; fx0 += 32) {   // uniform over the warp (shuffles below)
                     const int fx = fx0 + lane;
-                    float res[2][2] = {{0.f, 0.f}, {0.f, 0.f}};   // [dy][dz]
+                    T res[2][2] = {{T(0), T(0)}, {T(0), T(0)}};   // [dy][dz]
                     if (fx < n) {
-                        const float* q = b0 + fx;
-                        float c[2][2];
+                        const T* q = b0 + fx;
+                        T c[2][2];
 #pragma unroll
                         for (int dy = 0; dy < 2; dy++)
 #pragma unroll
@@ -114,36 +140,36 @@ __global__ void __launch_bounds__(kSvUnit) k_sv_phase(const SvItem* __restrict__
                         for (int dy = 0; dy < 2; dy++)
 #pragma unroll
                             for (int dz = 0; dz < 2; dz++) {
-                                const float* p = q + dy * Sy + dz * Sz;
+                                const T* p = q + dy * Sy + dz * Sz;
                                 // 0, +x, -x, +y, -y, +z, -z
-                                const float t[7] = {c[dy][dz], p[1], p[-1], dy == 0 ? c[1][dz] : p[Sy],
+                                const T t[7] = {c[dy][dz], p[1], p[-1], dy == 0 ? c[1][dz] : p[Sy],
                                                     dy == 1 ? c[0][dz] : p[-Sy], dz == 0 ? c[dy][1] : p[Sz],
                                                     dz == 1 ? c[dy][0] : p[-Sz]};
-                                const float rho = r0[fx + dy * n + (long long)dz * n * n];
-                                if (!it.k.helm) {
-                                    float v = dadd(0.f, rho);
+                                const T rho = r0[fx + dy * n + (long long)dz * n * n];
+                                if (!kk.helm) {
+                                    T v = dadd(T(0), rho);
 #pragma unroll
-                                    for (int j = 0; j < 7; j++) v = dadd(v, dmul(it.c.c[j], t[j]));
+                                    for (int j = 0; j < 7; j++) v = dadd(v, dmul(cf.c[j], t[j]));
                                     res[dy][dz] = v;
                                 } else {
-                                    float lp = 0.f;
+                                    T lp = T(0);
 #pragma unroll
-                                    for (int j = 0; j < 7; j++) lp = dadd(lp, dmul(it.c.c[j], t[j]));
-                                    res[dy][dz] = dsub(rho, dsub(dmul(it.alpha, t[0]), dmul(it.beta, lp)));
+                                    for (int j = 0; j < 7; j++) lp = dadd(lp, dmul(cf.c[j], t[j]));
+                                    res[dy][dz] = dsub(rho, dsub(dmul(al, t[0]), dmul(be, lp)));
                                 }
                             }
                     }
-                    float odd[2][2];
+                    T odd[2][2];
 #pragma unroll
                     for (int dy = 0; dy < 2; dy++)
 #pragma unroll
                         for (int dz = 0; dz < 2; dz++) odd[dy][dz] = __shfl_down_sync(0xffffffffu, res[dy][dz], 1);
                     if (fx < n && (fx & 1) == 0) {
-                        float acc = 0.f;
+                        T acc = T(0);
 #pragma unroll
                         for (int k = 0; k < 8; k++) {
                             const int dx = k & 1, dy = (k >> 1) & 1, dz = k >> 2;
-                            acc = dadd(acc, dmul(0.125f, dx ? odd[dy][dz] : res[dy][dz]));
+                            acc = dadd(acc, dmul(T(0.125), dx ? odd[dy][dz] : res[dy][dz]));
                         }
                         out[fx / 2] = acc;
                     }
@@ -151,17 +177,19 @@ __global__ void __launch_bounds__(kSvUnit) k_sv_phase(const SvItem* __restrict__
             } else {
                 const int y = row % n, z = row / n;
                 const int ey = edge_code(y, n), ez = edge_code(z, n);
-                const long long g0 = grown_index<float>(n, sx, 0, y, z);   // valid cell x = 0 of the row
+                const long long g0 = grown_index<T>(n, sx, 0, y, z);   // valid cell x = 0 of the row
                 const long long i0 = (long long)row * n;                    // its n^3 index
                 if constexpr (OP == SV_RELAX_FIRST) {
+                    T* const o = static_cast<T*>(it.out);
+                    const T* const rh = static_cast<const T*>(it.rhs);
                     for (int x = lane; x < n; x += 32)
-                        store_with_images(it.out, n, sx, it.out + g0 + x, edge_code(x, n), ey, ez,
-                                          relax_value(it.k, 0.f, 0.f, it.rhs[i0 + x], it.alpha));
+                        store_with_images(o, n, sx, o + g0 + x, edge_code(x, n), ey, ez, relax_value(kk, T(0), T(0), rh[i0 + x], al));
                 } else if constexpr (OP == SV_PROLONG) {
-                    const float* d = it.delta + grown_index<float>(n / 2, it.sxc, 0, y / 2, z / 2);
+                    const T* d = static_cast<const T*>(it.delta) + grown_index<T>(n / 2, it.sxc, 0, y / 2, z / 2);
+                    T* const f = static_cast<T*>(it.in);
                     for (int x = lane; x < n; x += 32) {
-                        float* q = it.in + g0 + x;
-                        store_with_images(it.in, n, sx, q, edge_code(x, n), ey, ez, dadd(*q, dmul(1.f, d[x / 2])));
+                        T* q = f + g0 + x;
+                        store_with_images(f, n, sx, q, edge_code(x, n), ey, ez, dadd(*q, dmul(T(1), d[x / 2])));
                     }
                 }
             }
@@ -197,6 +225,11 @@ __global__ void __launch_bounds__(kSvUnit, 3) k_sv_ring(const SvItem* __restrict
                                                      const SvPhaseHeader* __restrict__ hdr, double* norms)
 {
     constexpr int L = kSvLead, Q = kSvRing, PM = kSvPlane, RS = kSvRowStride;
+    // level type: the mixed engine's FP32 levels (K1 and UPDATE sweep FP32 levels too), or the FP64
+    // engine's levels (its sweeps and the norm pass stage FP64 planes)
+    constexpr bool L64 = (OP == SV_RELAX || OP == SV_NORM) && std::is_same<V, double>::value;
+    static_assert(OP != SV_NORM || L64, "the norm pass runs on FP64 levels");
+    using LT = std::conditional_t<L64, double, float>;
     constexpr int CE = 16 / sizeof(V);                    // elements per 16-byte chunk
     constexpr int NCH = (kSvTX + 2 + CE - 1) / CE;        // chunks per staged row
     constexpr int NST = NCH * (kSvTY + 2);                // chunks per staged plane
@@ -209,20 +242,22 @@ __global__ void __launch_bounds__(kSvUnit, 3) k_sv_ring(const SvItem* __restrict
     for (long long u = blockIdx.x; u < total; u += gridDim.x) {
         const SvItem* itp = items + sv_find(unit0, count, u);
         const int unit = (int)(u - itp->unit0);
-        const RelaxCoef<float> k = itp->k;
+        const RelaxCoef<LT> k = sv_k<LT>(*itp);
         const int n = k.n;
         const int zd = itp->zd;
-        float* const in32 = itp->in;
-        float* const out32 = itp->out;
-        const float* const rhs = itp->rhs;
+        LT* const in_l = static_cast<LT*>(itp->in);
+        LT* const out_l = static_cast<LT*>(itp->out);
+        const LT* const rhs = static_cast<const LT*>(itp->rhs);
         double* const u64 = itp->u64;
         const double* const f64 = itp->f64;
         const int sxd = itp->sxd;
-        const float alpha = itp->alpha;
+        const LT alpha = sv_alpha<LT>(*itp);
         const double alpha64 = itp->alpha64, beta64 = itp->beta64;
+        const double n1 = itp->nscale, n0 = -6.0 * n1;   // NORM: L(., 1/h^2) (centre, the six others)
         Coefs<V> cf;
-        if constexpr (OP == SV_K1) cf = itp->c64;
+        if constexpr (OP == SV_K1 || L64) cf = itp->c64;
         else cf = itp->c;
+        (void)n0;
         int XT, YT, ZT;
         sv_ring_units(n, zd, XT, YT, ZT);
         const int x0 = (unit % XT) * kSvTX, y0 = ((unit / XT) % YT) * kSvTY, z0 = (unit / (XT * YT)) * zd;
@@ -233,7 +268,7 @@ __global__ void __launch_bounds__(kSvUnit, 3) k_sv_ring(const SvItem* __restrict
             src = reinterpret_cast<const V*>(u64);
             sx = sxd;
         } else {
-            src = reinterpret_cast<const V*>(in32);
+            src = in_l;
             sx = k.sx;
         }
         const long long Sz = (long long)sx * (n + 2);
@@ -280,11 +315,11 @@ __global__ void __launch_bounds__(kSvUnit, 3) k_sv_ring(const SvItem* __restrict
         const int ex = xin ? edge_code(x, n) : 0;
         const int cidx = (YC * warp + 1) * RS + lane + 1;  // cell (x, ya) in a ring plane
         int i = act[0] ? x + n * (ya + n * z0) : 0;        // (x, ya, z) in the n^3 fields
-        // the grown field this phase writes (RELAX: out32, K1: in32, UPDATE: u64): cell (x, ya, z0),
+        // the grown field this phase writes (RELAX / NORM: out, K1: in, UPDATE: u64): cell (x, ya, z0),
         // advanced one plane per z step, and the offsets of the periodic images of this thread's
         // cells (x and y per thread and row, z per plane; 0 where there is none)
-        using Wt = std::conditional_t<OP == SV_UPDATE, double, float>;
-        Wt* const wbase = OP == SV_UPDATE ? reinterpret_cast<Wt*>(u64) : reinterpret_cast<Wt*>(OP == SV_K1 ? in32 : out32);
+        using Wt = std::conditional_t<OP == SV_UPDATE, double, LT>;
+        Wt* const wbase = OP == SV_UPDATE ? reinterpret_cast<Wt*>(u64) : reinterpret_cast<Wt*>(OP == SV_K1 ? in_l : out_l);
         const int wsx = OP == SV_UPDATE ? sxd : k.sx;
         const long long wSz = (long long)wsx * (n + 2);
         Wt* wp = wbase + (act[0] ? grown_index<Wt>(n, wsx, x, ya, z0) : 0);
@@ -294,7 +329,7 @@ __global__ void __launch_bounds__(kSvUnit, 3) k_sv_ring(const SvItem* __restrict
         for (int r = 0; r < YC; r++) oyo[r] = ey[r] == 1 ? n * wsx : (ey[r] == 2 ? -n * wsx : 0);
         const long long ozn = (long long)n * wSz;
         double m = 0.0;
-        bool bad = false;     // K1: a residual that is not finite (the norm itself skips NaN, as
+        bool bad = false;     // K1 / NORM: a residual that is not finite (the norm itself skips NaN, as
                               // Reduction<Abs> does); the solve's norm is then reported as +inf
         // v at q (a valid cell) and at its periodic images (the stores store_with_images makes)
         auto put = [&](Wt* q, int oy, long long oz, Wt v) {
@@ -311,7 +346,7 @@ __global__ void __launch_bounds__(kSvUnit, 3) k_sv_ring(const SvItem* __restrict
             }
         };
         // one cell: the stencil taps, the plane's pointwise inputs and the outputs of this phase
-        auto cell = [&](Wt* q, int oy, long long oz, int ii, V zm, V zc, V zp, V xm, V xp, V ym, V yp, float rr,
+        auto cell = [&](Wt* q, int oy, long long oz, int ii, V zm, V zc, V zp, V xm, V xp, V ym, V yp, LT rr,
                         double dd) {
             // Laplacian insertion order: 0, +x, -x, +y, -y, +z, -z
             if constexpr (OP == SV_K1) {
@@ -341,29 +376,51 @@ __global__ void __launch_bounds__(kSvUnit, 3) k_sv_ring(const SvItem* __restrict
                 m = upd_abs(m, res);
                 bad = bad || !(fabs(res) <= DBL_MAX);
                 const float r32 = __double2float_rn(res);
-                out32[ii] = r32;
+                out_l[ii] = r32;
                 put(q, oy, oz, relax_value(k, 0.f, 0.f, r32, al));
             } else {
-                float acc = 0.f;
-                acc = dadd(acc, dmul(cf.c[0], (float)zc));
-                acc = dadd(acc, dmul(cf.c[1], (float)xp));
-                acc = dadd(acc, dmul(cf.c[2], (float)xm));
-                acc = dadd(acc, dmul(cf.c[3], (float)yp));
-                acc = dadd(acc, dmul(cf.c[4], (float)ym));
-                acc = dadd(acc, dmul(cf.c[5], (float)zp));
-                acc = dadd(acc, dmul(cf.c[6], (float)zm));
-                const float v = relax_value(k, acc, (float)zc, rr, alpha);
-                if constexpr (OP == SV_RELAX) put(q, oy, oz, v);
-                else put(q, oy, oz, dadd(dd, (double)v));
+                LT acc = LT(0);
+                acc = dadd(acc, dmul(cf.c[0], (LT)zc));
+                acc = dadd(acc, dmul(cf.c[1], (LT)xp));
+                acc = dadd(acc, dmul(cf.c[2], (LT)xm));
+                acc = dadd(acc, dmul(cf.c[3], (LT)yp));
+                acc = dadd(acc, dmul(cf.c[4], (LT)ym));
+                acc = dadd(acc, dmul(cf.c[5], (LT)zp));
+                acc = dadd(acc, dmul(cf.c[6], (LT)zm));
+                const LT v = relax_value(k, acc, (LT)zc, rr, alpha);
+                if constexpr (OP == SV_NORM) {
+                    // the FP64 solver's norm: Poisson (0 - rho) + L(phi, 1/h^2); Helmholtz
+                    // rho - (alpha*phi - beta*L(phi, 1/h^2)), whose sum is the sweep's own
+                    double r2;
+                    if (!k.helm) {
+                        r2 = dsub(0.0, (double)rr);
+                        r2 = dadd(r2, dmul(n0, (double)zc));
+                        r2 = dadd(r2, dmul(n1, (double)xp));
+                        r2 = dadd(r2, dmul(n1, (double)xm));
+                        r2 = dadd(r2, dmul(n1, (double)yp));
+                        r2 = dadd(r2, dmul(n1, (double)ym));
+                        r2 = dadd(r2, dmul(n1, (double)zp));
+                        r2 = dadd(r2, dmul(n1, (double)zm));
+                    } else {
+                        r2 = dsub((double)rr, dsub(dmul((double)alpha, (double)zc), dmul((double)k.beta, (double)acc)));
+                    }
+                    m = upd_abs(m, r2);
+                    bad = bad || !(fabs(r2) <= DBL_MAX);
+                    put(q, oy, oz, v);
+                } else if constexpr (OP == SV_RELAX) {
+                    put(q, oy, oz, v);
+                } else {
+                    put(q, oy, oz, dadd(dd, (double)v));
+                }
             }
         };
         int qz = 0;
         for (int z = z0; z < z1; z++) {
-            float rr[YC];
+            LT rr[YC];
             double dd[YC];
 #pragma unroll
             for (int r = 0; r < YC; r++) {
-                rr[r] = 0.f;
+                rr[r] = LT(0);
                 dd[r] = 0.0;
                 if constexpr (OP == SV_K1) {
                     if (act[r]) dd[r] = f64[i + r * n];
@@ -412,7 +469,7 @@ __global__ void __launch_bounds__(kSvUnit, 3) k_sv_ring(const SvItem* __restrict
         }
         cp_async_wait<0>();
         __syncthreads();              // the ring is free for the next unit
-        if constexpr (OP == SV_K1) {
+        if constexpr (OP == SV_K1 || OP == SV_NORM) {
             if (__any_sync(0xffffffffu, bad)) m = CUDART_INF;
             for (int o = 16; o > 0; o >>= 1) {
                 const double w = __shfl_down_sync(0xffffffffu, m, o);
@@ -435,7 +492,8 @@ static __global__ void __launch_bounds__(256) k_sv_pack_out(const double* __rest
 }
 
 // constant fill (alpha fields of the coarse levels)
-static __global__ void __launch_bounds__(256) k_sv_fill(float* p, long long n, float v)
+template <typename T>
+__global__ void __launch_bounds__(256) k_sv_fill(T* p, long long n, T v)
 {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) p[i] = v;
 }

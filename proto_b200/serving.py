@@ -5,7 +5,8 @@
                   alpha ~ U[0, 1] (Helmholtz, beta = 1), a right-hand side of 4 sine modes per request
                   (its own seed), tolerance on the relative max-norm residual.
   TraceData       every request's right-hand side and a result slot, in two page-locked host arrays.
-  serve_trace     the serving engine (pb_serve): requests join the in-flight batch as they arrive.
+  serve_trace     the serving engine (pb_serve, mixed precision or FP64): requests join the in-flight
+                  batch as they arrive.
   single_trace    plain multigrid (pb_mg, FP64 or mixed precision), one request at a time in arrival
                   order: the FP64 arm is the baseline, the mixed arm separates what precision gains
                   from what batching gains.
@@ -198,17 +199,20 @@ def verify(pb, trace, data, fp64):
     """Relative max-norm error of every result in data.out against the FP64 solver's solution of the
     same request: max |out - ref| / max |ref| per request; and the same with each field's mean
     removed first, since a periodic Poisson solution is defined up to a constant (and a Helmholtz
-    one with a small alpha only weakly fixes it). Returns max, p99 and median of both."""
+    one with a small alpha only weakly fixes it). Returns max, p99 and median of both, and how many
+    results are bitwise the FP64 solver's."""
     import torch
     errs = np.zeros(len(trace))
     errs0 = np.zeros(len(trace))
+    same = 0
     for r in trace:
         _, _, ref = fp64.solve(r, data.rhs_of(r["i"]))
         got = torch.from_numpy(data.out_of(r["i"])).to("cuda", non_blocking=True)
+        same += int(torch.equal(got, ref))
         errs[r["i"]] = float((got - ref).abs().max() / ref.abs().max())
         ref0 = ref - ref.mean()
         errs0[r["i"]] = float(((got - got.mean()) - ref0).abs().max() / ref0.abs().max())
 
     def stats(e):
         return {"max": float(e.max()), "p99": float(np.percentile(e, 99)), "median": float(np.median(e))}
-    return {"requests": len(trace), "rel_err": stats(errs), "rel_err_mean_removed": stats(errs0)}
+    return {"requests": len(trace), "bitwise_equal": same, "rel_err": stats(errs), "rel_err_mean_removed": stats(errs0)}

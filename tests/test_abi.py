@@ -122,12 +122,23 @@ def test_serve_host_rules():
     assert pb.Serve.request_bytes(16 * 12) > 8 * 192 ** 3 * 2
     assert pb.Serve.request_bytes(64) < pb.Serve.request_bytes(128)
     h = ctypes.c_void_p()
-    bad = pb.pb_serve_params(1 << 30, 0, 4, 4, 10, 2.0 / 3.0, 1e-8, 100)   # no slots
+    bad = pb.pb_serve_params(1 << 30, 0, 4, 4, 10, 2.0 / 3.0, 1e-8, 100, pb.MG_MIXED)   # no slots
     assert L.pb_serve_create(ctypes.byref(bad), ctypes.byref(h)) == -1
-    bad = pb.pb_serve_params(1 << 30, 4, 0, 4, 10, 2.0 / 3.0, 1e-8, 100)   # nu1 = 0
+    bad = pb.pb_serve_params(1 << 30, 4, 0, 4, 10, 2.0 / 3.0, 1e-8, 100, pb.MG_MIXED)   # nu1 = 0
     assert L.pb_serve_create(ctypes.byref(bad), ctypes.byref(h)) == -1
-    bad = pb.pb_serve_params(0, 4, 4, 4, 10, 2.0 / 3.0, 1e-8, 100)         # no budget
+    bad = pb.pb_serve_params(0, 4, 4, 4, 10, 2.0 / 3.0, 1e-8, 100, pb.MG_MIXED)   # no budget
     assert L.pb_serve_create(ctypes.byref(bad), ctypes.byref(h)) == -1
+    bad = pb.pb_serve_params(1 << 30, 4, 4, 4, 10, 2.0 / 3.0, 1e-8, 100, 7)  # no such precision
+    assert L.pb_serve_create(ctypes.byref(bad), ctypes.byref(h)) == -1
+    bad = pb.pb_serve_params(1 << 30, 4, 4, 3, 10, 2.0 / 3.0, 1e-8, 100, pb.MG_FP64)   # FP64: nu1 + nu2 odd
+    assert L.pb_serve_create(ctypes.byref(bad), ctypes.byref(h)) == -1
+    # an FP64 hierarchy: every level in FP64 (the top level is the solution), no FP32 copies
+    n = 64
+    lv = sum(8 * (((e + 2 + 1) // 2 * 2) * (e + 2) ** 2 * 2 + e ** 3) for e in (64, 32))
+    assert pb.Serve.request_bytes(n, pb.MG_FP64) > lv
+    assert pb.Serve.request_bytes(33, pb.MG_FP64) == -1
+    assert L.pb_serve_hierarchy_bytes(64, 7) == -1
+    assert pb.Serve.request_bytes(64) == L.pb_serve_request_bytes(64)
 
 
 def test_wait_expiry_hook_validates_arguments():

@@ -97,7 +97,7 @@ int read_error_serve();
 int read_error_fas();
 
 // ---------------------------------------------------------------------------------------------
-// Exact arithmetic: one IEEE rounding per operation, never contracted into FMA
+// Exact arithmetic: one IEEE rounding per operation, never contracted into FMA (FP32 sums: dmadd)
 // ---------------------------------------------------------------------------------------------
 __device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
@@ -107,6 +107,13 @@ __device__ __forceinline__ float dmul(float a, float b) { return __fmul_rn(a, b)
 __device__ __forceinline__ float dadd(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ float dsub(float a, float b) { return __fsub_rn(a, b); }
 __device__ __forceinline__ float ddiv(float a, float b) { return __fdiv_rn(a, b); }
+// acc + a*b, the step of every stencil, restriction and smoother sum: FP64 rounds the product and
+// the sum separately (the reference's arithmetic, bit for bit); FP32 (mixed-precision cycles and the
+// FP32 API, not held to the reference's rounding) takes one fused multiply-add, half the instructions
+// of the issue-bound FP32 sweeps. Every FP32 level kernel, single-solve and served, uses it, so their
+// results stay bitwise equal to one another.
+__device__ __forceinline__ double dmadd(double acc, double a, double b) { return __dadd_rn(acc, __dmul_rn(a, b)); }
+__device__ __forceinline__ float dmadd(float acc, float a, float b) { return __fmaf_rn(a, b, acc); }
 // the quotient of a Jacobi update: FP64 keeps the correctly rounded division (the reference's
 // arithmetic, bit for bit); FP32 (mixed-precision cycles, whose error the FP64 residual and
 // correction remove) takes the reciprocal-multiply form (within 2 ulp), two instructions instead

@@ -164,7 +164,7 @@ struct RelaxCoef {
 template <typename T>
 __device__ __forceinline__ T relax_value(const RelaxCoef<T>& k, T acc, T c, T rho, T al)
 {
-    if (!k.helm) return dadd(c, dadd(acc, dmul(k.neg_lambda, rho)));
+    if (!k.helm) return dadd(c, dmadd(acc, k.neg_lambda, rho));
     const T r = dsub(rho, dsub(dmul(al, c), dmul(k.beta, acc)));
     return dadd(c, squot(dmul(k.omega, r), dadd(al, k.diagB)));
 }
@@ -366,7 +366,7 @@ __global__ void __launch_bounds__(256) k_bottom_direct(const T* __restrict__ ain
     const int N = n * n * n;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
         T acc = T(0);
-        for (int j = 0; j < N; j++) acc = dadd(acc, dmul(ainv[(long long)i * N + j], rhs[j]));
+        for (int j = 0; j < N; j++) acc = dmadd(acc, ainv[(long long)i * N + j], rhs[j]);
         store_periodic(out, n, sx, i % n, (i / n) % n, i / (n * n), acc);
     }
 }
@@ -388,7 +388,7 @@ __device__ __forceinline__ T fine_residual(const T* phi, long long gi, long long
 #pragma unroll
         for (int j = 0; j < ShapeLap7::NT; j++) {
             const long long o = ShapeLap7::off(j, 0) + Sy * ShapeLap7::off(j, 1) + Sz * ShapeLap7::off(j, 2);
-            r = dadd(r, dmul(cf.c[j], phi[gi + o]));
+            r = dmadd(r, cf.c[j], phi[gi + o]);
         }
         return r;
     }
@@ -396,7 +396,7 @@ __device__ __forceinline__ T fine_residual(const T* phi, long long gi, long long
 #pragma unroll
     for (int j = 0; j < ShapeLap7::NT; j++) {
         const long long o = ShapeLap7::off(j, 0) + Sy * ShapeLap7::off(j, 1) + Sz * ShapeLap7::off(j, 2);
-        lp = dadd(lp, dmul(cf.c[j], phi[gi + o]));
+        lp = dmadd(lp, cf.c[j], phi[gi + o]);
     }
     return dsub(rho, dsub(dmul(al, phi[gi]), dmul(beta, lp)));
 }
@@ -420,7 +420,7 @@ __global__ void __launch_bounds__(256) k_resid_restrict(const T* __restrict__ ph
         const long long fi = fx + (long long)nf * (fy + (long long)nf * fz);
         const T al = helm ? __ldg(alpha + fi) : T(0);
         const T r = fine_residual(phi, grown_index<T>(nf, sx, fx, fy, fz), Sy, Sz, __ldg(rhs + fi), al, helm, cf, beta);
-        acc = dadd(acc, dmul(eighth, r));
+        acc = dmadd(acc, eighth, r);
     }
     rhs_c[cx + (long long)nc * (cy + (long long)nc * cz)] = acc;
 }
@@ -470,7 +470,7 @@ struct EpiRestrict {
         if (!r.act) return;
         T res = acc;
         if (helm) res = dsub(ax.get<T>(0), dsub(dmul(ax.get<T>(1), c), dmul(beta, acc)));
-        sum = dadd(sum, dmul(T(1.0 / 8), res));
+        sum = dmadd(sum, T(1.0 / 8), res);
         if (child == 7) r.out[(long long)(zo >> 1) * nc * nc] = sum;
     }
     __device__ __forceinline__ void end_warp() const {}
@@ -531,12 +531,12 @@ __global__ void __launch_bounds__(256) k_resid_restrict_z(const T* __restrict__ 
                     if (!helm) {
                         T v = dadd(T(0), rho);
 #pragma unroll
-                        for (int j = 0; j < 7; j++) v = dadd(v, dmul(cf.c[j], t[j]));
+                        for (int j = 0; j < 7; j++) v = dmadd(v, cf.c[j], t[j]);
                         res[r][pz] = v;
                     } else {
                         T lp = T(0);
 #pragma unroll
-                        for (int j = 0; j < 7; j++) lp = dadd(lp, dmul(cf.c[j], t[j]));
+                        for (int j = 0; j < 7; j++) lp = dmadd(lp, cf.c[j], t[j]);
                         res[r][pz] = dsub(rho, dsub(dmul(__ldg(alpha + fi), c), dmul(beta, lp)));
                     }
                 }
@@ -555,7 +555,7 @@ __global__ void __launch_bounds__(256) k_resid_restrict_z(const T* __restrict__ 
 #pragma unroll
             for (int k = 0; k < 8; k++) {
                 const int dx = k & 1, dy = (k >> 1) & 1, dz = k >> 2;
-                acc = dadd(acc, dmul(eighth, dx ? odd[dy][dz] : res[dy][dz]));
+                acc = dmadd(acc, eighth, dx ? odd[dy][dz] : res[dy][dz]);
             }
             rhs_c[fx / 2 + (long long)nc * (cy + (long long)nc * cz)] = acc;
         }
@@ -734,7 +734,7 @@ __device__ void coarse_relax(const CoarseLevel<T>& L, int cur, bool first)
 #pragma unroll
             for (int j = 0; j < ShapeLap7::NT; j++) {
                 const long long o = ShapeLap7::off(j, 0) + Sy * ShapeLap7::off(j, 1) + Sz * ShapeLap7::off(j, 2);
-                acc = dadd(acc, dmul(L.crelax.c[j], src[g + o]));
+                acc = dmadd(acc, L.crelax.c[j], src[g + o]);
             }
             v = relax_value(L.k, acc, src[g], L.rhs[i], al);
         }
@@ -813,7 +813,7 @@ __device__ void coarse_cycle_body(const CoarseArgs<T>& ga, const CoarseOffsets& 
                 const T al = L.k.helm ? L.alpha[fi] : T(0);
                 const T r = fine_residual(phi, grown_index<T>(nf, sx, fx, fy, fz), Sy, Sz, L.rhs[fi], al, L.k.helm,
                                           L.cres, a.beta);
-                acc = dadd(acc, dmul(T(1.0 / 8), r));
+                acc = dmadd(acc, T(1.0 / 8), r);
             }
             C.rhs[i] = acc;
         }
@@ -826,7 +826,7 @@ __device__ void coarse_cycle_body(const CoarseArgs<T>& ga, const CoarseOffsets& 
             const int n = B.k.n, N = n * n * n;
             for (int i = threadIdx.x; i < N; i += blockDim.x) {
                 T acc = T(0);
-                for (int j = 0; j < N; j++) acc = dadd(acc, dmul(a.ainv[(long long)i * N + j], B.rhs[j]));
+                for (int j = 0; j < N; j++) acc = dmadd(acc, a.ainv[(long long)i * N + j], B.rhs[j]);
                 store_periodic(B.phi[0], n, B.k.sx, i % n, (i / n) % n, i / (n * n), acc);
             }
             __syncthreads();

@@ -261,7 +261,7 @@ __global__ void __launch_bounds__(2 * NXT + 32, relax2_min_blocks(2 * NXT + 32))
         for (int r = 0; r < RG; r++) oyr[r] = image_offset(ys + JO + r, N, sx);
         // relax_value with the form fixed at compile time (the same operations in the same order)
         auto rv = [&](T acc, T c, T rho, T al) -> T {
-            if constexpr (!HELM) return dadd(c, dadd(acc, dmul(k.neg_lambda, rho)));
+            if constexpr (!HELM) return dadd(c, dmadd(acc, k.neg_lambda, rho));
             else {
                 const T r = dsub(rho, dsub(dmul(al, c), dmul(k.beta, acc)));
                 return dadd(c, squot(dmul(k.omega, r), dadd(al, k.diagB)));
@@ -350,25 +350,25 @@ __global__ void __launch_bounds__(2 * NXT + 32, relax2_min_blocks(2 * NXT + 32))
                         tpz = w0[SN][j][v];
                         tmz = w0[SO][j][v];
                         T acc = T(0);
-                        acc = dadd(acc, dmul(a.c.c[0], tc));
-                        acc = dadd(acc, dmul(a.c.c[1], tpx));
-                        acc = dadd(acc, dmul(a.c.c[2], tmx));
-                        acc = dadd(acc, dmul(a.c.c[3], tpy));
-                        acc = dadd(acc, dmul(a.c.c[4], tmy));
-                        acc = dadd(acc, dmul(a.c.c[5], tpz));
-                        acc = dadd(acc, dmul(a.c.c[6], tmz));
+                        acc = dmadd(acc, a.c.c[0], tc);
+                        acc = dmadd(acc, a.c.c[1], tpx);
+                        acc = dmadd(acc, a.c.c[2], tmx);
+                        acc = dmadd(acc, a.c.c[3], tpy);
+                        acc = dmadd(acc, a.c.c[4], tmy);
+                        acc = dmadd(acc, a.c.c[5], tpz);
+                        acc = dmadd(acc, a.c.c[6], tmz);
                         v1 = rv(acc, tc, rho, al);
                     }
                     // the norm at the tile's own rows and planes only: every cell of the level once
                     if (NORM && j - JO >= 0 && j - JO < RG && own_plane) {
                         T a2 = HELM ? T(0) : dsub(T(0), rho);
-                        a2 = dadd(a2, dmul(a.c2.c[0], tc));
-                        a2 = dadd(a2, dmul(a.c2.c[1], tpx));
-                        a2 = dadd(a2, dmul(a.c2.c[2], tmx));
-                        a2 = dadd(a2, dmul(a.c2.c[3], tpy));
-                        a2 = dadd(a2, dmul(a.c2.c[4], tmy));
-                        a2 = dadd(a2, dmul(a.c2.c[5], tpz));
-                        a2 = dadd(a2, dmul(a.c2.c[6], tmz));
+                        a2 = dmadd(a2, a.c2.c[0], tc);
+                        a2 = dmadd(a2, a.c2.c[1], tpx);
+                        a2 = dmadd(a2, a.c2.c[2], tmx);
+                        a2 = dmadd(a2, a.c2.c[3], tpy);
+                        a2 = dmadd(a2, a.c2.c[4], tmy);
+                        a2 = dmadd(a2, a.c2.c[5], tpz);
+                        a2 = dmadd(a2, a.c2.c[6], tmz);
                         if constexpr (!HELM) m = upd_abs(m, (double)a2);
                         else m = upd_abs(m, (double)dsub(rho, dsub(dmul(al, tc), dmul(a.beta, a2))));
                     }
@@ -405,13 +405,13 @@ __global__ void __launch_bounds__(2 * NXT + 32, relax2_min_blocks(2 * NXT + 32))
                         const T tmy = r > 0 ? p1[QC][r - 1][v] : b1r[(r - 1) * N + x];
                         const T tpz = p1[QP][r][v], tmz = p1[QM][r][v];
                         T acc = T(0);
-                        acc = dadd(acc, dmul(a.c.c[0], tc));
-                        acc = dadd(acc, dmul(a.c.c[1], tpx));
-                        acc = dadd(acc, dmul(a.c.c[2], tmx));
-                        acc = dadd(acc, dmul(a.c.c[3], tpy));
-                        acc = dadd(acc, dmul(a.c.c[4], tmy));
-                        acc = dadd(acc, dmul(a.c.c[5], tpz));
-                        acc = dadd(acc, dmul(a.c.c[6], tmz));
+                        acc = dmadd(acc, a.c.c[0], tc);
+                        acc = dmadd(acc, a.c.c[1], tpx);
+                        acc = dmadd(acc, a.c.c[2], tmx);
+                        acc = dmadd(acc, a.c.c[3], tpy);
+                        acc = dmadd(acc, a.c.c[4], tmy);
+                        acc = dmadd(acc, a.c.c[5], tpz);
+                        acc = dmadd(acc, a.c.c[6], tmz);
                         T al = T(0);
                         if constexpr (HELM) al = ao2[r][v];
                         v2s[r][v] = rv(acc, tc, ro2[r][v], al);

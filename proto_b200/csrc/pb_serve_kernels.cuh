@@ -149,12 +149,12 @@ __global__ void __launch_bounds__(kSvUnit) k_sv_phase(const SvItem* __restrict__
                                 if (!kk.helm) {
                                     T v = dadd(T(0), rho);
 #pragma unroll
-                                    for (int j = 0; j < 7; j++) v = dadd(v, dmul(cf.c[j], t[j]));
+                                    for (int j = 0; j < 7; j++) v = dmadd(v, cf.c[j], t[j]);
                                     res[dy][dz] = v;
                                 } else {
                                     T lp = T(0);
 #pragma unroll
-                                    for (int j = 0; j < 7; j++) lp = dadd(lp, dmul(cf.c[j], t[j]));
+                                    for (int j = 0; j < 7; j++) lp = dmadd(lp, cf.c[j], t[j]);
                                     res[dy][dz] = dsub(rho, dsub(dmul(al, t[0]), dmul(be, lp)));
                                 }
                             }
@@ -169,7 +169,7 @@ __global__ void __launch_bounds__(kSvUnit) k_sv_phase(const SvItem* __restrict__
 #pragma unroll
                         for (int k = 0; k < 8; k++) {
                             const int dx = k & 1, dy = (k >> 1) & 1, dz = k >> 2;
-                            acc = dadd(acc, dmul(T(0.125), dx ? odd[dy][dz] : res[dy][dz]));
+                            acc = dmadd(acc, T(0.125), dx ? odd[dy][dz] : res[dy][dz]);
                         }
                         out[fx / 2] = acc;
                     }
@@ -380,13 +380,13 @@ __global__ void __launch_bounds__(kSvUnit, 3) k_sv_ring(const SvItem* __restrict
                 put(q, oy, oz, relax_value(k, 0.f, 0.f, r32, al));
             } else {
                 LT acc = LT(0);
-                acc = dadd(acc, dmul(cf.c[0], (LT)zc));
-                acc = dadd(acc, dmul(cf.c[1], (LT)xp));
-                acc = dadd(acc, dmul(cf.c[2], (LT)xm));
-                acc = dadd(acc, dmul(cf.c[3], (LT)yp));
-                acc = dadd(acc, dmul(cf.c[4], (LT)ym));
-                acc = dadd(acc, dmul(cf.c[5], (LT)zp));
-                acc = dadd(acc, dmul(cf.c[6], (LT)zm));
+                acc = dmadd(acc, cf.c[0], (LT)zc);
+                acc = dmadd(acc, cf.c[1], (LT)xp);
+                acc = dmadd(acc, cf.c[2], (LT)xm);
+                acc = dmadd(acc, cf.c[3], (LT)yp);
+                acc = dmadd(acc, cf.c[4], (LT)ym);
+                acc = dmadd(acc, cf.c[5], (LT)zp);
+                acc = dmadd(acc, cf.c[6], (LT)zm);
                 const LT v = relax_value(k, acc, (LT)zc, rr, alpha);
                 if constexpr (OP == SV_NORM) {
                     // the FP64 solver's norm: Poisson (0 - rho) + L(phi, 1/h^2); Helmholtz

@@ -352,8 +352,8 @@ __global__ void __launch_bounds__(kStarTX * (TY / YB) + 32, star_min_blocks(TY, 
                     else if (oy == 0 && v + ox >= 0 && v + ox < XV) val = win[r][v + ox][IC];   // this thread's point
                     else if (ox == 0 && r + oy >= 0 && r + oy < YB) val = win[r + oy][v][IC];   // this thread's row
                     else val = pc[sc0 + (r + oy) * SM::BX + v + ox];
-                    acc = dadd(acc, dmul(cf.c[j], val));
-                    if constexpr (two_sums<Epi>::value) acc2 = dadd(acc2, dmul(epi.c2.c[j], val));
+                    acc = dmadd(acc, cf.c[j], val);
+                    if constexpr (two_sums<Epi>::value) acc2 = dmadd(acc2, epi.c2.c[j], val);
                 }
                 if constexpr (two_sums<Epi>::value) epi.template finish2<ZE>(rows[r], zo, v, acc, acc2, win[r][v][IC], ax);
                 else epi.template finish<ZE>(rows[r], zo, v, acc, win[r][v][IC], ax);
@@ -411,8 +411,8 @@ __global__ void __launch_bounds__(256) k_star_simple(const T* __restrict__ src, 
         for (int j = 0; j < S::NT; j++) {
             const long long o = S::off(j, 0) + Sx * S::off(j, 1) + Sxy * S::off(j, 2);
             const T val = __ldg(src + base + o);
-            acc = dadd(acc, dmul(cf.c[j], val));
-            if constexpr (two_sums<Epi>::value) acc2 = dadd(acc2, dmul(epi.c2.c[j], val));
+            acc = dmadd(acc, cf.c[j], val);
+            if constexpr (two_sums<Epi>::value) acc2 = dmadd(acc2, epi.c2.c[j], val);
         }
         bool ze = false;
         if constexpr (Epi::kZEdge) ze = epi.z_edge(z);

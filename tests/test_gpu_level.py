@@ -129,9 +129,10 @@ def test_level13_graph_steps_golden(golden, pb, tune):
     pb.device_check()
 
 
-def test_amr_level_full_size_against_port(golden, pb, port):
-    """The 512-patch uneven level (widths from seed 2), autotuned tiles, 4 graph steps: bitwise the
-    C port's periodic stepping on the whole domain."""
+@pytest.mark.parametrize("steps", [4, 100])
+def test_amr_level_full_size_against_port(golden, pb, port, steps):
+    """The 512-patch uneven level (widths from seed 2), autotuned tiles, 4 graph steps and the
+    measured workload's 100: bitwise the C port's periodic stepping on the whole domain."""
     import torch
     widths = W.amr_widths(seed=2)
     lv, S, (c, o), u, a, L = _level13(golden, pb, widths, 7)
@@ -139,14 +140,14 @@ def test_amr_level_full_size_against_port(golden, pb, port):
     h = 1.0 / L[0]
     b = torch.zeros_like(a)
     lv.autotune(S, a, b, scale=1.0 / (h * h))
-    lv.steps(S, pb.EPI_EULER, a, b, 4, scale=1.0 / (h * h), a=0.1 * h * h)
+    lv.steps(S, pb.EPI_EULER, a, b, steps, scale=1.0 / (h * h), a=0.1 * h * h)
     torch.cuda.synchronize()
     got = a.cpu().numpy()
     gh = 2
     G = np.zeros((L[2] + 2 * gh, L[1] + 2 * gh, L[0] + 2 * gh))
     G[gh:-gh, gh:-gh, gh:-gh] = u
     G = G.reshape(-1).copy()
-    port.periodic_steps(L, gh, c, o.reshape(-1), h, 0.1 * h * h, 4, G)
+    port.periodic_steps(L, gh, c, o.reshape(-1), h, 0.1 * h * h, steps, G)
     ref = G.reshape(L[2] + 2 * gh, L[1] + 2 * gh, L[0] + 2 * gh)[gh:-gh, gh:-gh, gh:-gh]
     out = np.zeros_like(u)
     for p, off in zip(lv.patches, lv.offsets):

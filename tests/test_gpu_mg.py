@@ -113,6 +113,31 @@ def test_direct_bottom_poisson_bitwise(pb, port):
     assert np.array_equal(phi, p2)
 
 
+@pytest.mark.parametrize("form", ["poisson", "helmholtz"])
+def test_odd_coarsest_direct_bottom_bitwise(pb, port, form):
+    """An odd coarsest grid (96^3 over five halvings to 3^3, the shape of the 384^3 hierarchy) with
+    the exact bottom solve, Poisson and per-cell-alpha Helmholtz: history and solution bitwise the C
+    port's."""
+    N, lev = 96, 5
+    alpha = W.helmholtz_alpha(N, seed=3) if form == "helmholtz" else None
+    rhs = -W.poisson_rho(N, seed=1) if alpha is not None else W.poisson_rho(N, seed=1)
+    it, hist, phi = _gpu_solve(pb, N, lev, pb.MG_FP64, max_iter=20, alpha=alpha, rhs=rhs, bottom=1)
+    p2 = np.zeros(N ** 3)
+    n2, h2 = port.mg_cs(N, lev, 4, 4, 10, 2.0 / 3.0, 1.0, None if alpha is None else alpha.reshape(-1).copy(), 20,
+                        1e-10, rhs.reshape(-1).copy(), p2, bottom=1)
+    assert it == n2 and hist == list(h2)
+    assert np.array_equal(phi, p2)
+    assert hist[-1] < 1e-10 * hist[0]
+    # mixed precision on the same hierarchy reaches the tolerance close to the FP64 solution
+    itm, hm, phim = _gpu_solve(pb, N, lev, pb.MG_MIXED, max_iter=20, alpha=alpha, rhs=rhs, bottom=1)
+    assert hm[-1] < 1e-10 * hm[0] and itm <= it + 2
+    d = phim - phi
+    ref = phi
+    if alpha is None:   # a periodic Poisson solution is defined up to a constant
+        d, ref = d - d.mean(), phi - phi.mean()
+    assert np.max(np.abs(d)) / np.max(np.abs(ref)) < 1e-7
+
+
 def test_mixed_helmholtz_direct_bottom(pb):
     N, lev = 64, 3
     alpha = W.helmholtz_alpha(N, seed=3)

@@ -561,6 +561,112 @@ __global__ void __launch_bounds__(256) k_resid_restrict_z(const T* __restrict__ 
         }
     }
 }
+// The same restriction with x pairs: lane = coarse x, so a thread's fine columns 2cx and 2cx+1 (a
+// coarse cell's x children) and their x neighbours 2cx-1 and 2cx+2 come from two aligned 2-wide
+// loads per row and plane (grown x index 2cx is even and rows start 16-byte aligned), a warp covers
+// 64 consecutive fine cells, and no shuffle is needed. Block (32, 8) = 32 coarse x by 8 coarse rows;
+// the block walks coarse planes [cz0, cz0 + czc) with the register window of k_resid_restrict_z.
+// Same taps, same order, same child sum: bitwise that kernel's results. Needs nf even, nf >= 64.
+template <typename T> struct Pair;
+template <> struct Pair<float> { using type = float2; };
+template <> struct Pair<double> { using type = double2; };
+template <typename T>
+__global__ void __launch_bounds__(256) k_resid_restrict_x2(const T* __restrict__ phi, const T* __restrict__ rhs,
+                                                           const T* __restrict__ alpha, T* rhs_c, int nf, int sx,
+                                                           int helm, Coefs<T> cf, T beta, int czc)
+{
+    using P2 = typename Pair<T>::type;
+    const int nc = nf / 2;
+    const int cx = blockIdx.x * 32 + threadIdx.x, cy = blockIdx.y * 8 + threadIdx.y;
+    const int cz0 = blockIdx.z * czc, cz1 = min(cz0 + czc, nc);
+    const bool act = cx < nc && cy < nc;
+    const long long Sy = sx, Sz = (long long)sx * (nf + 2);
+    const T eighth = T(1.0 / 8);
+    const int fx = 2 * cx, fy0 = 2 * cy;
+    // fine (fx - 1, fy0, 0): the first element of an aligned pair
+    const T* base = phi + (act ? grown_index<T>(nf, sx, fx - 1, fy0, 0) : 0);
+    T w[2][4][4];                                 // [row][fine plane 2cz-1 .. 2cz+2][fine x fx-1 .. fx+2]
+    auto load4 = [&](T* d, const T* q) {
+        const P2 a = *reinterpret_cast<const P2*>(q), b = *reinterpret_cast<const P2*>(q + 2);
+        d[0] = a.x;
+        d[1] = a.y;
+        d[2] = b.x;
+        d[3] = b.y;
+    };
+    if (act) {
+#pragma unroll
+        for (int r = 0; r < 2; r++) {
+            load4(w[r][2], base + r * Sy + (long long)(2 * cz0 - 1) * Sz);
+            load4(w[r][3], base + r * Sy + (long long)(2 * cz0) * Sz);
+        }
+    }
+    for (int cz = cz0; cz < cz1; cz++) {
+        if (!act) continue;
+#pragma unroll
+        for (int r = 0; r < 2; r++) {
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                w[r][0][i] = w[r][2][i];
+                w[r][1][i] = w[r][3][i];
+            }
+            load4(w[r][2], base + r * Sy + (long long)(2 * cz + 1) * Sz);
+            load4(w[r][3], base + r * Sy + (long long)(2 * cz + 2) * Sz);
+        }
+        T res[2][2][2];                           // [row][fine plane 2cz, 2cz+1][dx]
+#pragma unroll
+        for (int pz = 0; pz < 2; pz++) {
+            const int fz = 2 * cz + pz;
+            // the rows beyond the thread's two: fy0 - 1 and fy0 + 2 at (fx, fx + 1)
+            const T* qm = base + 1 - Sy + (long long)fz * Sz;
+            const T* qp = base + 1 + 2 * Sy + (long long)fz * Sz;
+            const T om[2] = {qm[0], qm[1]}, op[2] = {qp[0], qp[1]};
+#pragma unroll
+            for (int r = 0; r < 2; r++) {
+                const long long fi = fx + (long long)nf * ((fy0 + r) + (long long)nf * fz);
+                const P2 rr = *reinterpret_cast<const P2*>(rhs + fi);
+                P2 aa;
+                if (helm) aa = *reinterpret_cast<const P2*>(alpha + fi);
+#pragma unroll
+                for (int dx = 0; dx < 2; dx++) {
+                    const T c = w[r][pz + 1][1 + dx];
+                    // taps in the Laplacian's order: 0, +x, -x, +y, -y, +z, -z
+                    const T t[7] = {c, w[r][pz + 1][2 + dx], w[r][pz + 1][dx], r == 0 ? w[1][pz + 1][1 + dx] : op[dx],
+                                    r == 1 ? w[0][pz + 1][1 + dx] : om[dx], w[r][pz + 2][1 + dx], w[r][pz][1 + dx]};
+                    const T rho = dx ? rr.y : rr.x;
+                    if (!helm) {
+                        T v = dadd(T(0), rho);
+#pragma unroll
+                        for (int j = 0; j < 7; j++) v = dmadd(v, cf.c[j], t[j]);
+                        res[r][pz][dx] = v;
+                    } else {
+                        T lp = T(0);
+#pragma unroll
+                        for (int j = 0; j < 7; j++) lp = dmadd(lp, cf.c[j], t[j]);
+                        res[r][pz][dx] = dsub(rho, dsub(dmul(dx ? aa.y : aa.x, c), dmul(beta, lp)));
+                    }
+                }
+            }
+        }
+        // children k = dx + 2 dy + 4 dz
+        T acc = T(0);
+#pragma unroll
+        for (int k = 0; k < 8; k++) acc = dmadd(acc, eighth, res[(k >> 1) & 1][k >> 2][k & 1]);
+        rhs_c[cx + (long long)nc * (cy + (long long)nc * cz)] = acc;
+    }
+}
+static inline int restrict_x2_chunk(int nf, int sms)
+{
+    const int nc = nf / 2;
+    const long long bxy = (long long)((nc + 31) / 32) * ((nc + 7) / 8);
+    const long long want = (long long)sms * 8;
+    int czc = (int)((nc * bxy + want - 1) / want);
+    return czc < 1 ? 1 : (czc > nc ? nc : czc);
+}
+static inline dim3 restrict_x2_grid(int nf, int czc)
+{
+    return dim3((nf / 2 + 31) / 32, (nf / 2 + 7) / 8, (nf / 2 + czc - 1) / czc);
+}
+
 // z chunk: about two waves of 8 blocks per SM
 static inline int restrict_z_chunk(int nf, int sms)
 {

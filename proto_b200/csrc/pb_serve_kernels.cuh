@@ -187,9 +187,22 @@ __global__ void __launch_bounds__(kSvUnit) k_sv_phase(const SvItem* __restrict__
                 } else if constexpr (OP == SV_PROLONG) {
                     const T* d = static_cast<const T*>(it.delta) + grown_index<T>(n / 2, it.sxc, 0, y / 2, z / 2);
                     T* const f = static_cast<T*>(it.in);
-                    for (int x = lane; x < n; x += 32) {
-                        T* q = f + g0 + x;
-                        store_with_images(f, n, sx, q, edge_code(x, n), ey, ez, dadd(*q, dmul(T(1), d[x / 2])));
+                    // four cells per lane in flight: their loads before their stores (a lane's stores
+                    // touch only its own valid cells and their ghost images, which no load here reads)
+                    for (int x0 = lane; x0 < n; x0 += 128) {
+                        T v[4], dv[4];
+#pragma unroll
+                        for (int k = 0; k < 4; k++) {
+                            const int x = x0 + 32 * k;
+                            v[k] = x < n ? f[g0 + x] : T(0);
+                            dv[k] = x < n ? d[x / 2] : T(0);
+                        }
+#pragma unroll
+                        for (int k = 0; k < 4; k++) {
+                            const int x = x0 + 32 * k;
+                            if (x < n)
+                                store_with_images(f, n, sx, f + g0 + x, edge_code(x, n), ey, ez, dadd(v[k], dmul(T(1), dv[k])));
+                        }
                     }
                 }
             }
